@@ -1,0 +1,312 @@
+/*
+ * luminara_gpu.h -- C ABI of the B200 path-tracing core.
+ *
+ * This header is the drop-in boundary for the per-pixel sample loop of the Luminara
+ * renderer.  Every type here is plain C: fixed-width integers, doubles, floats and
+ * pointers.  No CUDA, C++ or Python type crosses the boundary, so the library can be
+ * bound from Rust (`extern "C"`), ctypes, cgo or JNI alike.
+ *
+ * Reference interfaces replaced (paths are relative to the Luminara project root):
+ *   render()            src/render.rs:1557-1562   pub fn render(config, camera, world, lights) -> RenderResult
+ *   Hittable::hit       src/hit.rs:47-53          closest hit of one ray (here: lum_intersect on a ray set)
+ *   SceneWorld          src/scene.rs:774-839      BVH of bounded objects + linear list of planes
+ *   BvhNode::build      src/bvh.rs:16-58          (the library builds its own SAH BVH inside lum_scene_create)
+ *   LightInfo           src/render.rs:16-39       NEE light records (lum_light)
+ *   CameraConfig        src/camera.rs:17-41       (lum_camera)
+ *   RenderConfig        src/render.rs:239-431     (lum_render_params: the fields the sample loop reads)
+ *   Material / Texture  src/material.rs:15-28, src/texture.rs:4-50   (lum_material)
+ *
+ * Conventions
+ *   - Every entry point returns a lum_status; LUM_OK is 0.  On failure, lum_last_error()
+ *     returns a message for the calling thread.
+ *   - Host buffers are owned by the caller.  Device buffers created by lum_scene_create
+ *     are owned by the scene handle and freed by lum_scene_destroy.
+ *   - A scene handle owns one CUDA stream; calls on one handle are serialised on it.
+ *     Distinct handles may be used from distinct threads.
+ *   - Geometry and material parameters are given in double precision (the reference is
+ *     f64 throughout); the device computes in f32.
+ *   - Output images are float32 linear RGB, row-major, top row first, W*H*3 values
+ *     (src/render.rs:2610-2624 with exposure applied).
+ */
+#ifndef LUMINARA_GPU_H
+#define LUMINARA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LUM_ABI_VERSION 1
+
+typedef int32_t lum_status;
+enum {
+    LUM_OK = 0,
+    LUM_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad index, bad size */
+    LUM_ERR_UNSUPPORTED = 2,      /* a feature outside the GPU path (e.g. panorama camera) */
+    LUM_ERR_CUDA = 3,             /* a CUDA runtime call failed */
+    LUM_ERR_OUT_OF_MEMORY = 4,    /* device allocation failed */
+    LUM_ERR_NO_DEVICE = 5,        /* no CUDA device visible */
+    LUM_ERR_KERNEL = 6,           /* a kernel reported an error flag (stack overflow, wait limit) */
+    LUM_ERR_TOO_LARGE = 7         /* request exceeds a fixed capacity */
+};
+
+/* ------------------------------------------------------------------------------------
+ * Scene description
+ * ---------------------------------------------------------------------------------- */
+
+/* Object kinds.  Parameter layout in lum_object.p[] is given per kind.
+ * Each kind restates one reference Hittable. */
+enum {
+    LUM_OBJ_SPHERE = 1,        /* src/sphere.rs:7-68      p[0..2] center, p[3] radius */
+    LUM_OBJ_MOVING_SPHERE = 2, /* src/sphere.rs:71-125    p[0..2] center0, p[3..5] center1, p[6] radius */
+    LUM_OBJ_QUAD = 3,          /* src/quad.rs:7-72        p[0..2] Q, p[3..5] u, p[6..8] v */
+    LUM_OBJ_RECT_XY = 4,       /* src/rect.rs:8-45        p[0] x0, p[1] x1, p[2] y0, p[3] y1, p[4] k (z=k) */
+    LUM_OBJ_RECT_XZ = 5,       /* src/rect.rs:48-85       p[0] x0, p[1] x1, p[2] z0, p[3] z1, p[4] k (y=k) */
+    LUM_OBJ_RECT_YZ = 6,       /* src/rect.rs:88-125      p[0] y0, p[1] y1, p[2] z0, p[3] z1, p[4] k (x=k) */
+    LUM_OBJ_TRIANGLE = 7,      /* src/triangle.rs:7-70    p[0..2] v0, p[3..5] v1, p[6..8] v2 */
+    LUM_OBJ_DISK = 8,          /* src/disk.rs:7-65        p[0..2] center, p[3..5] normal, p[6] radius */
+    LUM_OBJ_PLANE = 9,         /* src/plane.rs:7-74       p[0..2] point, p[3..5] normal (unbounded) */
+    LUM_OBJ_BOX = 10,          /* src/rect.rs:128-141 + src/scene.rs:1561-1600
+                                  p[0..2] p_min, p[3..5] p_max: six axis rects.  With a
+                                  transform the six rects form one composite object. */
+    LUM_OBJ_FOG_SPHERE = 11,   /* src/constant_medium.rs:9-74 over a sphere boundary
+                                  p[0..2] center, p[3] radius, p[4] density; material = ISOTROPIC */
+    LUM_OBJ_FOG_BOX = 12       /* constant medium over a make_box boundary
+                                  p[0..2] p_min, p[3..5] p_max, p[6] density; material = ISOTROPIC */
+};
+
+typedef struct lum_object {
+    int32_t kind;      /* LUM_OBJ_* */
+    int32_t material;  /* index into lum_scene_desc.materials */
+    int32_t transform; /* -1, or index into lum_scene_desc.transforms */
+    int32_t reserved;
+    double p[12];
+} lum_object;
+
+/* Transform operations, applied in order (first op innermost), mirroring the wrapper
+ * order of src/scene.rs:1573-1592 (scale, rotate_x, rotate_y, rotate_z, translate). */
+enum {
+    LUM_XF_TRANSLATE = 1, /* src/transform.rs:7-29    arg xyz */
+    LUM_XF_ROTATE_X = 2,  /* src/transform.rs:108-179 arg[0] degrees */
+    LUM_XF_ROTATE_Y = 3,  /* src/transform.rs:31-106  arg[0] degrees */
+    LUM_XF_ROTATE_Z = 4,  /* src/transform.rs:181-256 arg[0] degrees */
+    LUM_XF_SCALE = 5      /* src/transform.rs:258-284 arg[0] factor */
+};
+#define LUM_MAX_XF_OPS 6
+typedef struct lum_transform {
+    int32_t n_ops;
+    int32_t op[LUM_MAX_XF_OPS];
+    int32_t reserved;
+    double arg[LUM_MAX_XF_OPS][3];
+} lum_transform;
+
+/* Triangle mesh: one reference MeshTriangle per triangle (src/obj.rs:250-320). */
+typedef struct lum_mesh {
+    const double* positions;      /* n_vertices * 3 */
+    const double* normals;        /* n_vertices * 3, or NULL for flat normals */
+    uint32_t n_vertices;
+    uint32_t n_triangles;
+    const uint32_t* indices;      /* n_triangles * 3 */
+    const int32_t* tri_material;  /* n_triangles material indices, or NULL */
+    int32_t material;             /* used when tri_material is NULL */
+    int32_t reserved;
+} lum_mesh;
+
+enum {
+    LUM_MAT_LAMBERTIAN = 1, /* src/material.rs:43-71 */
+    LUM_MAT_METAL = 2,      /* src/material.rs:75-107 */
+    LUM_MAT_DIELECTRIC = 3, /* src/material.rs:111-214 */
+    LUM_MAT_EMISSIVE = 4,   /* src/material.rs:218-244 */
+    LUM_MAT_MICROFACET = 5, /* src/material.rs:248-391 */
+    LUM_MAT_ISOTROPIC = 6   /* src/constant_medium.rs:77-89 */
+};
+enum {
+    LUM_TEX_SOLID = 0,  /* src/texture.rs:9-23 */
+    LUM_TEX_CHECKER = 1 /* src/texture.rs:26-50 */
+};
+typedef struct lum_material {
+    int32_t kind;       /* LUM_MAT_* */
+    int32_t texture;    /* LUM_TEX_* (albedo texture of Lambertian/Microfacet, colour of Emissive) */
+    double color[3];    /* albedo, emission colour, or checker "even" colour */
+    double color2[3];   /* checker "odd" colour */
+    double tex_scale;   /* checker scale */
+    double fuzz;        /* Metal (clamped to <= 1 as Metal::new does) */
+    double ior;         /* Dielectric refraction index */
+    double roughness;   /* Dielectric frost / Microfacet roughness (clamped to [0.01,1]) */
+    double metallic;    /* Microfacet (clamped to [0,1]) */
+    double intensity;   /* Emissive */
+    double dispersion;  /* Dielectric */
+    double tint[3];     /* Dielectric Beer tint; (1,1,1) = clear */
+} lum_material;
+
+enum {
+    LUM_LIGHT_SPHERE = 1, /* p0 center, radius */
+    LUM_LIGHT_RECT = 2,   /* p0 origin, u, v, normal */
+    LUM_LIGHT_DISK = 3    /* p0 center, normal, radius */
+};
+/* One NEE light (src/render.rs:16-39).  The list is given explicitly: the reference's
+ * scene loader harvests it from emissive objects (src/scene.rs:1180-1200, 1329-1344,
+ * 1388-1412, 1503-1532, 1607-1619). */
+typedef struct lum_light {
+    int32_t kind;
+    int32_t reserved;
+    double p0[3];
+    double u[3];
+    double v[3];
+    double normal[3];
+    double radius;
+    double emission[3];
+} lum_light;
+
+typedef struct lum_camera {
+    double look_from[3];
+    double look_at[3];
+    double vup[3];
+    double vfov_degrees;
+    double aspect_ratio;
+    double aperture;
+    double focus_dist;
+    int32_t panorama;   /* must be 0: the panorama branch is not on the GPU path */
+    int32_t reserved;
+} lum_camera;
+
+typedef struct lum_scene_desc {
+    const lum_object* objects;
+    uint32_t n_objects;
+    uint32_t n_meshes;
+    const lum_mesh* meshes;
+    const lum_material* materials;
+    uint32_t n_materials;
+    uint32_t n_transforms;
+    const lum_transform* transforms;
+    const lum_light* lights;
+    uint32_t n_lights;
+    uint32_t reserved;
+    lum_camera camera;
+} lum_scene_desc;
+
+/* ------------------------------------------------------------------------------------
+ * Render parameters (the RenderConfig fields the sample loop reads)
+ * ---------------------------------------------------------------------------------- */
+enum {
+    LUM_BG_SKY = 0,      /* src/render.rs:75-79 */
+    LUM_BG_SOLID = 1,    /* src/render.rs:80 */
+    LUM_BG_GRADIENT = 2, /* src/render.rs:81-85 */
+    LUM_BG_SUN = 3       /* src/render.rs:152-169 */
+};
+enum {
+    LUM_FILTER_BOX = 0, /* src/render.rs:201-237 */
+    LUM_FILTER_TRIANGLE = 1,
+    LUM_FILTER_GAUSSIAN = 2,
+    LUM_FILTER_MITCHELL = 3
+};
+typedef struct lum_render_params {
+    uint32_t width;
+    uint32_t height;
+    uint32_t samples_per_pixel; /* rounded up to a square as src/render.rs:1589-1590 */
+    uint32_t max_depth;
+    uint64_t seed;
+    int32_t background;         /* LUM_BG_* */
+    int32_t pixel_filter;       /* LUM_FILTER_* */
+    double bg_color[3];         /* SOLID colour, GRADIENT bottom, SUN sun colour */
+    double bg_color2[3];        /* GRADIENT top, SUN sky colour */
+    double bg_dir[3];           /* SUN direction */
+    double bg_intensity;        /* SUN intensity */
+    double exposure;            /* multiplies the f32 output (src/render.rs:2616-2618) */
+    int32_t has_crop;
+    uint32_t crop[4];           /* x, y, w, h  (src/render.rs:1575-1583) */
+    uint32_t sample_begin;      /* first stratum index rendered (0 for a full render) */
+    uint32_t sample_count;      /* strata rendered; 0 = all sqrt_spp^2 strata */
+    uint32_t reserved;
+} lum_render_params;
+
+typedef struct lum_stats {
+    uint64_t paths;        /* camera samples traced: the reference's "rays" count (src/main.rs:702) */
+    uint64_t segments;     /* closest-hit rays traced */
+    uint64_t shadow_rays;  /* NEE any-hit rays traced */
+    double kernel_ms;      /* device time of the render kernel(s) */
+    double total_ms;       /* host wall time of the call */
+    uint32_t error_flags;  /* kernel-reported error bits (LUM_KERR_*) */
+    uint32_t reserved;
+} lum_stats;
+
+enum {
+    LUM_KERR_STACK_OVERFLOW = 1u << 0, /* traversal stack overflowed (ray treated as miss) */
+    LUM_KERR_QUEUE_OVERFLOW = 1u << 1, /* wavefront queue overflow */
+    LUM_KERR_ITERATION_CAP = 1u << 2   /* persistent loop hit its iteration cap */
+};
+
+/* One ray of a ray set; time is the motion-blur time (src/ray.rs). */
+typedef struct lum_ray {
+    float org[3];
+    float tmin;
+    float dir[3];
+    float tmax;
+    float time;
+    float pad[3];
+} lum_ray;
+
+/* Closest-hit record (src/hit.rs:7-44).  prim_id < 0 means miss.  Primitive ids count
+ * the expanded primitives in description order: one per object (six per LUM_OBJ_BOX,
+ * in make_box order), then every mesh triangle in mesh order. */
+typedef struct lum_hit {
+    float t;
+    float u;
+    float v;
+    float normal[3];   /* faces the ray */
+    int32_t prim_id;
+    int32_t front_face;
+    int32_t material;
+    int32_t reserved;
+} lum_hit;
+
+typedef struct lum_scene lum_scene; /* opaque */
+
+/* ------------------------------------------------------------------------------------
+ * Entry points
+ * ---------------------------------------------------------------------------------- */
+
+/* ABI version (LUM_ABI_VERSION). */
+int32_t lum_abi_version(void);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* lum_last_error(void);
+
+/* Replaces scene::load_scene's world construction + SceneWorld::from_list
+ * (src/scene.rs:846-1645, 786-808): flattens transforms, builds the BVH on the host and
+ * uploads structure-of-arrays device buffers.  An empty scene is valid (every ray misses). */
+lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out_scene);
+
+/* Frees the scene's device buffers and stream. */
+lum_status lum_scene_destroy(lum_scene* scene);
+
+/* Number of expanded primitives and BVH nodes (diagnostics). */
+lum_status lum_scene_info(const lum_scene* scene, uint32_t* n_prims, uint32_t* n_nodes,
+                          uint32_t* n_lights, uint64_t* device_bytes);
+
+/* Replaces render::render (src/render.rs:1557-1731): renders into a caller-owned HOST
+ * buffer of width*height*3 floats (crop size when has_crop).  Device output buffers are
+ * owned by the scene.  stats may be NULL. */
+lum_status lum_render(lum_scene* scene, const lum_render_params* params, float* out_rgb,
+                      lum_stats* stats);
+
+/* Same as lum_render but writes a caller-owned DEVICE buffer on the caller's CUDA stream
+ * (cudaStream_t passed as void*, NULL = the scene's stream); no host copies. */
+lum_status lum_render_device(lum_scene* scene, const lum_render_params* params,
+                             float* d_out_rgb, void* stream, lum_stats* stats);
+
+/* Replaces SceneWorld::hit (src/scene.rs:816-834) for a set of rays: closest hit of each
+ * ray in [tmin, tmax].  rays/hits are HOST arrays of n entries. */
+lum_status lum_intersect(lum_scene* scene, const lum_ray* rays, uint32_t n, lum_hit* hits);
+
+/* Any-hit (shadow) query, src/render.rs:1457-1460: occluded[i] = 1 if world.hit(ray) is
+ * Some.  HOST arrays. */
+lum_status lum_occluded(lum_scene* scene, const lum_ray* rays, uint32_t n, int32_t* occluded);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LUMINARA_GPU_H */

@@ -1,0 +1,434 @@
+"""Scene construction mirroring the reference's Rust types.
+
+Reference names are kept: ``Sphere``, ``MovingSphere``, ``Quad``, ``XyRect``/``XzRect``/
+``YzRect``, ``Triangle``, ``Disk``, ``Plane``, ``make_box``, ``Translate``, ``RotateX/Y/Z``,
+``Scale``, ``ConstantMedium``, materials ``Lambertian``/``Metal``/``Dielectric``/``Emissive``/
+``Microfacet``/``Isotropic``, textures ``SolidColor``/``Checker``, ``LightInfo`` and
+``CameraConfig`` (src/sphere.rs, quad.rs, rect.rs, triangle.rs, disk.rs, plane.rs,
+transform.rs, constant_medium.rs, material.rs, texture.rs, render.rs:16-39, camera.rs:17-41).
+
+A :class:`World` collects objects the way ``HittableList`` does and is flattened into a
+``lum_scene_desc`` (include/luminara_gpu.h); the GPU library and the CPU oracle both consume
+that description.  Objects that the reference wraps in transforms become one description
+object with a transform record (boxes) or a transformed primitive.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import abi
+
+Vec = Sequence[float]
+
+
+# --------------------------------------------------------------------------------------
+# Textures and materials
+# --------------------------------------------------------------------------------------
+@dataclass
+class SolidColor:
+    color: Vec
+
+
+@dataclass
+class Checker:
+    even: Vec
+    odd: Vec
+    scale: float = 1.0
+
+
+@dataclass
+class Material:
+    kind: int
+    color: Vec = (0.0, 0.0, 0.0)
+    texture: object = None
+    fuzz: float = 0.0
+    ior: float = 1.5
+    roughness: float = 0.0
+    metallic: float = 0.0
+    intensity: float = 1.0
+    dispersion: float = 0.0
+    tint: Vec = (1.0, 1.0, 1.0)
+
+    def to_c(self) -> abi.LumMaterial:
+        m = abi.LumMaterial()
+        m.kind = self.kind
+        m.texture = abi.TEX_SOLID
+        m.color[:] = list(map(float, self.color))
+        m.tex_scale = 1.0
+        tex = self.texture
+        if isinstance(tex, SolidColor):
+            m.color[:] = list(map(float, tex.color))
+        elif isinstance(tex, Checker):
+            m.texture = abi.TEX_CHECKER
+            m.color[:] = list(map(float, tex.even))
+            m.color2[:] = list(map(float, tex.odd))
+            m.tex_scale = float(tex.scale)
+        m.fuzz = float(self.fuzz)
+        m.ior = float(self.ior)
+        m.roughness = float(self.roughness)
+        m.metallic = float(self.metallic)
+        m.intensity = float(self.intensity)
+        m.dispersion = float(self.dispersion)
+        m.tint[:] = list(map(float, self.tint))
+        return m
+
+
+def Lambertian(albedo: Vec = (0.5, 0.5, 0.5), texture=None) -> Material:
+    return Material(abi.MAT_LAMBERTIAN, color=albedo, texture=texture)
+
+
+def Metal(albedo: Vec, fuzz: float = 0.0) -> Material:
+    return Material(abi.MAT_METAL, color=albedo, fuzz=fuzz)
+
+
+def Dielectric(refraction_index: float, tint: Vec = (1.0, 1.0, 1.0), roughness: float = 0.0,
+               dispersion: float = 0.0) -> Material:
+    return Material(abi.MAT_DIELECTRIC, ior=refraction_index, tint=tint, roughness=roughness,
+                    dispersion=dispersion)
+
+
+def Emissive(color: Vec, intensity: float = 1.0, texture=None) -> Material:
+    return Material(abi.MAT_EMISSIVE, color=color, intensity=intensity, texture=texture)
+
+
+def Microfacet(albedo: Vec, roughness: float = 0.5, metallic: float = 0.0, texture=None) -> Material:
+    return Material(abi.MAT_MICROFACET, color=albedo, roughness=roughness, metallic=metallic, texture=texture)
+
+
+def Isotropic(albedo: Vec) -> Material:
+    return Material(abi.MAT_ISOTROPIC, color=albedo)
+
+
+# --------------------------------------------------------------------------------------
+# Geometry
+# --------------------------------------------------------------------------------------
+@dataclass
+class Prim:
+    kind: int
+    params: List[float]
+    material: Optional[Material]
+    xforms: List[tuple] = field(default_factory=list)
+
+
+def Sphere(center: Vec, radius: float, material: Material) -> Prim:
+    return Prim(abi.OBJ_SPHERE, [*center, radius], material)
+
+
+def MovingSphere(center0: Vec, center1: Vec, radius: float, material: Material) -> Prim:
+    return Prim(abi.OBJ_MOVING_SPHERE, [*center0, *center1, radius], material)
+
+
+def Quad(q: Vec, u: Vec, v: Vec, material: Material) -> Prim:
+    return Prim(abi.OBJ_QUAD, [*q, *u, *v], material)
+
+
+def XyRect(x0, x1, y0, y1, k, material) -> Prim:
+    return Prim(abi.OBJ_RECT_XY, [x0, x1, y0, y1, k], material)
+
+
+def XzRect(x0, x1, z0, z1, k, material) -> Prim:
+    return Prim(abi.OBJ_RECT_XZ, [x0, x1, z0, z1, k], material)
+
+
+def YzRect(y0, y1, z0, z1, k, material) -> Prim:
+    return Prim(abi.OBJ_RECT_YZ, [y0, y1, z0, z1, k], material)
+
+
+def Triangle(v0: Vec, v1: Vec, v2: Vec, material: Material) -> Prim:
+    return Prim(abi.OBJ_TRIANGLE, [*v0, *v1, *v2], material)
+
+
+def Disk(center: Vec, normal: Vec, radius: float, material: Material) -> Prim:
+    return Prim(abi.OBJ_DISK, [*center, *normal, radius], material)
+
+
+def Plane(point: Vec, normal: Vec, material: Material) -> Prim:
+    return Prim(abi.OBJ_PLANE, [*point, *normal], material)
+
+
+def make_box(p_min: Vec, p_max: Vec, material: Material) -> Prim:
+    """Six axis rects (src/rect.rs:128-141) kept together so transforms wrap them as one
+    composite object, as src/scene.rs:1561-1600 does."""
+    return Prim(abi.OBJ_BOX, [*p_min, *p_max], material)
+
+
+def ConstantMedium(boundary: Prim, density: float, color: Vec) -> Prim:
+    """Fog inside a sphere or box boundary (src/constant_medium.rs:9-74)."""
+    if boundary.kind == abi.OBJ_SPHERE:
+        return Prim(abi.OBJ_FOG_SPHERE, [*boundary.params[:4], density], Isotropic(color))
+    if boundary.kind == abi.OBJ_BOX:
+        return Prim(abi.OBJ_FOG_BOX, [*boundary.params[:6], density], Isotropic(color))
+    raise ValueError("ConstantMedium boundary must be a Sphere or make_box")
+
+
+def _wrap(obj: Prim, op: int, arg) -> Prim:
+    return Prim(obj.kind, obj.params, obj.material, obj.xforms + [(op, arg)])
+
+
+def Translate(obj: Prim, offset: Vec) -> Prim:
+    return _wrap(obj, abi.XF_TRANSLATE, tuple(offset))
+
+
+def RotateX(obj: Prim, degrees: float) -> Prim:
+    return _wrap(obj, abi.XF_ROTATE_X, (degrees, 0.0, 0.0))
+
+
+def RotateY(obj: Prim, degrees: float) -> Prim:
+    return _wrap(obj, abi.XF_ROTATE_Y, (degrees, 0.0, 0.0))
+
+
+def RotateZ(obj: Prim, degrees: float) -> Prim:
+    return _wrap(obj, abi.XF_ROTATE_Z, (degrees, 0.0, 0.0))
+
+
+def Scale(obj: Prim, factor: float) -> Prim:
+    return _wrap(obj, abi.XF_SCALE, (factor, 0.0, 0.0))
+
+
+@dataclass
+class Mesh:
+    """Triangle mesh (MeshTriangle, src/obj.rs:250-320): one primitive per triangle."""
+    positions: np.ndarray            # (V,3) float64
+    indices: np.ndarray              # (T,3) uint32
+    material: Optional[Material] = None
+    tri_material: Optional[np.ndarray] = None   # (T,) indices into World.materials
+    normals: Optional[np.ndarray] = None        # (V,3)
+
+
+# --------------------------------------------------------------------------------------
+# Lights and camera
+# --------------------------------------------------------------------------------------
+@dataclass
+class LightInfo:
+    kind: int
+    p0: Vec = (0.0, 0.0, 0.0)
+    u: Vec = (0.0, 0.0, 0.0)
+    v: Vec = (0.0, 0.0, 0.0)
+    normal: Vec = (0.0, 1.0, 0.0)
+    radius: float = 0.0
+    emission: Vec = (0.0, 0.0, 0.0)
+
+    @staticmethod
+    def Sphere(center: Vec, radius: float, emission: Vec) -> "LightInfo":
+        return LightInfo(abi.LIGHT_SPHERE, p0=center, radius=radius, emission=emission)
+
+    @staticmethod
+    def Rect(origin: Vec, u: Vec, v: Vec, normal: Vec, emission: Vec) -> "LightInfo":
+        return LightInfo(abi.LIGHT_RECT, p0=origin, u=u, v=v, normal=normal, emission=emission)
+
+    @staticmethod
+    def Disk(center: Vec, normal: Vec, radius: float, emission: Vec) -> "LightInfo":
+        return LightInfo(abi.LIGHT_DISK, p0=center, normal=normal, radius=radius, emission=emission)
+
+    def to_c(self) -> abi.LumLight:
+        l = abi.LumLight()
+        l.kind = self.kind
+        l.p0[:] = list(map(float, self.p0))
+        l.u[:] = list(map(float, self.u))
+        l.v[:] = list(map(float, self.v))
+        l.normal[:] = list(map(float, self.normal))
+        l.radius = float(self.radius)
+        l.emission[:] = list(map(float, self.emission))
+        return l
+
+
+@dataclass
+class CameraConfig:
+    """camera.rs:17-41 defaults."""
+    look_from: Vec = (0.0, 1.0, 3.0)
+    look_at: Vec = (0.0, 0.0, 0.0)
+    vup: Vec = (0.0, 1.0, 0.0)
+    vfov_degrees: float = 40.0
+    aspect_ratio: float = 16.0 / 9.0
+    aperture: float = 0.0
+    focus_dist: float = 1.0
+    panorama: bool = False
+
+    def to_c(self) -> abi.LumCamera:
+        c = abi.LumCamera()
+        c.look_from[:] = list(map(float, self.look_from))
+        c.look_at[:] = list(map(float, self.look_at))
+        c.vup[:] = list(map(float, self.vup))
+        c.vfov_degrees = float(self.vfov_degrees)
+        c.aspect_ratio = float(self.aspect_ratio)
+        c.aperture = float(self.aperture)
+        c.focus_dist = float(self.focus_dist)
+        c.panorama = 1 if self.panorama else 0
+        return c
+
+
+@dataclass
+class RenderConfig:
+    """The RenderConfig fields the sample loop reads (render.rs:239-431 defaults)."""
+    width: int = 800
+    height: int = 450
+    samples_per_pixel: int = 100
+    max_depth: int = 50
+    seed: int = 31337
+    background: int = abi.BG_SKY
+    bg_color: Vec = (0.0, 0.0, 0.0)
+    bg_color2: Vec = (0.0, 0.0, 0.0)
+    bg_dir: Vec = (0.0, 1.0, 0.0)
+    bg_intensity: float = 0.0
+    pixel_filter: int = abi.FILTER_BOX
+    exposure: float = 1.0
+    crop: Optional[Sequence[int]] = None
+    sample_begin: int = 0
+    sample_count: int = 0
+
+    def to_c(self) -> abi.LumRenderParams:
+        p = abi.LumRenderParams()
+        p.width = int(self.width)
+        p.height = int(self.height)
+        p.samples_per_pixel = int(self.samples_per_pixel)
+        p.max_depth = int(self.max_depth)
+        p.seed = int(self.seed) & 0xFFFFFFFFFFFFFFFF
+        p.background = int(self.background)
+        p.pixel_filter = int(self.pixel_filter)
+        p.bg_color[:] = list(map(float, self.bg_color))
+        p.bg_color2[:] = list(map(float, self.bg_color2))
+        p.bg_dir[:] = list(map(float, self.bg_dir))
+        p.bg_intensity = float(self.bg_intensity)
+        p.exposure = float(self.exposure)
+        if self.crop is not None:
+            p.has_crop = 1
+            p.crop[:] = [int(x) for x in self.crop]
+        p.sample_begin = int(self.sample_begin)
+        p.sample_count = int(self.sample_count)
+        return p
+
+    def out_shape(self):
+        w = max(self.width, 1)
+        h = max(self.height, 1)
+        if self.crop is not None:
+            w = min(self.crop[2], w)
+            h = min(self.crop[3], h)
+        return (h, w, 3)
+
+
+# --------------------------------------------------------------------------------------
+# World -> lum_scene_desc
+# --------------------------------------------------------------------------------------
+class World:
+    """An ordered object list (HittableList) plus NEE lights and camera.
+
+    ``add`` keeps insertion order, which fixes primitive ids: one id per object (six for a
+    box), then mesh triangles in mesh order.
+    """
+
+    def __init__(self):
+        self.objects: List[Prim] = []
+        self.meshes: List[Mesh] = []
+        self.lights: List[LightInfo] = []
+        self.materials: List[Material] = []
+        self._mat_index = {}
+        self.camera = CameraConfig()
+
+    def material_index(self, m: Optional[Material]) -> int:
+        if m is None:
+            return -1
+        key = id(m)
+        if key not in self._mat_index:
+            self._mat_index[key] = len(self.materials)
+            self.materials.append(m)
+        return self._mat_index[key]
+
+    def add(self, obj: Prim) -> int:
+        """Adds an object; returns its first primitive id."""
+        first = self.n_prims()
+        self.objects.append(obj)
+        self.material_index(obj.material)
+        return first
+
+    def add_mesh(self, mesh: Mesh) -> int:
+        first = self.n_prims()
+        self.meshes.append(mesh)
+        if mesh.material is not None:
+            self.material_index(mesh.material)
+        return first
+
+    def add_light(self, light: LightInfo) -> None:
+        self.lights.append(light)
+
+    def n_prims(self) -> int:
+        n = sum(6 if o.kind == abi.OBJ_BOX else 1 for o in self.objects)
+        return n + sum(int(m.indices.shape[0]) for m in self.meshes)
+
+    def desc(self) -> "SceneDesc":
+        return SceneDesc(self)
+
+
+class SceneDesc:
+    """Owns the ctypes arrays behind one lum_scene_desc."""
+
+    def __init__(self, world: World):
+        objs = []
+        xforms = []
+        for o in world.objects:
+            lo = abi.LumObject()
+            lo.kind = o.kind
+            lo.material = world.material_index(o.material)
+            lo.transform = -1
+            p = list(map(float, o.params)) + [0.0] * (12 - len(o.params))
+            lo.p[:] = p[:12]
+            if o.xforms:
+                if len(o.xforms) > abi.MAX_XF_OPS:
+                    raise ValueError("too many transform ops")
+                t = abi.LumTransform()
+                t.n_ops = len(o.xforms)
+                for i, (op, arg) in enumerate(o.xforms):
+                    t.op[i] = op
+                    t.arg[i][:] = list(map(float, arg))
+                lo.transform = len(xforms)
+                xforms.append(t)
+            objs.append(lo)
+        self._objects = (abi.LumObject * max(len(objs), 1))(*objs)
+        self._xforms = (abi.LumTransform * max(len(xforms), 1))(*xforms)
+        self._keep = []
+        meshes = []
+        for m in world.meshes:
+            pos = np.ascontiguousarray(m.positions, dtype=np.float64)
+            idx = np.ascontiguousarray(m.indices, dtype=np.uint32)
+            lm = abi.LumMesh()
+            lm.positions = pos.ctypes.data_as(C.POINTER(C.c_double))
+            lm.n_vertices = pos.shape[0]
+            lm.indices = idx.ctypes.data_as(C.POINTER(C.c_uint32))
+            lm.n_triangles = idx.shape[0]
+            self._keep += [pos, idx]
+            if m.normals is not None:
+                nrm = np.ascontiguousarray(m.normals, dtype=np.float64)
+                lm.normals = nrm.ctypes.data_as(C.POINTER(C.c_double))
+                self._keep.append(nrm)
+            if m.tri_material is not None:
+                tm = np.ascontiguousarray(m.tri_material, dtype=np.int32)
+                lm.tri_material = tm.ctypes.data_as(C.POINTER(C.c_int32))
+                self._keep.append(tm)
+            lm.material = world.material_index(m.material)
+            meshes.append(lm)
+        self._meshes = (abi.LumMesh * max(len(meshes), 1))(*meshes)
+        mats = [m.to_c() for m in world.materials]
+        self._materials = (abi.LumMaterial * max(len(mats), 1))(*mats)
+        lights = [l.to_c() for l in world.lights]
+        self._lights = (abi.LumLight * max(len(lights), 1))(*lights)
+        d = abi.LumSceneDesc()
+        d.objects = self._objects
+        d.n_objects = len(objs)
+        d.meshes = self._meshes
+        d.n_meshes = len(meshes)
+        d.materials = self._materials
+        d.n_materials = len(mats)
+        d.transforms = self._xforms
+        d.n_transforms = len(xforms)
+        d.lights = self._lights
+        d.n_lights = len(lights)
+        d.camera = world.camera.to_c()
+        self.c = d
+        self.n_prims = world.n_prims()
+        self.n_materials = len(mats)
+
+    def ref(self):
+        return C.byref(self.c)

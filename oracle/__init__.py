@@ -1,0 +1,256 @@
+"""ctypes binding of the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline leg, as the checker.  The product package never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from luminara_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+MODE_STREAM = 0
+MODE_KEYED = 1
+
+
+class OrcStats(C.Structure):
+    _fields_ = [
+        ("paths", C.c_uint64),
+        ("segments", C.c_uint64),
+        ("shadow_rays", C.c_uint64),
+        ("seconds", C.c_double),
+        ("threads", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+ORC_RAY = np.dtype([("org", "<f8", 3), ("tmin", "<f8"), ("dir", "<f8", 3), ("tmax", "<f8"), ("time", "<f8"),
+                    ("pad", "<f8")])
+ORC_HIT = np.dtype([("t", "<f8"), ("u", "<f8"), ("v", "<f8"), ("point", "<f8", 3), ("normal", "<f8", 3),
+                    ("prim_id", "<i4"), ("front_face", "<i4"), ("material", "<i4"), ("reserved", "<i4")])
+
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compiles liboracle.so with the committed Makefile."""
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < max(
+            os.path.getmtime(os.path.join(HERE, f)) for f in ("oracle.cpp", "oracle.h", "Makefile")):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        dp = C.POINTER(C.c_double)
+        L.orc_scene_create.argtypes = [C.POINTER(abi.LumSceneDesc), C.POINTER(vp)]
+        L.orc_scene_destroy.argtypes = [vp]
+        L.orc_intersect.argtypes = [vp, vp, C.c_uint32, vp]
+        L.orc_occluded.argtypes = [vp, vp, C.c_uint32, vp]
+        L.orc_render.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.c_int, C.c_int, dp, C.POINTER(OrcStats)]
+        L.orc_render_rows.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.c_int, C.c_int, C.c_uint32,
+                                      C.c_uint32, dp, C.POINTER(OrcStats)]
+        L.orc_scatter.argtypes = [C.POINTER(abi.LumMaterial), dp, dp, dp, C.c_double, C.c_double, C.c_double,
+                                  C.c_uint64, C.c_int, dp]
+        L.orc_schlick.argtypes = [C.c_double, C.c_double]
+        L.orc_schlick.restype = C.c_double
+        L.orc_ggx_d.argtypes = [C.c_double, C.c_double]
+        L.orc_ggx_d.restype = C.c_double
+        L.orc_camera_ray.argtypes = [C.POINTER(abi.LumCamera), C.c_double, C.c_double, C.c_uint64, dp]
+        L.orc_filter_weight.argtypes = [C.c_int, C.c_double, C.c_double]
+        L.orc_filter_weight.restype = C.c_double
+        L.orc_sample_direct_light.argtypes = [vp, dp, dp, dp, C.c_uint64, C.c_int, dp]
+        L.orc_aabb_hit.argtypes = [dp, dp, dp, C.c_double, C.c_double]
+        L.orc_scene_bbox.argtypes = [vp, C.c_int32, dp]
+        L.orc_bvh_stats.argtypes = [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+        L.orc_refract.argtypes = [dp, dp, C.c_double, dp]
+        L.orc_reflect.argtypes = [dp, dp, dp]
+        L.orc_stream_u64.argtypes = [C.c_uint64, C.c_uint32, C.POINTER(C.c_uint64)]
+        L.orc_stream_f64.argtypes = [C.c_uint64, C.c_uint32, dp]
+        L.orc_philox.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+        L.orc_xoshiro_from_state.argtypes = [C.POINTER(C.c_uint64), C.c_uint32, C.POINTER(C.c_uint64)]
+        L.orc_seed_state.argtypes = [C.c_uint64, C.POINTER(C.c_uint64)]
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a, a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class OracleScene:
+    """An oracle SceneWorld built from a luminara_b200.scene.World."""
+
+    def __init__(self, world):
+        self.desc = world.desc()
+        h = C.c_void_p()
+        rc = lib().orc_scene_create(self.desc.ref(), C.byref(h))
+        if rc != 0:
+            raise RuntimeError(f"orc_scene_create failed: {rc}")
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_scene_destroy(self.h)
+            self.h = None
+
+    def intersect(self, rays: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, dtype=ORC_RAY)
+        hits = np.zeros(rays.shape[0], dtype=ORC_HIT)
+        lib().orc_intersect(self.h, rays.ctypes.data, rays.shape[0], hits.ctypes.data)
+        return hits
+
+    def occluded(self, rays: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, dtype=ORC_RAY)
+        occ = np.zeros(rays.shape[0], dtype=np.int32)
+        lib().orc_occluded(self.h, rays.ctypes.data, rays.shape[0], occ.ctypes.data)
+        return occ
+
+    def render(self, cfg, mode=MODE_STREAM, threads=0, rows=None):
+        p = cfg.to_c()
+        shape = cfg.out_shape()
+        out = np.zeros(shape, dtype=np.float64)
+        st = OrcStats()
+        if rows is None:
+            rc = lib().orc_render(self.h, C.byref(p), mode, threads,
+                                  out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(st))
+        else:
+            rc = lib().orc_render_rows(self.h, C.byref(p), mode, threads, rows[0], rows[1],
+                                       out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(st))
+        if rc != 0:
+            raise RuntimeError(f"orc_render failed: {rc}")
+        return out, st
+
+    def sample_direct_light(self, p, n, albedo, seed, n_iter):
+        out = np.zeros((n_iter, 3))
+        pa, pp = _d(p)
+        na, nn = _d(n)
+        aa, ap = _d(albedo)
+        lib().orc_sample_direct_light(self.h, pp, nn, ap, seed, n_iter, out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out
+
+    def object_bbox(self, i):
+        out = np.zeros(6)
+        rc = lib().orc_scene_bbox(self.h, i, out.ctypes.data_as(C.POINTER(C.c_double)))
+        return None if rc else out
+
+    def bvh_stats(self):
+        n = C.c_uint32()
+        d = C.c_uint32()
+        lib().orc_bvh_stats(self.h, C.byref(n), C.byref(d))
+        return n.value, d.value
+
+
+def make_rays(org, dir, tmin=0.001, tmax=np.inf, time=0.0) -> np.ndarray:
+    org = np.atleast_2d(np.asarray(org, dtype=np.float64))
+    dir = np.atleast_2d(np.asarray(dir, dtype=np.float64))
+    n = max(org.shape[0], dir.shape[0])
+    r = np.zeros(n, dtype=ORC_RAY)
+    r["org"] = org
+    r["dir"] = dir
+    r["tmin"] = tmin
+    r["tmax"] = tmax
+    r["time"] = time
+    return r
+
+
+def scatter(material, ray_o, ray_d, point, outward_normal, t=1.0, u=0.5, v=0.5, seed=42, n_iter=1, time=0.0):
+    m = material.to_c()
+    ray = np.array([*ray_o, *ray_d, time], dtype=np.float64)
+    out = np.zeros((n_iter, 8))
+    p = np.asarray(point, dtype=np.float64)
+    n = np.asarray(outward_normal, dtype=np.float64)
+    lib().orc_scatter(C.byref(m), ray.ctypes.data_as(C.POINTER(C.c_double)),
+                      p.ctypes.data_as(C.POINTER(C.c_double)), n.ctypes.data_as(C.POINTER(C.c_double)),
+                      t, u, v, seed, n_iter, out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out
+
+
+def schlick(cosine, ref_idx):
+    return lib().orc_schlick(cosine, ref_idx)
+
+
+def ggx_d(n_dot_h, alpha):
+    return lib().orc_ggx_d(n_dot_h, alpha)
+
+
+def camera_ray(cam_cfg, s, t, seed=0):
+    c = cam_cfg.to_c()
+    out = np.zeros(7)
+    lib().orc_camera_ray(C.byref(c), s, t, seed, out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out[:3], out[3:6], out[6]
+
+
+def filter_weight(f, dx, dy):
+    return lib().orc_filter_weight(f, dx, dy)
+
+
+def aabb_hit(mn, mx, o, d, tmin=0.001, tmax=np.inf):
+    mn = np.asarray(mn, dtype=np.float64)
+    mx = np.asarray(mx, dtype=np.float64)
+    ray = np.array([*o, *d, 0.0], dtype=np.float64)
+    P = C.POINTER(C.c_double)
+    return bool(lib().orc_aabb_hit(mn.ctypes.data_as(P), mx.ctypes.data_as(P), ray.ctypes.data_as(P), tmin, tmax))
+
+
+def refract(v, n, eta):
+    v = np.asarray(v, dtype=np.float64)
+    n = np.asarray(n, dtype=np.float64)
+    out = np.zeros(3)
+    P = C.POINTER(C.c_double)
+    lib().orc_refract(v.ctypes.data_as(P), n.ctypes.data_as(P), eta, out.ctypes.data_as(P))
+    return out
+
+
+def reflect(v, n):
+    v = np.asarray(v, dtype=np.float64)
+    n = np.asarray(n, dtype=np.float64)
+    out = np.zeros(3)
+    P = C.POINTER(C.c_double)
+    lib().orc_reflect(v.ctypes.data_as(P), n.ctypes.data_as(P), out.ctypes.data_as(P))
+    return out
+
+
+def stream_u64(seed, n):
+    out = (C.c_uint64 * n)()
+    lib().orc_stream_u64(seed, n, out)
+    return [int(x) for x in out]
+
+
+def stream_f64(seed, n):
+    out = np.zeros(n)
+    lib().orc_stream_f64(seed, n, out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out
+
+
+def philox(ctr, key):
+    c = (C.c_uint32 * 4)(*ctr)
+    k = (C.c_uint32 * 2)(*key)
+    o = (C.c_uint32 * 4)()
+    lib().orc_philox(c, k, o)
+    return [int(x) for x in o]
+
+
+def xoshiro_from_state(state, n):
+    st = (C.c_uint64 * 4)(*state)
+    out = (C.c_uint64 * n)()
+    lib().orc_xoshiro_from_state(st, n, out)
+    return [int(x) for x in out]
+
+
+def seed_state(seed):
+    out = (C.c_uint64 * 4)()
+    lib().orc_seed_state(seed, out)
+    return [int(x) for x in out]

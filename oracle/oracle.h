@@ -1,0 +1,99 @@
+/*
+ * oracle.h -- TEST INFRASTRUCTURE, not part of the product.
+ *
+ * CPU f64 restatement of the Luminara per-pixel sample loop, used only by tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg as the checker.  Nothing in
+ * luminara_b200/ links or calls it.
+ *
+ * Parity status: the Rust reference cannot be built on this machine (no cargo/rustc, no
+ * vendored crates), so this restatement is pinned against the reference's own unit-test
+ * known answers (restated in tests/test_oracle_kat.py), not against reference output.
+ * Bitwise image parity with the reference is unpinned: its RNG (rand 0.9.2 SmallRng) is
+ * restated from the published xoshiro256++/SplitMix64 definitions, but no reference test
+ * pins RNG-stream values.
+ */
+#ifndef LUMINARA_ORACLE_H
+#define LUMINARA_ORACLE_H
+
+#include "../include/luminara_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_scene orc_scene;
+
+enum { ORC_MODE_STREAM = 0, ORC_MODE_KEYED = 1 };
+
+typedef struct orc_stats {
+    uint64_t paths;
+    uint64_t segments;
+    uint64_t shadow_rays;
+    double seconds;
+    int32_t threads;
+    int32_t reserved;
+} orc_stats;
+
+/* A ray in double precision: org[3], tmin, dir[3], tmax, time, pad. */
+typedef struct orc_ray {
+    double org[3];
+    double tmin;
+    double dir[3];
+    double tmax;
+    double time;
+    double pad;
+} orc_ray;
+
+typedef struct orc_hit {
+    double t, u, v;
+    double point[3];
+    double normal[3];
+    int32_t prim_id;
+    int32_t front_face;
+    int32_t material;
+    int32_t reserved;
+} orc_hit;
+
+int orc_scene_create(const lum_scene_desc* desc, orc_scene** out);
+void orc_scene_destroy(orc_scene* s);
+/* Closest hit of each ray (SceneWorld::hit).  hits[i].prim_id < 0 on a miss. */
+int orc_intersect(const orc_scene* s, const orc_ray* rays, uint32_t n, orc_hit* hits);
+/* Shadow query: occluded[i] = world.hit(ray).is_some(). */
+int orc_occluded(const orc_scene* s, const orc_ray* rays, uint32_t n, int32_t* occluded);
+/* render() non-adaptive branch; out_rgb = W*H*3 doubles (exposure applied, not cast to f32). */
+int orc_render(const orc_scene* s, const lum_render_params* p, int mode, int threads,
+               double* out_rgb, orc_stats* stats);
+/* Renders only rows [row_begin, row_end) of the (cropped) image into out_rgb rows of the
+ * same index; used for bounded CPU-baseline samples. */
+int orc_render_rows(const orc_scene* s, const lum_render_params* p, int mode, int threads,
+                    uint32_t row_begin, uint32_t row_end, double* out_rgb, orc_stats* stats);
+
+/* Known-answer helpers mirroring the reference's unit tests. */
+int orc_scatter(const lum_material* m, const double ray[7], const double hit_point[3],
+                const double outward_normal[3], double t, double u, double v, uint64_t seed,
+                int n_iter, double* out /* n_iter * 8: ok, dir[3], att[3], front */);
+double orc_schlick(double cosine, double ref_idx);
+double orc_ggx_d(double n_dot_h, double alpha);
+int orc_camera_ray(const lum_camera* c, double s, double t, uint64_t seed, double out[7]);
+double orc_filter_weight(int filter, double dx, double dy);
+int orc_sample_direct_light(const orc_scene* s, const double p[3], const double n[3],
+                            const double albedo[3], uint64_t seed, int n_iter, double* out);
+int orc_aabb_hit(const double mn[3], const double mx[3], const double ray[7], double tmin,
+                 double tmax);
+int orc_scene_bbox(const orc_scene* s, int32_t object_index, double out[6]);
+int orc_bvh_stats(const orc_scene* s, uint32_t* n_nodes, uint32_t* depth);
+/* Vector helpers (vec3.rs): refract, reflect. */
+void orc_refract(const double v[3], const double n[3], double eta, double out[3]);
+void orc_reflect(const double v[3], const double n[3], double out[3]);
+/* RNG pins: SmallRng stream outputs and Philox4x32-10 blocks. */
+void orc_stream_u64(uint64_t seed, uint32_t n, uint64_t* out);
+void orc_stream_f64(uint64_t seed, uint32_t n, double* out);
+void orc_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+/* xoshiro256++ outputs from a raw state, and the SplitMix64-expanded state of a u64 seed. */
+void orc_xoshiro_from_state(const uint64_t state[4], uint32_t n, uint64_t* out);
+void orc_seed_state(uint64_t seed, uint64_t out[4]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,378 @@
+"""Pins the CPU oracle against the reference's own known answers.
+
+Each test restates one of the reference's unit tests for the hot path (file:line in the
+Luminara project) and runs it against the oracle, plus the published test vectors of the
+RNGs the oracle restates.  CPU only.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle as O
+from luminara_b200 import abi
+from luminara_b200 import scene as S
+
+INF = math.inf
+GRAY = (0.5, 0.5, 0.5)
+
+
+def world_of(*objs):
+    w = S.World()
+    for o in objs:
+        w.add(o)
+    return O.OracleScene(w)
+
+
+def hit1(sc, o, d, tmin=0.001, tmax=INF):
+    h = sc.intersect(O.make_rays(o, d, tmin, tmax))[0]
+    return h if h["prim_id"] >= 0 else None
+
+
+# ---------------------------------------------------------------- RNG pins
+def test_xoshiro256pp_published_vector():
+    # xoshiro256++ reference test vector (state 1,2,3,4)
+    exp = [41943041, 58720359, 3588806011781223, 3591011842654386, 9228616714210784205,
+           9973669472204895162, 14011001112246962877, 12406186145184390807, 15849039046786891736,
+           10450023813501588000]
+    assert O.xoshiro_from_state([1, 2, 3, 4], 10) == exp
+
+
+def test_splitmix64_seed_expansion():
+    # SplitMix64 from state 0: first output 0xe220a8397b1dcdaf (published value)
+    assert O.seed_state(0)[0] == 0xE220A8397B1DCDAF
+
+
+def test_f64_draws_in_unit_interval():
+    x = O.stream_f64(31337, 10000)
+    assert x.min() >= 0.0 and x.max() < 1.0
+    assert abs(x.mean() - 0.5) < 0.02
+
+
+def test_philox_random123_kat():
+    assert O.philox([0, 0, 0, 0], [0, 0]) == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+    assert O.philox([0xFFFFFFFF] * 4, [0xFFFFFFFF] * 2) == [0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD]
+    assert O.philox([0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344], [0xA4093822, 0x299F31D0]) == \
+        [0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]
+
+
+# ---------------------------------------------------------------- vec3.rs:261-295
+def test_reflect():
+    r = O.reflect([1.0, -1.0, 0.0], [0.0, 1.0, 0.0])
+    assert abs(r[0] - 1.0) < 1e-10 and abs(r[1] - 1.0) < 1e-10
+
+
+def test_refract_normal_incidence():
+    r = O.refract([0.0, -1.0, 0.0], [0.0, 1.0, 0.0], 1.0 / 1.5)
+    assert abs(r[0]) < 1e-6 and r[1] < 0.0
+
+
+# ---------------------------------------------------------------- aabb.rs:197-224
+def test_aabb_hit_miss_negative():
+    assert O.aabb_hit([-1, -1, -1], [1, 1, 1], [0, 0, -5], [0, 0, 1])
+    assert not O.aabb_hit([-1, -1, -1], [1, 1, 1], [0, 5, -5], [0, 0, 1])
+    assert O.aabb_hit([-1, -1, -1], [1, 1, 1], [0, 0, 5], [0, 0, -1])
+
+
+# ---------------------------------------------------------------- bvh.rs:437-471
+def test_bvh_basic_hit():
+    sc = world_of(S.Sphere((0, 0, -1), 0.5, S.Lambertian(GRAY)), S.Sphere((2, 0, -1), 0.5, S.Lambertian(GRAY)))
+    assert hit1(sc, (0, 0, 0), (0, 0, -1)) is not None
+    assert hit1(sc, (0, 5, 0), (0, 0, -1)) is None
+
+
+def test_bvh_many_objects():
+    w = S.World()
+    for i in range(50):
+        w.add(S.Sphere((i * 2.0, 0, 0), 0.5, S.Lambertian(GRAY)))
+    sc = O.OracleScene(w)
+    h = hit1(sc, (0, 0, -2), (0, 0, 1))
+    assert h is not None and h["prim_id"] == 0
+    assert hit1(sc, (0, 5, 0), (0, 0, 1)) is None
+    nodes, depth = sc.bvh_stats()
+    assert nodes == 49  # binary tree over 50 single-object leaves
+
+
+# ---------------------------------------------------------------- sphere.rs:141-244
+def test_sphere_bbox_and_uv():
+    w = S.World()
+    w.add(S.Sphere((1, 2, 3), 0.5, S.Lambertian(GRAY)))
+    sc = O.OracleScene(w)
+    bb = sc.object_bbox(0)
+    np.testing.assert_allclose(bb, [0.5, 1.5, 2.5, 1.5, 2.5, 3.5], atol=1e-6)
+    sc = world_of(S.Sphere((0, 0, 0), 1.0, S.Lambertian(GRAY)))
+    for d in [(0, 0, -1), (0, 0, 1), (1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (1, 1, 1), (-1, -1, -1)]:
+        o = -3.0 * np.asarray(d, dtype=float)
+        h = hit1(sc, o, d)
+        if h is not None:
+            assert 0.0 <= h["u"] <= 1.0 and 0.0 <= h["v"] <= 1.0
+
+
+def test_moving_sphere_time():
+    sc = world_of(S.MovingSphere((0, 0, 0), (10, 0, 0), 1.0, S.Lambertian(GRAY)))
+    assert sc.intersect(O.make_rays((0, 0, -5), (0, 0, 1), time=0.0))[0]["prim_id"] == 0
+    assert sc.intersect(O.make_rays((10, 0, -5), (0, 0, 1), time=1.0))[0]["prim_id"] == 0
+    assert sc.intersect(O.make_rays((0, 0, -5), (0, 0, 1), time=1.0))[0]["prim_id"] == -1
+
+
+def test_sphere_miss():
+    sc = world_of(S.Sphere((1, 2, 3), 0.5, S.Lambertian(GRAY)))
+    assert hit1(sc, (100, 100, 100), (0, 0, -1)) is None
+
+
+# ---------------------------------------------------------------- quad.rs:330-403
+def test_quad_hit_center_known_answer():
+    sc = world_of(S.Quad((0, 0, 0), (1, 0, 0), (0, 0, 1), S.Lambertian(GRAY)))
+    h = hit1(sc, (0.5, 1.0, 0.5), (0, -1, 0))
+    assert h is not None
+    assert abs(h["t"] - 1.0) < 1e-6 and abs(h["u"] - 0.5) < 1e-6 and abs(h["v"] - 0.5) < 1e-6
+
+
+def test_quad_miss_outside_parallel_and_tilted():
+    sc = world_of(S.Quad((0, 0, 0), (1, 0, 0), (0, 0, 1), S.Lambertian(GRAY)))
+    assert hit1(sc, (2.0, 1.0, 0.5), (0, -1, 0)) is None
+    assert hit1(sc, (0.5, 1.0, 0.5), (1, 0, 0)) is None
+    sc = world_of(S.Quad((0, 0, 0), (1, 1, 0), (0, 0, 1), S.Lambertian(GRAY)))
+    assert hit1(sc, (1.5, -0.5, 0.5), (-1, 1, 0)) is not None
+
+
+def test_quad_bbox_padding():
+    w = S.World()
+    w.add(S.Quad((0, 0, 0), (2, 0, 0), (0, 3, 0), S.Lambertian(GRAY)))
+    bb = O.OracleScene(w).object_bbox(0)
+    assert bb[0] < 0.001 and bb[3] > 1.999 and bb[4] > 2.999
+
+
+# ---------------------------------------------------------------- rect.rs:149-171
+def test_xz_rect_hit_miss_and_box():
+    sc = world_of(S.XzRect(0, 1, 0, 1, 0, S.Lambertian(GRAY)))
+    assert hit1(sc, (0.5, 1.0, 0.5), (0, -1, 0)) is not None
+    assert hit1(sc, (2.0, 1.0, 0.5), (0, -1, 0)) is None
+    w = S.World()
+    first = w.add(S.make_box((0, 0, 0), (1, 1, 1), S.Lambertian(GRAY)))
+    assert first == 0 and w.n_prims() == 6
+
+
+# ---------------------------------------------------------------- triangle.rs:251-287
+def test_triangle_hit_miss_bbox():
+    tri = S.Triangle((0, 0, 0), (1, 0, 0), (0, 1, 0), S.Lambertian(GRAY))
+    sc = world_of(tri)
+    assert hit1(sc, (0.2, 0.2, -1), (0, 0, 1)) is not None
+    assert hit1(sc, (2, 2, -1), (0, 0, 1)) is None
+    w = S.World()
+    w.add(tri)
+    bb = O.OracleScene(w).object_bbox(0)
+    assert bb[0] < 0.001 and bb[3] > 0.999 and bb[4] > 0.999
+
+
+# ---------------------------------------------------------------- disk.rs:361-383
+def test_disk_hit_and_miss_outside_radius():
+    sc = world_of(S.Disk((0, 0, 0), (0, 1, 0), 1.0, S.Lambertian(GRAY)))
+    assert hit1(sc, (0, 1, 0), (0, -1, 0)) is not None
+    assert hit1(sc, (5, 1, 0), (0, -1, 0)) is None
+
+
+# ---------------------------------------------------------------- plane.rs:470-507
+def test_plane_known_answers():
+    sc = world_of(S.Plane((0, 0, 0), (0, 1, 0), S.Lambertian(GRAY)))
+    h = hit1(sc, (0, 5, 0), (0, -1, 0))
+    assert h is not None and abs(h["t"] - 5.0) < 1e-6
+    assert hit1(sc, (0, 1, 0), (1, 0, 0)) is None
+    h = hit1(sc, (0.3, 5.0, 0.7), (0, -1, 0))
+    assert 0.0 <= h["u"] <= 1.0 and 0.0 <= h["v"] <= 1.0
+    w = S.World()
+    w.add(S.Plane((0, 0, 0), (0, 1, 0), S.Lambertian(GRAY)))
+    assert O.OracleScene(w).object_bbox(0) is None  # unbounded
+    # zero-normal fallback -> up normal: a downward ray hits with normal +y
+    sc = world_of(S.Plane((0, 0, 0), (0, 0, 0), S.Lambertian(GRAY)))
+    h = hit1(sc, (0, 5, 0), (0, -1, 0))
+    assert abs(h["normal"][1] - 1.0) < 1e-6
+
+
+# ---------------------------------------------------------------- transform.rs:365-422
+def test_translate():
+    sc = world_of(S.Translate(S.Sphere((0, 0, 0), 1.0, S.Lambertian(GRAY)), (5, 0, 0)))
+    assert hit1(sc, (5, 0, -5), (0, 0, 1)) is not None
+    assert hit1(sc, (0, 0, -5), (0, 0, 1)) is None
+
+
+def test_scale_hit_point():
+    w = S.World()
+    w.add(S.Scale(S.Sphere((0, 0, 0), 1.0, S.Lambertian(GRAY)), 2.0))
+    sc = O.OracleScene(w)
+    h = hit1(sc, (0, 0, -5), (0, 0, 1))
+    assert abs(h["point"][2] - -2.0) < 0.01
+    assert abs(sc.object_bbox(0)[3] - 2.0) < 0.01
+
+
+@pytest.mark.parametrize("rot,center,o,d", [
+    (S.RotateY, (2, 0, 0), (0, 0, -5), (0, 0, 1)),
+    (S.RotateX, (0, 2, 0), (0, 0, -5), (0, 0, 1)),
+    (S.RotateZ, (2, 0, 0), (0, 5, 0), (0, -1, 0)),
+])
+def test_rotations(rot, center, o, d):
+    sc = world_of(rot(S.Sphere(center, 0.5, S.Lambertian(GRAY)), 90.0))
+    assert hit1(sc, o, d) is not None
+
+
+# ---------------------------------------------------------------- constant_medium.rs:114-137
+def test_constant_medium_bbox_and_dense_hit():
+    w = S.World()
+    w.add(S.ConstantMedium(S.Sphere((0, 0, 0), 1.0, S.Lambertian(GRAY)), 0.5, (1, 1, 1)))
+    bb = O.OracleScene(w).object_bbox(0)
+    assert abs(bb[0] + 1.0) < 1e-4 and abs(bb[3] - 1.0) < 1e-4
+    sc = world_of(S.ConstantMedium(S.Sphere((0, 0, 0), 5.0, S.Lambertian(GRAY)), 100.0, (1, 1, 1)))
+    assert hit1(sc, (0, 0, -10), (0, 0, 1)) is not None
+
+
+# ---------------------------------------------------------------- camera.rs:480-548
+def test_camera_center_and_corners():
+    cam = S.CameraConfig(look_from=(0, 0, 0), look_at=(0, 0, -1), vfov_degrees=90.0, aspect_ratio=2.0)
+    _, d, _ = O.camera_ray(cam, 0.5, 0.5, seed=0)
+    d = d / np.linalg.norm(d)
+    assert abs(d[0]) < 1e-6 and abs(d[1]) < 1e-6 and d[2] < 0
+    _, d, _ = O.camera_ray(cam, 0.0, 0.0, seed=0)
+    assert d[0] < 0 and d[1] < 0
+    _, d, _ = O.camera_ray(cam, 1.0, 1.0, seed=0)
+    assert d[0] > 0 and d[1] > 0
+
+
+def test_camera_zero_aperture_origin():
+    cam = S.CameraConfig(look_from=(1, 2, 3), look_at=(0, 0, 0), vfov_degrees=40.0, aspect_ratio=1.0)
+    o, _, _ = O.camera_ray(cam, 0.5, 0.5, seed=99)
+    np.testing.assert_allclose(o, [1, 2, 3], atol=1e-6)
+
+
+# ---------------------------------------------------------------- material.rs:909-1235
+HIT = dict(ray_o=(0, 1, 0), ray_d=(0, -1, 0), point=(0, 0, 0), outward_normal=(0, 1, 0), t=1.0, u=0.5, v=0.5)
+
+
+def test_lambertian_hemisphere_and_attenuation():
+    out = O.scatter(S.Lambertian((0.8, 0.2, 0.2)), seed=42, n_iter=100, **HIT)
+    assert (out[:, 0] == 1).all()
+    assert (out[:, 2] >= 0.0).all()
+    np.testing.assert_allclose(out[:, 4:7], np.tile([0.8, 0.2, 0.2], (100, 1)), atol=1e-6)
+
+
+def test_metal_exact_mirror():
+    h = dict(HIT)
+    h["ray_o"] = (-1, 1, 0)
+    h["ray_d"] = tuple(np.array([1.0, -1.0, 0.0]) / math.sqrt(2))
+    out = O.scatter(S.Metal((0.9, 0.9, 0.9), 0.0), seed=42, **h)
+    d = out[0, 1:4] / np.linalg.norm(out[0, 1:4])
+    np.testing.assert_allclose(d, np.array([1, 1, 0]) / math.sqrt(2), atol=1e-6)
+
+
+def test_metal_absorbs_at_grazing_with_fuzz():
+    h = dict(HIT)
+    h["ray_o"] = (-1, 0.01, 0)
+    h["ray_d"] = tuple(np.array([1.0, -0.01, 0.0]) / np.linalg.norm([1.0, -0.01, 0.0]))
+    out = O.scatter(S.Metal((0.9, 0.9, 0.9), 1.0), seed=42, n_iter=200, **h)
+    assert (out[:, 0] == 0).any()
+
+
+def test_dielectric_white_attenuation_and_tir():
+    out = O.scatter(S.Dielectric(1.5), seed=42, n_iter=100, **HIT)
+    assert (out[:, 0] == 1).all()
+    np.testing.assert_allclose(out[:, 4:7], 1.0, atol=1e-6)
+    assert (np.linalg.norm(out[:, 1:4], axis=1) > 1e-6).all()
+    d = np.array([0.8, 0.6, 0.0]) / 1.0
+    out = O.scatter(S.Dielectric(2.5), ray_o=(0, -1, 0), ray_d=tuple(d), point=(0, 0, 0),
+                    outward_normal=(0, 1, 0), seed=42)
+    assert out[0, 0] == 1 and out[0, 7] == 0  # hit from inside
+    assert np.linalg.norm(out[0, 1:4]) > 1e-6
+
+
+def test_emissive_values_and_no_scatter():
+    out = O.scatter(S.Emissive((1.0, 0.8, 0.6), 2.0), seed=42, **HIT)
+    assert out[0, 0] == 0
+
+
+def test_schlick_known_answers():
+    ratio = 1.0 / 1.5
+    assert abs(O.schlick(1.0, ratio) - ((1 - ratio) / (1 + ratio)) ** 2) < 1e-6
+    assert O.schlick(0.01, ratio) > 0.9
+
+
+def test_microfacet_valid_and_diffuse():
+    out = O.scatter(S.Microfacet((0.9, 0.1, 0.1), 0.3, 1.0), seed=42, n_iter=200, **HIT)
+    ok = out[:, 0] == 1
+    assert ok.sum() > 50
+    assert (out[ok, 4:7] >= 0).all()
+    assert (np.linalg.norm(out[ok, 1:4], axis=1) > 1e-6).all()
+    out = O.scatter(S.Microfacet((0.8, 0.2, 0.1), 0.5, 0.0), seed=42, n_iter=100, **HIT)
+    ok = out[:, 0] == 1
+    assert (out[ok, 4] > out[ok, 5]).any()
+    assert O.ggx_d(1.0, 0.25) > O.ggx_d(0.5, 0.25) > 0
+
+
+def test_dielectric_dispersion_separates_channels():
+    out = O.scatter(S.Dielectric(1.5, dispersion=0.03), seed=42, n_iter=300, **HIT)
+    a = out[:, 4:7]
+    assert ((a[:, 0] > 1) & (a[:, 1] < 0.1) & (a[:, 2] < 0.1)).any()
+    assert ((a[:, 1] > 1) & (a[:, 0] < 0.1) & (a[:, 2] < 0.1)).any()
+    assert ((a[:, 2] > 1) & (a[:, 0] < 0.1) & (a[:, 1] < 0.1)).any()
+
+
+# ---------------------------------------------------------------- render.rs:3774-3880 (NEE)
+def _nee_scene(blocker: bool):
+    w = S.World()
+    if blocker:
+        w.add(S.Sphere((0, 2.5, 0), 1.0, S.Lambertian(GRAY)))
+        w.add(S.Sphere((0, 5, 0), 0.5, S.Emissive((1, 1, 1), 10.0)))
+        w.add_light(S.LightInfo.Sphere((0, 5, 0), 0.5, (10, 10, 10)))
+    else:
+        w.add(S.Sphere((0, -1000, 0), 1000.0, S.Lambertian((0.8, 0.8, 0.8))))
+        w.add(S.Sphere((0, 5, 0), 1.0, S.Emissive((1, 1, 1), 10.0)))
+        w.add_light(S.LightInfo.Sphere((0, 5, 0), 1.0, (10, 10, 10)))
+    return O.OracleScene(w)
+
+
+def test_nee_direct_light_nonzero():
+    r = _nee_scene(False).sample_direct_light((0, 0, 0), (0, 1, 0), (0.8, 0.8, 0.8), 42, 1000)
+    avg = r.mean(axis=0)
+    assert avg[0] > 0 and avg[1] > 0
+
+
+def test_nee_no_lights_zero():
+    sc = O.OracleScene(S.World())
+    r = sc.sample_direct_light((0, 0, 0), (0, 1, 0), (0.8, 0.8, 0.8), 42, 10)
+    assert (r == 0).all()
+
+
+def test_nee_occluded_zero():
+    r = _nee_scene(True).sample_direct_light((0, 0, 0), (0, 1, 0), (0.8, 0.8, 0.8), 42, 100)
+    assert r[:, 0].sum() == 0.0
+
+
+# ---------------------------------------------------------------- render.rs:3932-3953
+def test_pixel_filters():
+    assert O.filter_weight(abi.FILTER_BOX, 0, 0) == 1.0
+    assert O.filter_weight(abi.FILTER_BOX, 0.4, 0.4) == 1.0
+    assert O.filter_weight(abi.FILTER_BOX, -0.5, -0.5) == 1.0
+    assert O.filter_weight(abi.FILTER_GAUSSIAN, 0, 0) > O.filter_weight(abi.FILTER_GAUSSIAN, 0.4, 0.4)
+    assert O.filter_weight(abi.FILTER_MITCHELL, 0, 0) > 0.5
+
+
+# ---------------------------------------------------------------- render.rs:3979-4007
+@pytest.mark.parametrize("mode", [O.MODE_STREAM, O.MODE_KEYED])
+def test_render_minimal_scene(mode):
+    w = S.World()
+    w.add(S.Sphere((0, 0, -1), 0.5, S.Lambertian(GRAY)))
+    sc = O.OracleScene(w)
+    cfg = S.RenderConfig(width=10, height=10, samples_per_pixel=1, max_depth=3)
+    img, st = sc.render(cfg, mode=mode)
+    assert img.shape == (10, 10, 3)
+    assert st.paths == 100 and st.segments >= 100
+    assert np.isfinite(img).all() and img.max() > 0
+
+
+def test_stream_render_is_thread_count_independent():
+    w = S.World()
+    w.add(S.Sphere((0, 0, -1), 0.5, S.Lambertian(GRAY)))
+    w.add(S.Sphere((0, -100.5, -1), 100, S.Lambertian((0.8, 0.8, 0.0))))
+    sc = O.OracleScene(w)
+    cfg = S.RenderConfig(width=16, height=12, samples_per_pixel=4, max_depth=8)
+    a, _ = sc.render(cfg, threads=1)
+    b, _ = sc.render(cfg, threads=4)
+    assert np.array_equal(a, b)
