@@ -1,0 +1,392 @@
+#!/usr/bin/env python
+"""Benchmark of the path-tracing hot path: Mpaths/s on B200.
+
+One step renders one full frame of the workload (default: the random-spheres field,
+1920x1080, 256 spp, depth 16) with the megakernel, scene resident in HBM.  Prints ONE JSON
+line on rank 0.  Under torchrun each rank renders its own frame (independent seeds, weak
+scaling, no data-path collective).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference estimator on the host cores: the Rust reference cannot
+be built here, so its CPU restatement (oracle/, stream-RNG mode, all host threads) renders a
+bounded sample of the same workload per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Algorithmic cost per counted test (FP32 flops, bytes read): AABB 18/24, sphere 28/16,
+# quad 54/64, triangle 52/36, disk 28/32; a node visit slab-tests two child boxes.  Fog
+# tests (boundary roots + hash) and plane tests are charged like a disk.
+COST = {
+    "node_visits": (36, 48),
+    "sphere_tests": (28, 16),
+    "quad_tests": (54, 64),
+    "triangle_tests": (52, 36),
+    "disk_tests": (28, 32),
+    "fog_tests": (28, 32),
+    "plane_tests": (28, 32),
+}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", default="random_spheres")
+    ap.add_argument("--width", type=int, default=0)
+    ap.add_argument("--height", type=int, default=0)
+    ap.add_argument("--spp", type=int, default=0)
+    ap.add_argument("--depth", type=int, default=0)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def workload(args, rank=0):
+    from luminara_b200 import workloads as W
+
+    world, cfg = W.CONFIGS[args.config]()
+    if args.width:
+        cfg.width = args.width
+    if args.height:
+        cfg.height = args.height
+    if args.width or args.height:
+        world.camera.aspect_ratio = cfg.width / cfg.height
+    if args.spp:
+        cfg.samples_per_pixel = args.spp
+    if args.depth:
+        cfg.max_depth = args.depth
+    cfg.seed = cfg.seed + 7919 * rank
+    return world, cfg
+
+
+def strata(cfg):
+    import math
+
+    n = math.ceil(math.sqrt(cfg.samples_per_pixel))
+    return n * n
+
+
+def workload_name(args, cfg):
+    return f"{args.config} {cfg.width}x{cfg.height} {cfg.samples_per_pixel}spp ({strata(cfg)} strata) depth {cfg.max_depth}"
+
+
+# ------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region (200 ms period)."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+                power.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "power_w_max": max(power) if power else None, "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------------------------ peaks
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), d.get("sm_max_mhz", 1965.0), "measured"
+    return 6650.0, 1965.0, "fallback"
+
+
+def ncu_traffic(kernel="k_render", workload=None):
+    """DRAM bytes per launch recorded in profiles/<kernel>_<workload>.md by the ncu summary."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_full_launch:"):
+            try:
+                return int(float(line.split(":")[1].strip()))
+            except ValueError:
+                return None
+    return None
+
+
+# ------------------------------------------------------------------------------ CPU baseline
+def cpu_sample(world, cfg, target_s, threads=0):
+    """Reference estimator (oracle stream mode) on evenly spaced image rows, sized so the
+    sample takes about target_s seconds.  Returns (paths, seconds, rows, threads)."""
+    import oracle as O
+
+    sc = O.OracleScene(world)
+    h = cfg.height
+    total_paths, total_s, rows = 0, 0.0, []
+    # calibrate on two rows, then choose the row count for the target time
+    probe = [h // 3, (2 * h) // 3]
+    for j in probe:
+        _, st = sc.render(cfg, mode=O.MODE_STREAM, threads=threads, rows=(j, j + 1))
+        total_paths += st.paths
+        total_s += st.seconds
+        rows.append(j)
+        used = st.threads
+    per_row = total_s / len(probe)
+    n_more = max(0, int((target_s - total_s) / max(per_row, 1e-6)))
+    n_more = min(n_more, h - len(probe))
+    if n_more > 0:
+        step = h / n_more
+        for k in range(n_more):
+            j = int(k * step + step / 2)
+            _, st = sc.render(cfg, mode=O.MODE_STREAM, threads=threads, rows=(j, j + 1))
+            total_paths += st.paths
+            total_s += st.seconds
+            rows.append(j)
+    return total_paths, total_s, len(rows), used
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    world, cfg = workload(args)
+    per_step = max(2.0, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
+    for _ in range(args.warmup):
+        cpu_sample(world, cfg, per_step / 4)
+    paths, secs, rows, threads = 0, 0.0, 0, 0
+    for _ in range(args.steps):
+        p, s, r, threads = cpu_sample(world, cfg, per_step)
+        paths += p
+        secs += s
+        rows += r
+    value = paths / secs / 1e6
+    sample = (f"{rows} image rows (evenly spaced, {cfg.width} px x {strata(cfg)} strata each) over {args.steps} "
+              f"steps of ~{per_step:.0f} s")
+    line = {
+        "impl": "reference", "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_name(args, cfg)},
+        "cpu_baseline": {"value": value, "unit": "Mpaths/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "Rust reference not buildable on this machine (no cargo/rustc); timed its C++ f64 restatement "
+                "(oracle/, the reference's per-row SmallRng estimator) with OpenMP over rows",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------------------ our arm
+def run_ours(args):
+    import torch
+
+    import luminara_b200 as L
+
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world_size > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def allmax(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    world, cfg = workload(args, rank)
+    t0 = time.perf_counter()
+    sc = L.GpuScene(world)
+    build_s = time.perf_counter() - t0
+    info = sc.info()
+    H, Wd = cfg.out_shape()[:2]
+    paths_per_step = H * Wd * strata(cfg)
+    out = torch.empty((H, Wd, 3), dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")   # > 126 MB L2
+    stream = torch.cuda.current_stream()
+
+    counts = sc.count_tests(cfg)                   # counter build, same seeds (not timed)
+    for _ in range(args.warmup):
+        sc.render_device(cfg, out.data_ptr(), stream.cuda_stream)
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    kernel_ms, segs, shadows = [], 0, 0
+    ev0.record(stream)
+    for _ in range(args.steps):
+        flush.zero_()
+        st = sc.render_device(cfg, out.data_ptr(), stream.cuda_stream)
+        kernel_ms.append(st.kernel_ms)
+        segs += st.segments
+        shadows += st.shadow_rays
+        assert st.error_flags == 0
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clock_info = clocks.stop()
+    region_s = allmax(ev0.elapsed_time(ev1) / 1e3)
+    value = world_size * paths_per_step * args.steps / region_s / 1e6
+    avg_kernel_s = statistics.mean(kernel_ms) / 1e3
+
+    # roofline of the dominant kernel (k_render) from the counted tests of one launch
+    flops = sum(getattr(counts, k) * c[0] for k, c in COST.items())
+    nbytes = sum(getattr(counts, k) * c[1] for k, c in COST.items())
+    hbm_peak, sm_max_mhz, peak_kind = measured_peaks()
+    props = torch.cuda.get_device_properties(dev)
+    fp32_peak_tflops = props.multi_processor_count * 128 * 2 * sm_max_mhz * 1e6 / 1e12
+    ach_gbs = nbytes / avg_kernel_s / 1e9
+    ach_tflops = flops / avg_kernel_s / 1e12
+    frac_b, frac_f = ach_gbs / hbm_peak, ach_tflops / fp32_peak_tflops
+    traffic = ncu_traffic("k_render", args.config) if (not args.width and not args.spp) else None
+    roof = {
+        "kernel": "k_render",
+        "bound": "hbm" if frac_b >= frac_f else "fp32",
+        "achieved": ach_gbs if frac_b >= frac_f else ach_tflops,
+        "peak": hbm_peak if frac_b >= frac_f else fp32_peak_tflops,
+        "unit": "GB/s" if frac_b >= frac_f else "TFLOP/s",
+        "frac": max(frac_b, frac_f),
+        "traffic": traffic,
+        "peak_kind": (f"HBM {peak_kind} (MEASURED_PEAKS.json)" if frac_b >= frac_f else
+                      "FP32 nominal: SMs x 128 lanes x 2 x max SM clock (no measured FP32 peak available)"),
+        "bytes_per_launch": nbytes, "flops_per_launch": flops,
+        "hbm": {"achieved_gbs": ach_gbs, "peak_gbs": hbm_peak, "frac": frac_b, "of": peak_kind},
+        "fp32": {"achieved_tflops": ach_tflops, "peak_tflops": fp32_peak_tflops, "frac": frac_f, "of": "nominal"},
+        "avg_launch_ms": avg_kernel_s * 1e3,
+        "counts_per_launch": {k: int(getattr(counts, k)) for k in
+                              ("node_visits", "sphere_tests", "quad_tests", "triangle_tests", "disk_tests",
+                               "fog_tests", "plane_tests", "segments", "shadow_rays", "paths")},
+    }
+
+    # end to end through the public C ABI with host buffers: scene upload + render + readback
+    e2e = None
+    if not args.no_e2e:
+        def e2e_step():
+            s2 = L.GpuScene(world)
+            img, st2 = s2.render(cfg)
+            s2.close()
+            return img, st2
+
+        e2e_step()
+        barrier()
+        t1 = time.perf_counter()
+        for _ in range(args.steps):
+            img, st2 = e2e_step()
+        torch.cuda.synchronize()
+        e2e_s = allmax(time.perf_counter() - t1)
+        barrier()
+        e2e = {"value": world_size * paths_per_step * args.steps / e2e_s / 1e6, "unit": "Mpaths/s",
+               "h2d_bytes_per_step": int(info["device_bytes"]), "d2h_bytes_per_step": int(H * Wd * 3 * 4),
+               "path": "lum_scene_create (flatten + BVH + H2D) + lum_render (render + D2H) + lum_scene_destroy"}
+
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        p, s, rows, threads = cpu_sample(world, cfg, args.cpu_seconds)
+        cpu = {"value": p / s / 1e6, "unit": "Mpaths/s", "cores": threads, "kind": "port",
+               "sample": f"{rows} evenly spaced rows of the same frame ({rows * Wd * strata(cfg)} paths, {s:.1f} s), "
+                         f"reference estimator restated in C++ f64 (oracle/, stream RNG), OpenMP over rows"}
+
+    if rank == 0:
+        line = {
+            "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": world_size, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": region_s * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+            "config": {"workload": workload_name(args, cfg), "width": cfg.width, "height": cfg.height,
+                       "spp": strata(cfg), "max_depth": cfg.max_depth, "paths_per_step_per_gpu": paths_per_step,
+                       "prims": info["prims"], "bvh_nodes": info["nodes"], "scene_build_s": build_s,
+                       "l2": "L2 flushed before every timed step (256 MiB device write inside the timed region)",
+                       "parallelism": "one independent frame per GPU (seed offset by rank), no data-path collective"},
+            "mrays_per_s": world_size * (segs + shadows) / region_s / 1e6,
+            "segments_per_path": segs / (paths_per_step * args.steps),
+            "shadow_rays_per_path": shadows / (paths_per_step * args.steps),
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps,
+            "clocks": clock_info,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    sc.close()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

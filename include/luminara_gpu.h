@@ -262,6 +262,21 @@ typedef struct lum_hit {
     int32_t reserved;
 } lum_hit;
 
+/* Test counts of one render from the counter build of the render kernel (same seeds, same
+ * paths); used to turn kernel time into achieved flops/bytes of the counted tests. */
+typedef struct lum_test_counts {
+    uint64_t node_visits;     /* BVH node visits; each visit slab-tests two child boxes */
+    uint64_t sphere_tests;
+    uint64_t quad_tests;
+    uint64_t triangle_tests;
+    uint64_t disk_tests;
+    uint64_t fog_tests;
+    uint64_t plane_tests;
+    uint64_t segments;
+    uint64_t shadow_rays;
+    uint64_t paths;
+} lum_test_counts;
+
 typedef struct lum_scene lum_scene; /* opaque */
 
 /* ------------------------------------------------------------------------------------
@@ -296,6 +311,11 @@ lum_status lum_render(lum_scene* scene, const lum_render_params* params, float* 
  * (cudaStream_t passed as void*, NULL = the scene's stream); no host copies. */
 lum_status lum_render_device(lum_scene* scene, const lum_render_params* params,
                              float* d_out_rgb, void* stream, lum_stats* stats);
+
+/* Diagnostics: runs the counter build of the render kernel for `params` (output discarded)
+ * and returns its test counts.  No counterpart in the reference, which counts only paths
+ * (src/render.rs:1704). */
+lum_status lum_count_tests(lum_scene* scene, const lum_render_params* params, lum_test_counts* counts);
 
 /* Replaces SceneWorld::hit (src/scene.rs:816-834) for a set of rays: closest hit of each
  * ray in [tmin, tmax].  rays/hits are HOST arrays of n entries. */

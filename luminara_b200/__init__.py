@@ -1,0 +1,177 @@
+"""luminara_b200 -- B200 path-tracing core of the Luminara renderer.
+
+The product is ``libluminara_b200.so`` (CUDA sm_100a kernels + C++ host library) behind the
+C ABI in ``include/luminara_gpu.h``.  This package binds that ABI with ctypes and mirrors
+the reference's Rust entry point ``render(config, camera, world, lights) -> RenderResult``
+(src/render.rs:1557-1562) for Python callers.  There is no CPU fallback: if the shared
+library is missing or no CUDA device is visible, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import time
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import abi
+from .scene import (  # noqa: F401  (re-exported reference names)
+    CameraConfig, Checker, ConstantMedium, Dielectric, Disk, Emissive, Isotropic, Lambertian, LightInfo, Mesh,
+    Metal, Microfacet, MovingSphere, Plane, Quad, RenderConfig, RotateX, RotateY, RotateZ, Scale, SolidColor,
+    Sphere, Translate, Triangle, World, XyRect, XzRect, YzRect, make_box,
+)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libluminara_b200.so")
+CSRC = os.path.join(HERE, "csrc")
+
+
+class LuminaraError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"luminara status {status}: {message}")
+        self.status = status
+
+
+def build(force: bool = False) -> str:
+    """Compiles libluminara_b200.so for sm_100a with the committed Makefile."""
+    if force:
+        subprocess.run(["make", "-s", "-C", CSRC, "clean"], check=True)
+    subprocess.run(["make", "-s", "-C", CSRC], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    """Loads the shared library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing; build it with luminara_b200.build() or `make -C {CSRC}`")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    L.lum_abi_version.restype = C.c_int32
+    L.lum_last_error.restype = C.c_char_p
+    L.lum_scene_create.argtypes = [C.POINTER(abi.LumSceneDesc), C.POINTER(vp)]
+    L.lum_scene_destroy.argtypes = [vp]
+    L.lum_scene_info.argtypes = [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                 C.POINTER(C.c_uint64)]
+    L.lum_render.argtypes = [vp, C.POINTER(abi.LumRenderParams), vp, C.POINTER(abi.LumStats)]
+    L.lum_render_device.argtypes = [vp, C.POINTER(abi.LumRenderParams), vp, vp, C.POINTER(abi.LumStats)]
+    L.lum_count_tests.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.POINTER(abi.LumTestCounts)]
+    L.lum_intersect.argtypes = [vp, vp, C.c_uint32, vp]
+    L.lum_occluded.argtypes = [vp, vp, C.c_uint32, vp]
+    for name in ("lum_scene_create", "lum_scene_destroy", "lum_scene_info", "lum_render", "lum_render_device",
+                 "lum_count_tests", "lum_intersect", "lum_occluded"):
+        getattr(L, name).restype = C.c_int32
+    if L.lum_abi_version() != abi.LUM_ABI_VERSION:
+        raise ImportError("libluminara_b200.so ABI version mismatch")
+    _lib = L
+    return L
+
+
+def check(status: int) -> None:
+    if status != abi.LUM_OK:
+        raise LuminaraError(status, lib().lum_last_error().decode(errors="replace"))
+
+
+class GpuScene:
+    """A scene uploaded to the device (lum_scene_create)."""
+
+    def __init__(self, world: World):
+        self.desc = world.desc()
+        h = C.c_void_p()
+        check(lib().lum_scene_create(self.desc.ref(), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().lum_scene_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def info(self):
+        n_p, n_n, n_l = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        nb = C.c_uint64()
+        check(lib().lum_scene_info(self.h, C.byref(n_p), C.byref(n_n), C.byref(n_l), C.byref(nb)))
+        return {"prims": n_p.value, "nodes": n_n.value, "lights": n_l.value, "device_bytes": nb.value}
+
+    def render(self, cfg: RenderConfig, out: Optional[np.ndarray] = None):
+        """Renders into a host float32 array (H, W, 3); returns (image, lum_stats)."""
+        p = cfg.to_c()
+        shape = cfg.out_shape()
+        if out is None:
+            out = np.empty(shape, dtype=np.float32)
+        assert out.dtype == np.float32 and out.flags.c_contiguous and out.shape == shape
+        st = abi.LumStats()
+        check(lib().lum_render(self.h, C.byref(p), out.ctypes.data, C.byref(st)))
+        return out, st
+
+    def render_device(self, cfg: RenderConfig, d_out: int, stream: int = 0):
+        """Renders into a caller-owned device buffer (pointer as int) on `stream`."""
+        p = cfg.to_c()
+        st = abi.LumStats()
+        check(lib().lum_render_device(self.h, C.byref(p), C.c_void_p(d_out), C.c_void_p(stream), C.byref(st)))
+        return st
+
+    def count_tests(self, cfg: RenderConfig) -> abi.LumTestCounts:
+        """Node/primitive test counts of this render (counter build of the render kernel)."""
+        p = cfg.to_c()
+        c = abi.LumTestCounts()
+        check(lib().lum_count_tests(self.h, C.byref(p), C.byref(c)))
+        return c
+
+    def intersect(self, rays: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, dtype=abi.ray_dtype())
+        hits = np.zeros(rays.shape[0], dtype=abi.hit_dtype())
+        check(lib().lum_intersect(self.h, rays.ctypes.data, rays.shape[0], hits.ctypes.data))
+        return hits
+
+    def occluded(self, rays: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, dtype=abi.ray_dtype())
+        occ = np.zeros(rays.shape[0], dtype=np.int32)
+        check(lib().lum_occluded(self.h, rays.ctypes.data, rays.shape[0], occ.ctypes.data))
+        return occ
+
+
+@dataclass
+class RenderResult:
+    """src/render.rs:1540-1554 (the HDR part: linear f32 RGB with exposure applied)."""
+    hdr_data: np.ndarray
+    total_rays: int
+    render_time_secs: float
+    stats: abi.LumStats
+
+
+def render(config: RenderConfig, camera: CameraConfig, world: World, lights=None) -> RenderResult:
+    """Drop-in for render::render (src/render.rs:1557): uploads the scene, renders on the
+    GPU, returns the f32 linear image.  `lights` replaces world.lights when given."""
+    t0 = time.perf_counter()
+    world.camera = camera
+    if lights is not None:
+        world.lights = list(lights)
+    sc = GpuScene(world)
+    try:
+        img, st = sc.render(config)
+    finally:
+        sc.close()
+    return RenderResult(img, int(st.paths), time.perf_counter() - t0, st)
+
+
+def make_rays(org, dir, tmin=0.001, tmax=np.inf, time_=0.0) -> np.ndarray:
+    org = np.atleast_2d(np.asarray(org, dtype=np.float32))
+    dir = np.atleast_2d(np.asarray(dir, dtype=np.float32))
+    n = max(org.shape[0], dir.shape[0])
+    r = np.zeros(n, dtype=abi.ray_dtype())
+    r["org"] = org
+    r["dir"] = dir
+    r["tmin"] = tmin
+    r["tmax"] = tmax
+    r["time"] = time_
+    return r

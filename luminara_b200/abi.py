@@ -224,6 +224,12 @@ class LumHit(C.Structure):
     ]
 
 
+class LumTestCounts(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("node_visits", "sphere_tests", "quad_tests", "triangle_tests",
+                                          "disk_tests", "fog_tests", "plane_tests", "segments", "shadow_rays",
+                                          "paths")]
+
+
 # numpy dtypes of the ray/hit records (for bulk arrays)
 def ray_dtype():
     import numpy as np
@@ -262,4 +268,5 @@ STRUCT_SIZES = {
     "lum_stats": C.sizeof(LumStats),
     "lum_ray": C.sizeof(LumRay),
     "lum_hit": C.sizeof(LumHit),
+    "lum_test_counts": C.sizeof(LumTestCounts),
 }

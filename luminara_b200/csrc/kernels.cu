@@ -1,0 +1,248 @@
+// kernels.cu -- CUDA kernels of the path-tracing core and their launchers (sm_100a).
+//
+//   k_render      the single-scene megakernel (camera -> closest hit -> scatter/NEE/RR ->
+//                 per-pixel accumulation), replacing render.rs:1598-1706 + ray_color.
+//   k_intersect   closest hit of a ray set (SceneWorld::hit, scene.rs:816-834).
+//   k_occluded    any hit of a ray set (the NEE shadow query, render.rs:1457-1460).
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+#include "tracer.cuh"
+
+namespace lum {
+
+constexpr int kRenderThreads = 128;
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ void flush_counters(WorkCounters* wc, uint32_t err, uint32_t nseg, uint32_t nsh) {
+    unsigned long long s = nseg, h = nsh;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_xor_sync(kFull, s, o);
+        h += __shfl_xor_sync(kFull, h, o);
+        err |= __shfl_xor_sync(kFull, err, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&wc->segments, s);
+        atomicAdd(&wc->shadow_rays, h);
+        if (err) atomicOr(&wc->error_flags, err);
+    }
+}
+
+// Persistent megakernel.  Each warp takes 8x4 pixel tiles from a global counter; each lane
+// owns one pixel and walks its strata [s_begin, s_end), starting a new path as soon as the
+// previous one ends (path regeneration keeps lanes busy).  The per-pixel sum is taken in a
+// fixed order, so the image does not depend on scheduling.
+// COUNT = true is the counter build: same paths, plus node/primitive test tallies.
+template <bool COUNT>
+__global__ void __launch_bounds__(kRenderThreads) k_render(SceneDev S, RenderDev R, float* __restrict__ out,
+                                                           WorkCounters* wc) {
+    extern __shared__ int s_stack[];
+    int* stack = s_stack + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    uint32_t err = 0, nseg = 0, nsh = 0;
+    TestTally tally{};
+    for (;;) {
+        uint32_t task = 0;
+        if (lane == 0) task = atomicAdd(&wc->next_task, 1u);
+        task = __shfl_sync(kFull, task, 0);
+        if (task >= R.n_tasks) break;
+        const uint32_t i = (task % R.tiles_x) * 8 + (lane & 7);
+        const uint32_t j = (task / R.tiles_x) * 4 + (lane >> 3);
+        const bool valid = i < R.w && j < R.h;
+        const uint32_t gi = i + R.crop_x, gj = j + R.crop_y;
+        const uint32_t pixel = gj * R.full_w + gi;
+        V acc = mk(0.f, 0.f, 0.f);
+        float wsum = 0.0f;
+        uint32_t st = R.s_begin;
+        bool active = false;
+        Path P;
+        for (;;) {
+            if (!active && valid && st < R.s_end) {
+                start_path(S, R, gi, gj, pixel, st, P);
+                ++st;
+                active = true;
+            }
+            if (!__any_sync(kFull, active)) break;
+            if (active && path_bounce<COUNT>(S, R, pixel, P, stack, err, nseg, nsh, &tally)) {
+                // luminance clamp and filter weight (render.rs:1692-1701)
+                float lum = 0.2126f * P.L.x + 0.7152f * P.L.y + 0.0722f * P.L.z;
+                V cl = lum > 100.0f ? P.L * (100.0f / lum) : P.L;
+                float w = filter_weight(R.pixel_filter, P.jx - 0.5f, P.jy - 0.5f);
+                acc = fma3(cl, w, acc);
+                wsum += w;
+                active = false;
+            }
+        }
+        if (valid) {
+            V px = wsum > 0.0f ? acc * (1.0f / wsum) : acc;                // render.rs:1705
+            float* o = out + 3 * ((size_t)j * R.w + i);
+            o[0] = px.x * R.exposure;
+            o[1] = px.y * R.exposure;
+            o[2] = px.z * R.exposure;
+        }
+    }
+    flush_counters(wc, err, nseg, nsh);
+    if constexpr (COUNT) {
+        atomicAdd(&wc->tally.node, tally.node);
+        for (int k = 0; k < 6; ++k) atomicAdd(&wc->tally.prim[k], tally.prim[k]);
+        atomicAdd(&wc->tally.plane, tally.plane);
+    }
+}
+
+// u, v of a hit as the reference's HitRecord carries them (uv per primitive type).
+__device__ void hit_uv(const SceneDev& S, const Ray& ray, const Hit& h, const Surface& sf, float& u, float& v) {
+    u = v = 0.0f;
+    if (h.prim <= -2) {                                                // plane.rs:60-62
+        const PlaneDev& P = S.planes[-2 - h.prim];
+        V local = sf.p - mk(P.p);
+        float a = dot(local, mk(P.ua)), b = dot(local, mk(P.va));
+        u = fabsf(a - truncf(a));
+        v = fabsf(b - truncf(b));
+        return;
+    }
+    int type = __ldg(S.meta + h.prim) & 15;
+    float4 a = ldp(S, h.prim, 0);
+    if (type == PT_SPHERE) {                                           // sphere.rs:48-52
+        float4 b = ldp(S, h.prim, 1);
+        V c = xyz(a);
+        if (b.w != 0.0f) c = fma3(xyz(b) - c, ray.time, c);
+        V on = (sf.p - c) * (1.0f / a.w);
+        float theta = acosf(fminf(fmaxf(-on.y, -1.0f), 1.0f));
+        float phi = atan2f(-on.z, on.x) + CUDART_PI_F;
+        u = phi / (2.0f * CUDART_PI_F);
+        v = theta / CUDART_PI_F;
+    } else if (type == PT_QUAD) {
+        float t, uv[2];
+        if (hit_quad(a, ldp(S, h.prim, 1), ldp(S, h.prim, 2), ldp(S, h.prim, 3), ray, -CUDART_INF_F, CUDART_INF_F, t, uv)) {
+            u = uv[0];
+            v = uv[1];
+        }
+    } else if (type == PT_TRIANGLE) {
+        u = h.b1;
+        v = h.b2;
+    } else if (type == PT_DISK) {                                      // disk.rs:38-41
+        V off = sf.p - xyz(a);
+        u = atan2f(off.z, off.x) / (2.0f * CUDART_PI_F) + 0.5f;
+        v = sqrtf(len2(off)) / a.w;
+    }
+}
+
+__global__ void __launch_bounds__(kRenderThreads) k_intersect(SceneDev S, const lum_ray* __restrict__ rays, uint32_t n,
+                                                              lum_hit* __restrict__ hits, WorkCounters* wc) {
+    extern __shared__ int s_stack[];
+    int* stack = s_stack + threadIdx.x;
+    uint32_t err = 0;
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+        lum_ray r = rays[idx];
+        Ray ray{mk(r.org), mk(r.dir), r.time};
+        Hit h;
+        h.t = r.tmax;
+        h.prim = -1;
+        h.b1 = h.b2 = 0.0f;
+        lum_hit out;
+        out.reserved = 0;
+        if (traverse<false>(S, ray, r.tmin, h, stack, err)) {
+            Surface sf = surface_of(S, ray, h);
+            out.t = h.t;
+            hit_uv(S, ray, h, sf, out.u, out.v);
+            out.normal[0] = sf.n.x;
+            out.normal[1] = sf.n.y;
+            out.normal[2] = sf.n.z;
+            out.prim_id = h.prim <= -2 ? S.planes[-2 - h.prim].orig_id : __ldg(S.orig + h.prim);
+            out.front_face = sf.front ? 1 : 0;
+            out.material = sf.mat;
+        } else {
+            out.t = r.tmax;
+            out.u = out.v = 0.0f;
+            out.normal[0] = out.normal[1] = out.normal[2] = 0.0f;
+            out.prim_id = -1;
+            out.front_face = 0;
+            out.material = -1;
+        }
+        hits[idx] = out;
+    }
+    if (err) atomicOr(&wc->error_flags, err);
+}
+
+__global__ void __launch_bounds__(kRenderThreads) k_occluded(SceneDev S, const lum_ray* __restrict__ rays, uint32_t n,
+                                                             int32_t* __restrict__ occ, WorkCounters* wc) {
+    extern __shared__ int s_stack[];
+    int* stack = s_stack + threadIdx.x;
+    uint32_t err = 0;
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+        lum_ray r = rays[idx];
+        Ray ray{mk(r.org), mk(r.dir), r.time};
+        Hit h;
+        h.t = r.tmax;
+        h.prim = -1;
+        occ[idx] = traverse<true>(S, ray, r.tmin, h, stack, err) ? 1 : 0;
+    }
+    if (err) atomicOr(&wc->error_flags, err);
+}
+
+// ------------------------------------------------------------------------------ launchers
+static int g_num_sms = 0;
+
+static int num_sms() {
+    if (g_num_sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+        if (g_num_sms <= 0) g_num_sms = 148;
+    }
+    return g_num_sms;
+}
+
+static size_t stack_bytes(int threads) { return (size_t)kStackDepth * threads * sizeof(int); }
+
+template <bool COUNT>
+static cudaError_t launch_render_t(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
+                                   cudaStream_t stream, int blocks_per_sm) {
+    static int occ = -1;
+    if (occ < 0) {
+        cudaFuncSetAttribute(k_render<COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)stack_bytes(kRenderThreads));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_render<COUNT>, kRenderThreads,
+                                                      stack_bytes(kRenderThreads));
+        if (occ <= 0) occ = 4;
+    }
+    if (blocks_per_sm <= 0) blocks_per_sm = occ;
+    int grid = num_sms() * blocks_per_sm;
+    int blocks_needed = (int)((R.n_tasks + 3) / 4);   // 4 warps per block, one tile per warp at least
+    if (grid > blocks_needed) grid = blocks_needed > 0 ? blocks_needed : 1;
+    k_render<COUNT><<<grid, kRenderThreads, stack_bytes(kRenderThreads), stream>>>(S, R, out, wc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_render(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc, cudaStream_t stream,
+                          int blocks_per_sm) {
+    return launch_render_t<false>(S, R, out, wc, stream, blocks_per_sm);
+}
+
+cudaError_t launch_render_counted(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
+                                  cudaStream_t stream) {
+    return launch_render_t<true>(S, R, out, wc, stream, 0);
+}
+
+cudaError_t launch_intersect(const SceneDev& S, const lum_ray* rays, uint32_t n, lum_hit* hits, WorkCounters* wc,
+                             cudaStream_t stream) {
+    int grid = (int)((n + kRenderThreads - 1) / kRenderThreads);
+    int cap = num_sms() * 16;
+    if (grid > cap) grid = cap;
+    if (grid < 1) grid = 1;
+    k_intersect<<<grid, kRenderThreads, stack_bytes(kRenderThreads), stream>>>(S, rays, n, hits, wc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_occluded(const SceneDev& S, const lum_ray* rays, uint32_t n, int32_t* occ, WorkCounters* wc,
+                            cudaStream_t stream) {
+    int grid = (int)((n + kRenderThreads - 1) / kRenderThreads);
+    int cap = num_sms() * 16;
+    if (grid > cap) grid = cap;
+    if (grid < 1) grid = 1;
+    k_occluded<<<grid, kRenderThreads, stack_bytes(kRenderThreads), stream>>>(S, rays, n, occ, wc);
+    return cudaGetLastError();
+}
+
+}  // namespace lum

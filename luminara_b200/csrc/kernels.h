@@ -1,0 +1,22 @@
+// kernels.h -- host-side declarations of the kernel launchers (internal to the library).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "device_scene.h"
+
+namespace lum {
+
+// Launches the megakernel on `stream`.  `wc` must be zeroed beforehand.  blocks_per_sm <= 0
+// picks the occupancy limit.
+cudaError_t launch_render(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc, cudaStream_t stream,
+                          int blocks_per_sm);
+// Counter build of the megakernel: same image, plus node/primitive test tallies in wc->tally.
+cudaError_t launch_render_counted(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
+                                  cudaStream_t stream);
+cudaError_t launch_intersect(const SceneDev& S, const lum_ray* rays, uint32_t n, lum_hit* hits, WorkCounters* wc,
+                             cudaStream_t stream);
+cudaError_t launch_occluded(const SceneDev& S, const lum_ray* rays, uint32_t n, int32_t* occ, WorkCounters* wc,
+                            cudaStream_t stream);
+
+}  // namespace lum

@@ -1,0 +1,766 @@
+// tracer.cuh -- device code of the path-tracing core (sm_100a).
+//
+// Restates the reference's hot path in f32 on the GPU:
+//   primitive hits   src/sphere.rs:23-62, quad.rs:29-62, triangle.rs:21-64, obj.rs:259-313,
+//                    disk.rs:31-58, plane.rs:42-69, constant_medium.rs:25-69, hit.rs:19-43
+//   traversal        src/bvh.rs:52-68 + src/scene.rs:816-834 (closest hit: BVH then planes)
+//   materials        src/material.rs:59-391, constant_medium.rs:81-89, texture.rs:9-50
+//   NEE              src/render.rs:1333-1466
+//   integrator       src/render.rs:1472-1537 (iterative form, see path_bounce)
+//   camera           src/camera.rs:82-102
+// Random numbers come from Philox4x32-10 keyed by (pixel, stratum, bounce, call).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math_constants.h>
+#include <stdint.h>
+
+#include "device_scene.h"
+
+namespace lum {
+
+// ------------------------------------------------------------------------------- vectors
+struct V {
+    float x, y, z;
+};
+__device__ __forceinline__ V mk(float x, float y, float z) { return V{x, y, z}; }
+__device__ __forceinline__ V mk(const float* p) { return V{p[0], p[1], p[2]}; }
+__device__ __forceinline__ V operator+(V a, V b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ V operator-(V a, V b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ V operator-(V a) { return {-a.x, -a.y, -a.z}; }
+__device__ __forceinline__ V operator*(V a, float t) { return {a.x * t, a.y * t, a.z * t}; }
+__device__ __forceinline__ V operator*(float t, V a) { return a * t; }
+__device__ __forceinline__ V mul(V a, V b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+__device__ __forceinline__ float dot(V a, V b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
+__device__ __forceinline__ V cross(V a, V b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ float len2(V a) { return dot(a, a); }
+__device__ __forceinline__ V unit(V a) { return a * rsqrtf(len2(a)); }
+__device__ __forceinline__ V fma3(V a, float t, V b) { return {fmaf(a.x, t, b.x), fmaf(a.y, t, b.y), fmaf(a.z, t, b.z)}; }
+__device__ __forceinline__ V xyz(float4 a) { return {a.x, a.y, a.z}; }
+__device__ __forceinline__ bool near_zero(V a) {
+    return fabsf(a.x) < 1e-8f && fabsf(a.y) < 1e-8f && fabsf(a.z) < 1e-8f;
+}
+__device__ __forceinline__ V reflect(V v, V n) { return v - n * (2.0f * dot(v, n)); }
+__device__ __forceinline__ bool has_nan(V a) { return isnan(a.x) || isnan(a.y) || isnan(a.z); }
+
+// -------------------------------------------------------------------------------- RNG
+// Philox4x32-10 (Salmon et al., SC'11).
+__device__ __forceinline__ uint4 philox(uint4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        if (r > 0) {
+            k0 += 0x9E3779B9u;
+            k1 += 0xBB67AE85u;
+        }
+        uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+        uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+        c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+    }
+    return c;
+}
+__device__ __forceinline__ float u24(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
+__device__ __forceinline__ float4 draw4(uint32_t k0, uint32_t k1, uint32_t pixel, uint32_t stratum, uint32_t bounce,
+                                        uint32_t call) {
+    uint4 o = philox(make_uint4(pixel, stratum, bounce, call), k0, k1);
+    return make_float4(u24(o.x), u24(o.y), u24(o.z), u24(o.w));
+}
+enum : uint32_t { CALL_CAMERA = 0, CALL_CAMERA2 = 1, CALL_SCATTER = 2, CALL_NEE = 3, CALL_EXTRA = 4 };
+
+// Direct (rejection-free) samplers; same distributions as src/vec3.rs:96-122.
+__device__ __forceinline__ V unit_vector(float a, float b) {
+    float z = 1.0f - 2.0f * a;
+    float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+    float s, c;
+    sincospif(2.0f * b, &s, &c);
+    return {r * c, r * s, z};
+}
+__device__ __forceinline__ V in_unit_sphere(float a, float b, float c) { return unit_vector(a, b) * cbrtf(c); }
+
+// ------------------------------------------------------------------------------ ray/hit
+struct Ray {
+    V o, d;
+    float time;
+};
+
+struct Hit {
+    float t;
+    int prim;     // index into the reordered primitive array; -1 none; <= -2 : plane (-2 - index)
+    float b1, b2; // triangle barycentrics (u, v)
+};
+
+__device__ __forceinline__ float4 ldp(const SceneDev& S, int i, int k) {
+    return __ldg(reinterpret_cast<const float4*>(S.prims) + 4 * i + k);
+}
+
+// Robust sphere roots (Haines et al., "Precision Improvements for Ray/Sphere Intersection",
+// Ray Tracing Gems 2019): discriminant from the ray-to-centre distance, near root from c/q.
+__device__ __forceinline__ bool sphere_roots(V c, float r, const Ray& ray, float& t0, float& t1) {
+    V oc = ray.o - c;
+    float a = len2(ray.d);
+    float b = dot(oc, ray.d);
+    V f = fma3(ray.d, -b / a, oc);
+    float disc = a * (r * r - len2(f));
+    if (disc < 0.0f) return false;
+    float cc = fmaf(-r, r, len2(oc));
+    float q = -b - copysignf(sqrtf(disc), b);
+    float ta = cc / q, tb = q / a;
+    if (q == 0.0f) ta = tb = -b / a;
+    t0 = fminf(ta, tb);
+    t1 = fmaxf(ta, tb);
+    return true;
+}
+
+// sphere.rs:24-45: near root if in [tmin, tmax], else far root.
+__device__ __forceinline__ bool hit_sphere(float4 a, float4 b, const Ray& ray, float tmin, float tmax, float& t) {
+    V c = xyz(a);
+    if (b.w != 0.0f) c = fma3(xyz(b) - c, ray.time, c);   // MovingSphere::center_at
+    float t0, t1;
+    if (!sphere_roots(c, a.w, ray, t0, t1)) return false;
+    if (t0 >= tmin && t0 <= tmax) { t = t0; return true; }
+    if (t1 >= tmin && t1 <= tmax) { t = t1; return true; }
+    return false;
+}
+
+// quad.rs:29-62.  The record keeps w = (u x v)/|u x v|^2 and |u x v|, so the plane test,
+// the parallel threshold on the unit normal and the planar coordinates are the reference's.
+__device__ __forceinline__ bool hit_quad(float4 a, float4 b, float4 c, float4 d, const Ray& ray, float tmin,
+                                         float tmax, float& t, float* uv = nullptr) {
+    V w = xyz(d);
+    float denom = dot(w, ray.d);
+    if (fabsf(denom * b.w) < 1e-8f) return false;
+    float tt = (a.w - dot(w, ray.o)) / denom;
+    if (!(tt >= tmin && tt <= tmax)) return false;
+    V p = fma3(ray.d, tt, ray.o);
+    V ph = p - xyz(a);
+    float alpha = dot(w, cross(ph, xyz(c)));
+    float beta = dot(w, cross(xyz(b), ph));
+    if (!(alpha >= 0.0f && alpha <= 1.0f && beta >= 0.0f && beta <= 1.0f)) return false;
+    t = tt;
+    if (uv) { uv[0] = alpha; uv[1] = beta; }
+    return true;
+}
+
+// triangle.rs:21-64 (Moller-Trumbore)
+__device__ __forceinline__ bool hit_tri(float4 a, float4 b, float4 c, const Ray& ray, float tmin, float tmax,
+                                        float& t, float& bu, float& bv) {
+    V e1 = xyz(b), e2 = xyz(c);
+    V h = cross(ray.d, e2);
+    float aa = dot(e1, h);
+    if (fabsf(aa) < 1e-8f) return false;
+    float f = 1.0f / aa;
+    V s = ray.o - xyz(a);
+    float u = f * dot(s, h);
+    if (!(u >= 0.0f && u <= 1.0f)) return false;
+    V q = cross(s, e1);
+    float v = f * dot(ray.d, q);
+    if (v < 0.0f || u + v > 1.0f) return false;
+    float tt = f * dot(e2, q);
+    if (!(tt >= tmin && tt <= tmax)) return false;
+    t = tt;
+    bu = u;
+    bv = v;
+    return true;
+}
+
+// disk.rs:31-58
+__device__ __forceinline__ bool hit_disk(float4 a, float4 b, const Ray& ray, float tmin, float tmax, float& t) {
+    V n = xyz(b);
+    float denom = dot(n, ray.d);
+    if (fabsf(denom) < 1e-8f) return false;
+    float tt = dot(xyz(a) - ray.o, n) / denom;
+    if (!(tt >= tmin && tt <= tmax)) return false;
+    V off = fma3(ray.d, tt, ray.o) - xyz(a);
+    if (len2(off) > a.w * a.w) return false;
+    t = tt;
+    return true;
+}
+
+// constant_medium.rs:25-69.  Boundary entry/exit over the whole line (t_min = -inf), the
+// second hit at least 1e-4 past the first; the free-flight distance is the reference's
+// deterministic hash of the ray, evaluated in f64 without contraction.
+__device__ __forceinline__ bool hit_fog(int type, float4 a, float4 b, float4 c, const Ray& ray, float tmin,
+                                        float tmax, float& t) {
+    float e0, e1;
+    if (type == PT_FOG_SPHERE) {
+        if (!sphere_roots(xyz(a), a.w, ray, e0, e1)) return false;
+    } else {
+        float lo = -CUDART_INF_F, hi = CUDART_INF_F;
+        float o[3] = {ray.o.x, ray.o.y, ray.o.z}, d[3] = {ray.d.x, ray.d.y, ray.d.z};
+        float mn[3] = {a.x, a.y, a.z}, mx[3] = {b.x, b.y, b.z};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            float inv = 1.0f / d[k];
+            float ta = (mn[k] - o[k]) * inv, tb = (mx[k] - o[k]) * inv;
+            lo = fmaxf(lo, fminf(ta, tb));
+            hi = fminf(hi, fmaxf(ta, tb));
+        }
+        if (!(lo <= hi)) return false;
+        e0 = lo;
+        e1 = hi;
+    }
+    if (!(e1 >= e0 + 0.0001f)) return false;
+    float t1 = fmaxf(e0, tmin), t2 = fminf(e1, tmax);
+    if (t1 >= t2) return false;
+    if (t1 < 0.0f) t1 = 0.0f;
+    float rl = sqrtf(len2(ray.d));
+    float inside = (t2 - t1) * rl;
+    double hv = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn((double)ray.o.x, 73856093.0), __dmul_rn((double)ray.o.y, 19349663.0)),
+                                    __dmul_rn((double)ray.o.z, 83492791.0)),
+                          __dmul_rn((double)ray.d.x, 47392381.0));
+    hv = fabs(hv - trunc(hv));
+    double hd = (double)c.x * log(fmax(1.0 - hv, 1e-10));
+    if (hd > (double)inside) return false;
+    t = t1 + (float)hd / rl;
+    return true;
+}
+
+// One primitive test; updates the closest hit when t is within [tmin, hit.t].
+template <bool COUNT = false>
+__device__ __forceinline__ bool test_prim(const SceneDev& S, int i, const Ray& ray, float tmin, Hit& hit,
+                                          TestTally* tl = nullptr) {
+    int type = __ldg(S.meta + i) & 15;
+    if constexpr (COUNT) tl->prim[type]++;
+    float4 a = ldp(S, i, 0);
+    float t;
+    switch (type) {
+        case PT_SPHERE: {
+            float4 b = ldp(S, i, 1);
+            if (hit_sphere(a, b, ray, tmin, hit.t, t)) { hit.t = t; hit.prim = i; return true; }
+            return false;
+        }
+        case PT_QUAD: {
+            float4 b = ldp(S, i, 1), c = ldp(S, i, 2), d = ldp(S, i, 3);
+            if (hit_quad(a, b, c, d, ray, tmin, hit.t, t)) { hit.t = t; hit.prim = i; return true; }
+            return false;
+        }
+        case PT_TRIANGLE: {
+            float4 b = ldp(S, i, 1), c = ldp(S, i, 2);
+            float bu, bv;
+            if (hit_tri(a, b, c, ray, tmin, hit.t, t, bu, bv)) {
+                hit.t = t; hit.prim = i; hit.b1 = bu; hit.b2 = bv;
+                return true;
+            }
+            return false;
+        }
+        case PT_DISK: {
+            float4 b = ldp(S, i, 1);
+            if (hit_disk(a, b, ray, tmin, hit.t, t)) { hit.t = t; hit.prim = i; return true; }
+            return false;
+        }
+        default: {
+            float4 b = ldp(S, i, 1), c = ldp(S, i, 2);
+            if (hit_fog(type, a, b, c, ray, tmin, hit.t, t)) { hit.t = t; hit.prim = i; return true; }
+            return false;
+        }
+    }
+}
+
+// plane.rs:42-69
+__device__ __forceinline__ bool hit_plane(const PlaneDev& P, const Ray& ray, float tmin, float tmax, float& t) {
+    V n = mk(P.n);
+    float denom = dot(n, ray.d);
+    if (fabsf(denom) < 1e-8f) return false;
+    float tt = dot(mk(P.p) - ray.o, n) / denom;
+    if (!(tt >= tmin && tt <= tmax)) return false;
+    t = tt;
+    return true;
+}
+
+// ------------------------------------------------------------------------------ traversal
+// Stack lives in shared memory: entry k of thread j at stack[k * blockDim.x + j].
+// ANY = true stops at the first accepted hit (shadow rays, src/render.rs:1457-1460).
+template <bool ANY, bool COUNT = false>
+__device__ __forceinline__ bool traverse(const SceneDev& S, const Ray& ray, float tmin, Hit& hit, int* stack,
+                                         uint32_t& err, TestTally* tl = nullptr) {
+    bool found = false;
+    if (S.n_nodes > 0) {
+        const float ix = 1.0f / ray.d.x, iy = 1.0f / ray.d.y, iz = 1.0f / ray.d.z;
+        const float ox = -ray.o.x * ix, oy = -ray.o.y * iy, oz = -ray.o.z * iz;
+        const float4* nodes = reinterpret_cast<const float4*>(S.nodes);
+        const int stride = blockDim.x;
+        int sp = 0;
+        int node = 0;
+        for (;;) {
+            float4 n0 = __ldg(nodes + 4 * node + 0);
+            float4 n1 = __ldg(nodes + 4 * node + 1);
+            float4 n2 = __ldg(nodes + 4 * node + 2);
+            int4 n3 = __ldg(reinterpret_cast<const int4*>(nodes) + 4 * node + 3);
+            if constexpr (COUNT) tl->node++;
+            // slab tests of both children (aabb.rs:18-56)
+            float a0 = fmaf(n0.x, ix, ox), a1 = fmaf(n0.y, ix, ox);
+            float b0 = fmaf(n0.z, iy, oy), b1 = fmaf(n0.w, iy, oy);
+            float c0 = fmaf(n2.x, iz, oz), c1 = fmaf(n2.y, iz, oz);
+            float en0 = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), tmin));
+            float ex0 = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), hit.t));
+            float d0 = fmaf(n1.x, ix, ox), d1 = fmaf(n1.y, ix, ox);
+            float e0 = fmaf(n1.z, iy, oy), e1 = fmaf(n1.w, iy, oy);
+            float f0 = fmaf(n2.z, iz, oz), f1 = fmaf(n2.w, iz, oz);
+            float en1 = fmaxf(fmaxf(fminf(d0, d1), fminf(e0, e1)), fmaxf(fminf(f0, f1), tmin));
+            float ex1 = fminf(fminf(fmaxf(d0, d1), fmaxf(e0, e1)), fminf(fmaxf(f0, f1), hit.t));
+            bool h0 = en0 < ex0, h1 = en1 < ex1;
+            if (h0 && n3.z > 0) {
+                for (int k = 0; k < n3.z; ++k) {
+                    if (test_prim<COUNT>(S, n3.x + k, ray, tmin, hit, tl)) {
+                        found = true;
+                        if (ANY) return true;
+                    }
+                }
+                h0 = false;
+            }
+            if (h1 && n3.w > 0) {
+                for (int k = 0; k < n3.w; ++k) {
+                    if (test_prim<COUNT>(S, n3.y + k, ray, tmin, hit, tl)) {
+                        found = true;
+                        if (ANY) return true;
+                    }
+                }
+                h1 = false;
+            }
+            if (h0 && h1) {
+                int nearc = en0 <= en1 ? n3.x : n3.y;
+                int farc = en0 <= en1 ? n3.y : n3.x;
+                if (sp < kStackDepth) {
+                    stack[sp * stride] = farc;
+                    ++sp;
+                } else {
+                    err |= LUM_KERR_STACK_OVERFLOW;
+                }
+                node = nearc;
+            } else if (h0) {
+                node = n3.x;
+            } else if (h1) {
+                node = n3.y;
+            } else {
+                if (sp == 0) break;
+                --sp;
+                node = stack[sp * stride];
+            }
+        }
+    }
+    for (int k = 0; k < S.n_planes; ++k) {                             // scene.rs:826-831
+        if constexpr (COUNT) tl->plane++;
+        float t;
+        if (hit_plane(S.planes[k], ray, tmin, hit.t, t)) {
+            hit.t = t;
+            hit.prim = -2 - k;
+            found = true;
+            if (ANY) return true;
+        }
+    }
+    return found;
+}
+
+// ---------------------------------------------------------------------------- hit details
+struct Surface {
+    V p, n;          // point, normal facing the ray
+    bool front;
+    int mat;
+};
+
+// Point, outward normal, face orientation and material of a hit (hit.rs:19-43).
+__device__ __forceinline__ Surface surface_of(const SceneDev& S, const Ray& ray, const Hit& h) {
+    Surface s;
+    s.p = fma3(ray.d, h.t, ray.o);
+    V on;
+    if (h.prim <= -2) {
+        const PlaneDev& P = S.planes[-2 - h.prim];
+        on = mk(P.n);
+        s.mat = P.material;
+    } else {
+        int meta = __ldg(S.meta + h.prim);
+        int type = meta & 15;
+        s.mat = meta >> 4;
+        float4 a = ldp(S, h.prim, 0);
+        switch (type) {
+            case PT_SPHERE: {
+                float4 b = ldp(S, h.prim, 1);
+                V c = xyz(a);
+                if (b.w != 0.0f) c = fma3(xyz(b) - c, ray.time, c);
+                on = (s.p - c) * (1.0f / a.w);
+                break;
+            }
+            case PT_QUAD: {
+                float4 d = ldp(S, h.prim, 3);
+                on = unit(xyz(d)) * d.w;
+                break;
+            }
+            case PT_TRIANGLE: {
+                float4 d = ldp(S, h.prim, 3);
+                int si = __float_as_int(d.w);
+                if (si >= 0) {
+                    const float* sn = S.smooth_n + 9 * si;
+                    float w0 = 1.0f - h.b1 - h.b2;
+                    on = unit(mk(sn) * w0 + mk(sn + 3) * h.b1 + mk(sn + 6) * h.b2);
+                } else {
+                    on = xyz(d);
+                }
+                break;
+            }
+            case PT_DISK: on = xyz(ldp(S, h.prim, 1)); break;
+            default: on = mk(1.0f, 0.0f, 0.0f); break;                 // constant_medium.rs:63
+        }
+    }
+    s.front = dot(ray.d, on) < 0.0f;
+    s.n = s.front ? on : -on;
+    return s;
+}
+
+// ------------------------------------------------------------------------------ shading
+__device__ __forceinline__ V tex_value(const MatDev& m, V p) {           // texture.rs:19-50
+    if (m.tex == 0) return mk(m.color);
+    float inv = 1.0f / m.tex_scale;
+    long long x = (long long)floorf(p.x * inv), y = (long long)floorf(p.y * inv), z = (long long)floorf(p.z * inv);
+    return ((x + y + z) % 2 == 0) ? mk(m.color) : mk(m.color2);
+}
+
+__device__ __forceinline__ V emitted(const MatDev& m, V p) {           // material.rs:241-243
+    return m.kind == 4 ? tex_value(m, p) * m.intensity : mk(0.0f, 0.0f, 0.0f);
+}
+
+__device__ __forceinline__ float schlick(float cosine, float ref_idx) { // material.rs:138-141
+    float r0 = (1.0f - ref_idx) / (1.0f + ref_idx);
+    r0 = r0 * r0;
+    float m = 1.0f - cosine;
+    float m2 = m * m;
+    return r0 + (1.0f - r0) * (m2 * m2 * m);
+}
+
+__device__ __forceinline__ V fresnel(float cos_t, V f0) {              // material.rs:291-294
+    float m = fmaxf(1.0f - cos_t, 0.0f);
+    float m2 = m * m;
+    float t = m2 * m2 * m;
+    return f0 * (1.0f - t) + mk(t, t, t);
+}
+
+// material.rs:297-319 with tan(theta) evaluated directly (same angle, no atan/sin/cos).
+__device__ __forceinline__ V ggx_normal(V n, float alpha, float r1, float r2) {
+    float tan2 = alpha * alpha * r1 / (1.0f - r1 + 1e-10f);
+    float ct = rsqrtf(1.0f + tan2);
+    float st = sqrtf(tan2) * ct;
+    float sp, cp;
+    sincospif(2.0f * r2, &sp, &cp);
+    V up = fabsf(n.y) < 0.999f ? mk(0.f, 1.f, 0.f) : mk(1.f, 0.f, 0.f);
+    V tg = unit(cross(up, n));
+    V bt = cross(n, tg);
+    return unit(tg * (st * cp) + bt * (st * sp) + n * ct);
+}
+
+struct Scatter {
+    V dir;
+    V att;
+};
+
+// Material::scatter; draws s = (s0..s3) of CALL_SCATTER, extra for dispersion.
+__device__ __forceinline__ bool scatter(const MatDev& m, const Ray& ray, const Surface& sf, float hit_t, float4 s,
+                                        const RenderDev& R, uint32_t pixel, uint32_t stratum, uint32_t bounce,
+                                        Scatter& out) {
+    switch (m.kind) {
+        case 1: {                                                      // material.rs:59-71
+            V d = sf.n + unit_vector(s.x, s.y);
+            if (near_zero(d)) d = sf.n;
+            out.dir = d;
+            out.att = tex_value(m, sf.p);
+            return true;
+        }
+        case 2: {                                                      // material.rs:94-106
+            V refl = reflect(unit(ray.d), sf.n);
+            V sc = refl + in_unit_sphere(s.x, s.y, s.z) * m.fuzz;
+            if (dot(sc, sf.n) > 0.0f) {
+                out.dir = sc;
+                out.att = mk(m.color);
+                return true;
+            }
+            return false;
+        }
+        case 3: {                                                      // material.rs:149-213
+            float ior = m.ior;
+            V chan = mk(1.f, 1.f, 1.f);
+            if (m.dispersion > 0.0f) {
+                float4 ex = draw4(R.key0, R.key1, pixel, stratum, bounce, CALL_EXTRA);
+                uint32_t ch = (uint32_t)(ex.x * 3.0f);
+                ior += ch == 0 ? -m.dispersion : (ch == 1 ? 0.0f : m.dispersion);
+                chan = ch == 0 ? mk(3.f, 0.f, 0.f) : (ch == 1 ? mk(0.f, 3.f, 0.f) : mk(0.f, 0.f, 3.f));
+            }
+            float eta = sf.front ? 1.0f / ior : ior;
+            V ud = unit(ray.d);
+            float ct = fminf(dot(-ud, sf.n), 1.0f);
+            float st = sqrtf(1.0f - ct * ct);
+            V d;
+            if (eta * st > 1.0f || schlick(ct, eta) > s.x) {
+                d = reflect(ud, sf.n);
+            } else {                                                   // vec3.rs:73-78
+                V rp = (ud + sf.n * ct) * eta;
+                d = rp + sf.n * -sqrtf(fabsf(1.0f - len2(rp)));
+            }
+            if (m.roughness > 0.0f) d = d + in_unit_sphere(s.y, s.z, s.w) * m.roughness;
+            V att;
+            if (!sf.front && !m.tint_white)
+                att = mk(__expf(-(1.0f - m.tint[0]) * hit_t), __expf(-(1.0f - m.tint[1]) * hit_t),
+                         __expf(-(1.0f - m.tint[2]) * hit_t));
+            else
+                att = mk(m.tint);
+            if (m.dispersion > 0.0f) att = mul(att, chan);
+            out.dir = d;
+            out.att = att;
+            return true;
+        }
+        case 5: {                                                      // material.rs:328-390
+            float alpha = m.roughness * m.roughness;
+            V v = unit(-ray.d);
+            V n = sf.n;
+            V alb = tex_value(m, sf.p);
+            float ndv = fmaxf(dot(n, v), 0.001f);
+            V f0 = mk(0.04f, 0.04f, 0.04f) * (1.0f - m.metallic) + alb * m.metallic;
+            V fw = fresnel(ndv, f0);
+            float sp = fminf(fmaxf((fw.x + fw.y + fw.z) * (1.0f / 3.0f), 0.1f), 0.9f);
+            if (s.x < sp) {
+                V h = ggx_normal(n, alpha, s.y, s.z);
+                V l = h * (2.0f * dot(v, h)) - v;
+                float ndl = dot(n, l);
+                if (ndl <= 0.0f) return false;
+                float ndh = fmaxf(dot(n, h), 0.0f);
+                float vdh = fmaxf(dot(v, h), 0.0f);
+                float k = (m.roughness + 1.0f) * (m.roughness + 1.0f) * 0.125f;
+                float g = (ndv / (ndv * (1.0f - k) + k)) * (ndl / (ndl * (1.0f - k) + k));
+                V f = fresnel(vdh, f0);
+                V w = ndh > 0.001f ? f * (g * vdh / (ndv * ndh)) : mk(0.f, 0.f, 0.f);
+                out.dir = l;
+                out.att = w * (1.0f / sp);
+                return true;
+            }
+            V d = n + unit_vector(s.y, s.z);
+            if (near_zero(d)) d = n;
+            V kd = (mk(1.f, 1.f, 1.f) - fw) * (1.0f - m.metallic);
+            out.dir = d;
+            out.att = mul(kd, alb) * (1.0f / (1.0f - sp));
+            return true;
+        }
+        case 6: {                                                      // constant_medium.rs:81-89
+            out.dir = in_unit_sphere(s.x, s.y, s.z);
+            out.att = mk(m.color);
+            return true;
+        }
+        default:                                                       // Emissive: no scatter
+            return false;
+    }
+}
+
+// render.rs:1333-1343 (Frisvad)
+__device__ __forceinline__ void build_onb(V n, V& a, V& b) {
+    if (n.z < -0.9999999f) {
+        a = mk(0.f, -1.f, 0.f);
+        b = mk(-1.f, 0.f, 0.f);
+        return;
+    }
+    float aa = 1.0f / (1.0f + n.z);
+    float bb = -n.x * n.y * aa;
+    a = mk(1.0f - n.x * n.x * aa, bb, -n.x);
+    b = mk(bb, 1.0f - n.y * n.y * aa, -n.y);
+}
+
+// Samples one light (render.rs:1346-1455).  Returns false when the sample contributes
+// nothing before visibility; otherwise the shadow ray and unoccluded contribution.
+__device__ __forceinline__ bool sample_light(const SceneDev& S, V hp, V normal, V albedo, float4 u, Ray& shadow,
+                                             float& shadow_tmax, V& contrib) {
+    int nl = S.n_lights;
+    int idx = min((int)(u.y * (float)nl), nl - 1);
+    const LightDev& L = S.lights[idx];
+    V lp, ln;
+    float area;
+    if (L.kind == 1) {
+        V to_c = mk(L.p0) - hp;
+        float d2c = len2(to_c);
+        if (d2c < L.radius * L.radius) return false;
+        float dc = sqrtf(d2c);
+        float stm = L.radius / dc;
+        float ctm = sqrtf(fmaxf(1.0f - stm * stm, 0.0f));
+        float ct = 1.0f - u.z * (1.0f - ctm);
+        float st = sqrtf(fmaxf(1.0f - ct * ct, 0.0f));
+        float sp, cp;
+        sincospif(2.0f * u.w, &sp, &cp);
+        V w = to_c * (1.0f / dc);
+        V a, b;
+        build_onb(w, a, b);
+        V dir = unit(a * (st * cp) + b * (st * sp) + w * ct);
+        V oc = hp - mk(L.p0);
+        float bc = dot(oc, dir);
+        float cc = len2(oc) - L.radius * L.radius;
+        float disc = bc * bc - cc;
+        float t;
+        if (disc > 0.0f) {
+            float sq = sqrtf(disc);
+            float t1 = -bc - sq;
+            t = t1 > 0.001f ? t1 : -bc + sq;
+        } else {
+            t = dc;
+        }
+        lp = fma3(dir, t, hp);
+        ln = unit(lp - mk(L.p0));
+        float solid = 2.0f * CUDART_PI_F * (1.0f - ctm);
+        area = solid * t * t / fmaxf(fabsf(dot(-dir, ln)), 0.001f);
+    } else if (L.kind == 2) {
+        lp = mk(L.p0) + mk(L.u) * u.z + mk(L.v) * u.w;
+        area = L.area;
+        ln = mk(L.n);
+    } else {
+        float r = sqrtf(u.z) * L.radius;
+        float sp, cp;
+        sincospif(2.0f * u.w, &sp, &cp);
+        V w = mk(L.n);
+        V av = fabsf(w.x) > 0.9f ? mk(0.f, 1.f, 0.f) : mk(1.f, 0.f, 0.f);
+        V ut = unit(cross(w, av));
+        V vt = cross(w, ut);
+        lp = mk(L.p0) + ut * (r * cp) + vt * (r * sp);
+        area = L.area;
+        ln = w;
+    }
+    V tl = lp - hp;
+    float d2 = len2(tl);
+    float dist = sqrtf(d2);
+    V dir = tl * (1.0f / dist);
+    float ct = dot(normal, dir);
+    if (ct <= 0.0f) return false;
+    float ctl = fabsf(dot(-dir, ln));
+    if (ctl <= 0.001f) return false;
+    shadow.o = hp;
+    shadow.d = dir;
+    shadow.time = 0.0f;                                                // Ray::new (render.rs:1457)
+    shadow_tmax = dist - 0.001f;
+    contrib = mul(mk(L.e), albedo) * (ct * ctl * area * (float)nl / (CUDART_PI_F * d2));
+    return true;
+}
+
+__device__ __forceinline__ V background(const RenderDev& R, const Ray& r) {  // render.rs:73-171
+    if (R.background == 1) return mk(R.bg_color);
+    V ud = unit(r.d);
+    float t = 0.5f * (ud.y + 1.0f);
+    if (R.background == 2) return mk(R.bg_color) * (1.0f - t) + mk(R.bg_color2) * t;
+    if (R.background == 3) {
+        V sky = mk(1.f, 1.f, 1.f) * (1.0f - t) + mk(R.bg_color2) * t;
+        float sd = dot(ud, unit(mk(R.bg_dir)));
+        if (sd > 0.9995f) return mk(R.bg_color) * R.bg_intensity;
+        if (sd > 0.995f) {
+            float glow = (sd - 0.995f) / (0.9995f - 0.995f);
+            return sky + mk(R.bg_color) * (R.bg_intensity * 0.3f * glow);
+        }
+        return sky;
+    }
+    return mk(1.f, 1.f, 1.f) * (1.0f - t) + mk(0.5f, 0.7f, 1.0f) * t;
+}
+
+__device__ __forceinline__ float mitchell_1d(float x) {                // render.rs:220-237
+    x = fabsf(x);
+    const float b = 1.0f / 3.0f, c = 1.0f / 3.0f;
+    if (x < 1.0f)
+        return ((12.f - 9.f * b - 6.f * c) * x * x * x + (-18.f + 12.f * b + 6.f * c) * x * x + (6.f - 2.f * b)) / 6.f;
+    if (x < 2.0f)
+        return ((-b - 6.f * c) * x * x * x + (6.f * b + 30.f * c) * x * x + (-12.f * b - 48.f * c) * x + (8.f * b + 24.f * c)) / 6.f;
+    return 0.0f;
+}
+__device__ __forceinline__ float filter_weight(int f, float dx, float dy) {  // render.rs:201-216
+    if (f == 1) return fmaxf(1.0f - fabsf(dx) * 2.0f, 0.0f) * fmaxf(1.0f - fabsf(dy) * 2.0f, 0.0f);
+    if (f == 2) return __expf(-(dx * dx + dy * dy) / (2.0f * 0.35f * 0.35f));
+    if (f == 3) return mitchell_1d(dx * 2.0f) * mitchell_1d(dy * 2.0f);
+    return 1.0f;
+}
+
+// ------------------------------------------------------------------------------ path state
+struct Path {
+    Ray ray;
+    V beta;        // throughput B_j
+    V L;           // accumulated radiance
+    float jx, jy;  // stratum jitter (pixel filter)
+    uint32_t stratum;
+    uint32_t bounce;
+    bool skip_emission;
+};
+
+// Camera ray of stratum st (render.rs:1683-1690, camera.rs:82-102).
+__device__ __forceinline__ void start_path(const SceneDev& S, const RenderDev& R, uint32_t gi, uint32_t gj,
+                                           uint32_t pixel, uint32_t st, Path& P) {
+    uint32_t sx = st % R.sqrt_spp, sy = st / R.sqrt_spp;
+    float4 c = draw4(R.key0, R.key1, pixel, st, 0, CALL_CAMERA);
+    float inv_n = 1.0f / (float)R.sqrt_spp;
+    P.jx = ((float)sx + c.x) * inv_n;
+    P.jy = ((float)sy + c.y) * inv_n;
+    float y = (float)(R.full_h - 1 - gj);
+    float uc = ((float)gi + P.jx) / (float)(R.full_w - 1);
+    float vc = (y + P.jy) / (float)(R.full_h - 1);
+    const CameraDev& C = S.cam;
+    V off = mk(0.f, 0.f, 0.f);
+    if (C.lens_radius > 0.0f) {
+        float r = sqrtf(c.z) * C.lens_radius, sp, cp;
+        sincospif(2.0f * c.w, &sp, &cp);
+        off = mk(C.u) * (r * cp) + mk(C.v) * (r * sp);
+    }
+    P.ray.o = mk(C.origin) + off;
+    P.ray.d = mk(C.llc) + mk(C.hor) * uc + mk(C.ver) * vc - mk(C.origin) - off;
+    P.ray.time = draw4(R.key0, R.key1, pixel, st, 0, CALL_CAMERA2).x;
+    P.beta = mk(1.f, 1.f, 1.f);
+    P.L = mk(0.f, 0.f, 0.f);
+    P.stratum = st;
+    P.bounce = 0;
+    P.skip_emission = false;
+}
+
+// One segment of the path (ray_color, render.rs:1472-1537, iterative form).
+// L = sum_j B_j (e_j + d_j), B_{j+1} = B_j att_j rrw_j; returns true when the path ended.
+template <bool COUNT = false>
+__device__ __forceinline__ bool path_bounce(const SceneDev& S, const RenderDev& R, uint32_t pixel, Path& P, int* stack,
+                                            uint32_t& err, uint32_t& n_seg, uint32_t& n_shadow,
+                                            TestTally* tl = nullptr) {
+    if (P.bounce >= R.max_depth) return true;                         // depth == 0 -> black
+    const uint32_t depth = R.max_depth - P.bounce;
+    Hit h;
+    h.t = CUDART_INF_F;
+    h.prim = -1;
+    ++n_seg;
+    if (!traverse<false, COUNT>(S, P.ray, 0.001f, h, stack, err, tl)) {
+        P.L = P.L + mul(P.beta, background(R, P.ray));
+        return true;
+    }
+    Surface sf = surface_of(S, P.ray, h);
+    const MatDev& m = S.mats[sf.mat];
+    V e = P.skip_emission ? mk(0.f, 0.f, 0.f) : emitted(m, sf.p);
+    float4 su = draw4(R.key0, R.key1, pixel, P.stratum, P.bounce, CALL_SCATTER);
+    Scatter sc;
+    if (!scatter(m, P.ray, sf, h.t, su, R, pixel, P.stratum, P.bounce, sc)) {
+        P.L = P.L + mul(P.beta, e);
+        return true;
+    }
+    float4 nu = draw4(R.key0, R.key1, pixel, P.stratum, P.bounce, CALL_NEE);
+    float surv = fminf(fmaxf(fmaxf(fmaxf(sc.att.x, sc.att.y), sc.att.z), 0.05f), 1.0f);
+    if (depth < 47 && nu.x > surv) {
+        P.L = P.L + mul(P.beta, e);
+        return true;
+    }
+    float rrw = depth < 47 ? 1.0f / surv : 1.0f;
+    bool use_nee = !m.specular && S.n_lights > 0;
+    V dl = mk(0.f, 0.f, 0.f);
+    if (use_nee) {
+        Ray shadow;
+        float stmax;
+        V contrib;
+        if (sample_light(S, sf.p, sf.n, sc.att, nu, shadow, stmax, contrib)) {
+            Hit sh;
+            sh.t = stmax;
+            sh.prim = -1;
+            ++n_shadow;
+            if (!traverse<true, COUNT>(S, shadow, 0.001f, sh, stack, err, tl)) dl = contrib;
+        }
+    }
+    V term = e + dl;
+    V nb = mul(P.beta, sc.att) * rrw;
+    if (has_nan(term) || has_nan(nb)) return true;                     // render.rs:1526-1531
+    P.L = P.L + mul(P.beta, term);
+    P.beta = nb;
+    P.skip_emission = use_nee;
+    P.ray.o = sf.p;
+    P.ray.d = sc.dir;
+    ++P.bounce;
+    return false;
+}
+
+}  // namespace lum

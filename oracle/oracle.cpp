@@ -788,7 +788,8 @@ struct Rotate : Hittable {
         }
     }
     bool hit(const Ray& r, double tmin, double tmax, HitRecord& rec) const override {
-        Ray rr{inv(r.o), inv(r.d), 0.0};
+        // RotateY builds its ray with Ray::new (time 0); RotateX/RotateZ keep the time.
+        Ray rr{inv(r.o), inv(r.d), ax == 1 ? 0.0 : r.time};
         if (!inner->hit(rr, tmin, tmax, rec)) return false;
         rec.p = fwd(rec.p);
         rec.n = fwd(rec.n);
