@@ -96,14 +96,26 @@ __device__ __forceinline__ float4 ldp(const SceneDev& S, int i, int k) {
 
 // Robust sphere roots (Haines et al., "Precision Improvements for Ray/Sphere Intersection",
 // Ray Tracing Gems 2019): discriminant from the ray-to-centre distance, near root from c/q.
+// Spheres of radius >= kBigSphere (ground spheres) evaluate o - c and |o - c|^2 - r^2 in
+// f64: in f32 that difference loses ~r * 6e-8 absolutely, which near the surface of an
+// r = 1000 sphere is a large relative error of the near root.
+constexpr float kBigSphere = 32.0f;
 __device__ __forceinline__ bool sphere_roots(V c, float r, const Ray& ray, float& t0, float& t1) {
-    V oc = ray.o - c;
+    V oc;
+    float cc;
+    if (r >= kBigSphere) {
+        double dx = (double)ray.o.x - (double)c.x, dy = (double)ray.o.y - (double)c.y, dz = (double)ray.o.z - (double)c.z;
+        oc = mk((float)dx, (float)dy, (float)dz);
+        cc = (float)fma(dx, dx, fma(dy, dy, fma(dz, dz, -(double)r * (double)r)));
+    } else {
+        oc = ray.o - c;
+        cc = fmaf(-r, r, len2(oc));
+    }
     float a = len2(ray.d);
     float b = dot(oc, ray.d);
     V f = fma3(ray.d, -b / a, oc);
     float disc = a * (r * r - len2(f));
     if (disc < 0.0f) return false;
-    float cc = fmaf(-r, r, len2(oc));
     float q = -b - copysignf(sqrtf(disc), b);
     float ta = cc / q, tb = q / a;
     if (q == 0.0f) ta = tb = -b / a;
@@ -276,7 +288,12 @@ __device__ __forceinline__ bool traverse(const SceneDev& S, const Ray& ray, floa
                                          uint32_t& err, TestTally* tl = nullptr) {
     bool found = false;
     if (S.n_nodes > 0) {
-        const float ix = 1.0f / ray.d.x, iy = 1.0f / ray.d.y, iz = 1.0f / ray.d.z;
+        // Reciprocals of direction components clamped away from zero: the FMA slab form
+        // lo*inv - o*inv would give inf - inf = NaN for an axis-parallel ray, while a finite
+        // +-1e20 keeps the ordering of the reference's (lo - o) * (1/d) (aabb.rs:23-25).
+        const float ix = 1.0f / (fabsf(ray.d.x) > 1e-20f ? ray.d.x : copysignf(1e-20f, ray.d.x));
+        const float iy = 1.0f / (fabsf(ray.d.y) > 1e-20f ? ray.d.y : copysignf(1e-20f, ray.d.y));
+        const float iz = 1.0f / (fabsf(ray.d.z) > 1e-20f ? ray.d.z : copysignf(1e-20f, ray.d.z));
         const float ox = -ray.o.x * ix, oy = -ray.o.y * iy, oz = -ray.o.z * iz;
         const float4* nodes = reinterpret_cast<const float4*>(S.nodes);
         const int stride = blockDim.x;

@@ -58,6 +58,7 @@ def lib():
         L.orc_scene_destroy.argtypes = [vp]
         L.orc_intersect.argtypes = [vp, vp, C.c_uint32, vp]
         L.orc_occluded.argtypes = [vp, vp, C.c_uint32, vp]
+        L.orc_tie_count.argtypes = [vp, vp, C.c_uint32, C.c_double, C.c_double, vp]
         L.orc_render.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.c_int, C.c_int, dp, C.POINTER(OrcStats)]
         L.orc_render_rows.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.c_int, C.c_int, C.c_uint32,
                                       C.c_uint32, dp, C.POINTER(OrcStats)]
@@ -111,6 +112,12 @@ class OracleScene:
         hits = np.zeros(rays.shape[0], dtype=ORC_HIT)
         lib().orc_intersect(self.h, rays.ctypes.data, rays.shape[0], hits.ctypes.data)
         return hits
+
+    def tie_count(self, rays: np.ndarray, rel=1e-6, abs_eps=1e-6) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, dtype=ORC_RAY)
+        c = np.zeros(rays.shape[0], dtype=np.int32)
+        lib().orc_tie_count(self.h, rays.ctypes.data, rays.shape[0], rel, abs_eps, c.ctypes.data)
+        return c
 
     def occluded(self, rays: np.ndarray) -> np.ndarray:
         rays = np.ascontiguousarray(rays, dtype=ORC_RAY)

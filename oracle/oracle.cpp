@@ -1085,6 +1085,7 @@ struct orc_scene {
     std::vector<Material> mats;
     HPtr bvh;
     std::vector<HPtr> unbounded;
+    std::vector<const Hittable*> top;   // every top-level object (tie queries)
     std::vector<Light> lights;
     std::vector<Aabb> object_boxes;
     std::vector<int> object_has_box;
@@ -1308,6 +1309,7 @@ int orc_scene_create(const lum_scene_desc* d, orc_scene** out) {
     }
     // SceneWorld::from_list: bounded objects into the BVH, unbounded into a list.
     std::vector<HPtr> bounded;
+    for (auto& o : world) s->top.push_back(o.get());
     for (auto& o : world) {
         Aabb b;
         bool hb = o->bbox(b);
@@ -1359,6 +1361,26 @@ int orc_intersect(const orc_scene* s, const orc_ray* rays, uint32_t n, orc_hit* 
             h.prim_id = -1;
             h.material = -1;
         }
+    }
+    return 0;
+}
+
+int orc_tie_count(const orc_scene* s, const orc_ray* rays, uint32_t n, double rel, double abs_eps, int32_t* counts) {
+    if (!s || (!rays && n) || (!counts && n)) return 1;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        const orc_ray& r = rays[i];
+        Ray ray{from(r.org), from(r.dir), r.time};
+        HitRecord rec;
+        counts[i] = 0;
+        if (!s->hit(ray, r.tmin, r.tmax, rec)) continue;
+        double lo = std::fmax(r.tmin, rec.t - rel * rec.t - abs_eps), hi = rec.t + rel * rec.t + abs_eps;
+        int c = 0;
+        for (const Hittable* o : s->top) {
+            HitRecord tmp;
+            if (o->hit(ray, lo, hi, tmp)) ++c;
+        }
+        counts[i] = c;
     }
     return 0;
 }

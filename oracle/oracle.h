@@ -58,6 +58,9 @@ int orc_scene_create(const lum_scene_desc* desc, orc_scene** out);
 void orc_scene_destroy(orc_scene* s);
 /* Closest hit of each ray (SceneWorld::hit).  hits[i].prim_id < 0 on a miss. */
 int orc_intersect(const orc_scene* s, const orc_ray* rays, uint32_t n, orc_hit* hits);
+/* Number of top-level objects hit within [t(1-rel)-abs_eps, t(1+rel)+abs_eps] around each
+ * ray's closest hit t (0 on a miss); > 1 marks a tie such as coplanar coincident faces. */
+int orc_tie_count(const orc_scene* s, const orc_ray* rays, uint32_t n, double rel, double abs_eps, int32_t* counts);
 /* Shadow query: occluded[i] = world.hit(ray).is_some(). */
 int orc_occluded(const orc_scene* s, const orc_ray* rays, uint32_t n, int32_t* occluded);
 /* render() non-adaptive branch; out_rgb = W*H*3 doubles (exposure applied, not cast to f32). */

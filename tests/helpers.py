@@ -92,6 +92,10 @@ def robust_mask(orc_scene, o, d, tmin, tmax, rng, scale, rel=1e-5, n_perturb=6, 
         r["org"], r["dir"], r["tmin"], r["tmax"] = po, pd, tmin, tmax
         h = rs.intersect(r)
         ok &= h["prim_id"] == ref["prim_id"]
+    # exact ties (coplanar coincident faces, e.g. a box bottom on the floor): the winner
+    # depends on traversal order, so such rays are not comparable
+    if orc_scene.desc.n_prims <= 20000:
+        ok &= orc_scene.tie_count(to_orc_rays(o, d, tmin, tmax)) <= 1
     return base, ok
 
 
@@ -114,3 +118,21 @@ def luminance(img):
 
 def rmse(a, b):
     return float(np.sqrt(np.mean((np.asarray(a, float) - np.asarray(b, float)) ** 2)))
+
+
+def t_tolerance(t_ref, d, n_ref, scale):
+    """Allowed |t_gpu - t_ref|: 2e-4 relative, plus f32 coordinate quantization (4e-7 of
+    the scene scale, ~4 ulps) measured along the normal and divided by the incidence."""
+    dl = np.linalg.norm(d, axis=1)
+    cos = np.abs((n_ref * d).sum(1)) / dl
+    return 2e-4 * np.maximum(1.0, t_ref) + 4e-7 * scale / (np.maximum(cos, 1e-2) * dl)
+
+
+def dump(name, **arrays):
+    """Saves arrays for offline diagnosis when LUM_TEST_DUMP_DIR is set."""
+    import os
+
+    d = os.environ.get("LUM_TEST_DUMP_DIR")
+    if d:
+        os.makedirs(d, exist_ok=True)
+        np.savez_compressed(os.path.join(d, name + ".npz"), **arrays)

@@ -2,8 +2,10 @@
 
 Tolerances (f32 device vs f64 oracle on the same f32-representable rays):
   - hit/miss and primitive id: exact on rays the oracle finds robust (unchanged under
-    1e-5 relative perturbations of origin and direction); at least 98% of rays are robust.
-  - t: |t_gpu - t_ref| <= 2e-4 * max(1, t_ref)
+    1e-5 relative perturbations of origin and direction, and not an exact tie between
+    coincident surfaces); at least 98% of primary rays are robust.
+  - t: |t_gpu - t_ref| <= 2e-4 * max(1, t_ref) + 4e-7 * scale / (|cos| * |d|), i.e. relative
+    2e-4 plus ~4 f32 ulps of the scene's coordinates along the normal (helpers.t_tolerance)
   - normal: |n_gpu - n_ref| <= 2e-3 (unit vectors, facing the ray), front_face exact
 """
 import numpy as np
@@ -99,11 +101,15 @@ def compare_sets(world, o, d, tmin, tmax, scale, rng, min_robust=0.98, normals=N
     g = gpu.intersect(H.to_gpu_rays(o, d, tmin, tmax))
     assert ok.mean() >= min_robust, f"only {ok.mean():.4f} of rays are robust"
     bad = ok & (g["prim_id"] != base["prim_id"])
-    assert bad.sum() == 0, f"{bad.sum()} robust rays disagree on prim id (of {ok.sum()})"
     hit = ok & (base["prim_id"] >= 0)
     t_ref = base["t"][hit]
-    t_err = np.abs(g["t"][hit] - t_ref) / np.maximum(1.0, t_ref)
-    assert t_err.max(initial=0) <= T_TOL, f"max t error {t_err.max()}"
+    t_tol = H.t_tolerance(t_ref, d[hit].astype(np.float64), base["normal"][hit], scale)
+    t_bad = np.abs(g["t"][hit] - t_ref) > t_tol
+    if bad.any() or t_bad.any():
+        H.dump(f"intersect_fail_{len(o)}_{int(scale)}", o=o, d=d, gpu_prim=g["prim_id"], gpu_t=g["t"],
+               ref_prim=base["prim_id"], ref_t=base["t"], ok=ok)
+    assert bad.sum() == 0, f"{bad.sum()} robust rays disagree on prim id (of {ok.sum()})"
+    assert not t_bad.any(), f"{t_bad.sum()} t errors above tolerance, worst excess {(np.abs(g['t'][hit] - t_ref) / t_tol).max()}"
     n_err = np.abs(g["normal"][hit] - base["normal"][hit]).max(axis=1)
     assert n_err.max(initial=0) <= N_TOL, f"max normal error {n_err.max()}"
     assert (g["front_face"][hit] == base["front_face"][hit]).all()

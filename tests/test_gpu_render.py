@@ -52,8 +52,12 @@ def test_keyed_paths_match_oracle(name, w, h, spp):
     assert abs(st.shadow_rays - ost.shadow_rays) <= 0.01 * max(ost.shadow_rays, 100)
 
 
-def test_keyed_dense_mesh_with_fog():
-    world, cfg = W.dense_mesh(level=5, width=64, height=36, spp=4)
+def test_keyed_dense_mesh():
+    # Without the fog: its free-flight distance is the reference's hash of the exact ray
+    # (constant_medium.rs:47-51), which f32 path vertices cannot reproduce bit for bit, so
+    # keyed paths part ways at the first fog test.  Fog is covered by the ray-set tests
+    # (exact on identical rays) and by the converged check below.
+    world, cfg = W.dense_mesh(level=5, width=64, height=36, spp=4, fog=False)
     world.camera.aspect_ratio = 64 / 36
     keyed_compare(world, cfg, frac=0.95)
 
@@ -86,6 +90,12 @@ def test_converged_box_room_matches_reference_estimator():
 
 def test_converged_random_spheres_matches_reference_estimator():
     world, cfg = small("random_spheres", 64, 36, 256)
+    converged_check(world, cfg, 256, 1024)
+
+
+def test_converged_dense_mesh_with_fog_matches_reference_estimator():
+    world, cfg = W.dense_mesh(level=5, width=48, height=27)
+    world.camera.aspect_ratio = 48 / 27
     converged_check(world, cfg, 256, 1024)
 
 
