@@ -103,7 +103,9 @@ class ClockSampler:
         self.proc = None
         self.lines = []
 
-    def start(self):
+    def start(self, wait_s=20.0):
+        """Starts sampling and waits (up to wait_s) for the first sample, so nvidia-smi's own
+        start-up does not overlap the timed region."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
@@ -112,6 +114,11 @@ class ClockSampler:
             self.t.start()
         except FileNotFoundError:
             self.proc = None
+            return
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < wait_s and self.proc.poll() is None:
+            time.sleep(0.05)
+        self.lines.clear()
 
     def _read(self):
         for line in self.proc.stdout:
@@ -273,14 +280,16 @@ def run_ours(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")   # > 126 MB L2
     stream = torch.cuda.current_stream()
 
+    t1 = time.perf_counter()
     counts = sc.count_tests(cfg)                   # counter build, same seeds (not timed)
+    t2 = time.perf_counter()
+    clocks = ClockSampler(dev)
+    clocks.start()
     for _ in range(args.warmup):
         sc.render_device(cfg, out.data_ptr(), stream.cuda_stream)
     barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(dev)
-    clocks.start()
-    time.sleep(0.3)
+    log(f"scene build {build_s:.3f}s, counter build {t2 - t1:.3f}s, warmup {time.perf_counter() - t2:.3f}s")
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     kernel_ms, segs, shadows = [], 0, 0

@@ -12,6 +12,10 @@
 namespace lum {
 
 constexpr int kRenderThreads = 128;
+// Minimum resident blocks per SM requested from the register allocator for the megakernel.
+#ifndef LUM_RENDER_MIN_BLOCKS
+#define LUM_RENDER_MIN_BLOCKS 4
+#endif
 constexpr unsigned kFull = 0xffffffffu;
 
 __device__ __forceinline__ void flush_counters(WorkCounters* wc, uint32_t err, uint32_t nseg, uint32_t nsh) {
@@ -31,11 +35,13 @@ __device__ __forceinline__ void flush_counters(WorkCounters* wc, uint32_t err, u
 
 // Persistent megakernel.  Each warp takes 8x4 pixel tiles from a global counter; each lane
 // owns one pixel and walks its strata [s_begin, s_end), starting a new path as soon as the
-// previous one ends (path regeneration keeps lanes busy).  The per-pixel sum is taken in a
-// fixed order, so the image does not depend on scheduling.
-// COUNT = true is the counter build: same paths, plus node/primitive test tallies.
+// previous one ends (path regeneration).  Every loop iteration runs exactly one traversal
+// per active lane -- the closest hit of a path segment or the any hit of an NEE shadow
+// ray, through the same code -- followed by that lane's shading step, so traversal stays
+// convergent across lanes at different bounces.  The per-pixel sum is taken in a fixed
+// order, so the image does not depend on scheduling.
 template <bool COUNT>
-__global__ void __launch_bounds__(kRenderThreads) k_render(SceneDev S, RenderDev R, float* __restrict__ out,
+__global__ void __launch_bounds__(kRenderThreads, LUM_RENDER_MIN_BLOCKS) k_render(SceneDev S, RenderDev R, float* __restrict__ out,
                                                            WorkCounters* wc) {
     extern __shared__ int s_stack[];
     int* stack = s_stack + threadIdx.x;
@@ -55,23 +61,44 @@ __global__ void __launch_bounds__(kRenderThreads) k_render(SceneDev S, RenderDev
         V acc = mk(0.f, 0.f, 0.f);
         float wsum = 0.0f;
         uint32_t st = R.s_begin;
-        bool active = false;
+        int state = ST_IDLE;
         Path P;
+        Pending pend;
         for (;;) {
-            if (!active && valid && st < R.s_end) {
+            if (state == ST_IDLE && valid && st < R.s_end) {
                 start_path(S, R, gi, gj, pixel, st, P);
                 ++st;
-                active = true;
+                state = R.max_depth > 0 ? ST_CLOSEST : ST_DONE;
             }
-            if (!__any_sync(kFull, active)) break;
-            if (active && path_bounce<COUNT>(S, R, pixel, P, stack, err, nseg, nsh, &tally)) {
+            if (!__any_sync(kFull, state != ST_IDLE)) break;
+            if (state == ST_CLOSEST || state == ST_SHADOW) {
+                const bool shadow = state == ST_SHADOW;
+                Ray r;
+                r.o = P.ray.o;
+                r.d = shadow ? pend.dir : P.ray.d;
+                r.time = shadow ? 0.0f : P.ray.time;                  // Ray::new (render.rs:1457)
+                Hit h;
+                h.t = shadow ? pend.tmax : CUDART_INF_F;
+                h.prim = -1;
+                h.b1 = h.b2 = 0.0f;
+                const bool found = trace<COUNT>(S, r, 0.001f, shadow, h, stack, err, &tally);
+                if (shadow) {
+                    ++nsh;
+                    if (!found) P.L = P.L + pend.contrib;
+                    state = P.bounce >= R.max_depth ? ST_DONE : ST_CLOSEST;
+                } else {
+                    ++nseg;
+                    state = shade(S, R, pixel, P, found, h, pend);
+                }
+            }
+            if (state == ST_DONE) {
                 // luminance clamp and filter weight (render.rs:1692-1701)
                 float lum = 0.2126f * P.L.x + 0.7152f * P.L.y + 0.0722f * P.L.z;
                 V cl = lum > 100.0f ? P.L * (100.0f / lum) : P.L;
                 float w = filter_weight(R.pixel_filter, P.jx - 0.5f, P.jy - 0.5f);
                 acc = fma3(cl, w, acc);
                 wsum += w;
-                active = false;
+                state = ST_IDLE;
             }
         }
         if (valid) {
@@ -142,7 +169,7 @@ __global__ void __launch_bounds__(kRenderThreads) k_intersect(SceneDev S, const 
         h.b1 = h.b2 = 0.0f;
         lum_hit out;
         out.reserved = 0;
-        if (traverse<false>(S, ray, r.tmin, h, stack, err)) {
+        if (trace(S, ray, r.tmin, false, h, stack, err)) {
             Surface sf = surface_of(S, ray, h);
             out.t = h.t;
             hit_uv(S, ray, h, sf, out.u, out.v);
@@ -176,7 +203,7 @@ __global__ void __launch_bounds__(kRenderThreads) k_occluded(SceneDev S, const l
         Hit h;
         h.t = r.tmax;
         h.prim = -1;
-        occ[idx] = traverse<true>(S, ray, r.tmin, h, stack, err) ? 1 : 0;
+        occ[idx] = trace(S, ray, r.tmin, true, h, stack, err) ? 1 : 0;
     }
     if (err) atomicOr(&wc->error_flags, err);
 }

@@ -281,11 +281,22 @@ __device__ __forceinline__ bool hit_plane(const PlaneDev& P, const Ray& ray, flo
 }
 
 // ------------------------------------------------------------------------------ traversal
-// Stack lives in shared memory: entry k of thread j at stack[k * blockDim.x + j].
-// ANY = true stops at the first accepted hit (shadow rays, src/render.rs:1457-1460).
-template <bool ANY, bool COUNT = false>
-__device__ __forceinline__ bool traverse(const SceneDev& S, const Ray& ray, float tmin, Hit& hit, int* stack,
-                                         uint32_t& err, TestTally* tl = nullptr) {
+// BVH2 traversal with postponed leaves (the "while-while" organisation of Aila & Laine,
+// "Understanding the Efficiency of Ray Traversal on GPUs", HPG 2009): a lane that reaches a
+// leaf keeps it pending and goes on descending inner nodes until every active lane of the
+// warp holds a leaf; then all lanes test their leaves together.  Inner nodes are visited
+// near child first.  Stack entries (shared memory, entry k of thread j at
+// stack[k * blockDim.x + j]) are inner-node indices (>= 0) or leaf ranges ~(first << 3 |
+// count - 1); kSentinel marks the empty stack.
+//
+// Closest hit (any = false) keeps the nearest accepted t; any = true returns at the first
+// accepted hit (the shadow query, render.rs:1457-1460).  Unbounded planes follow the BVH
+// (scene.rs:826-831).
+constexpr int kSentinel = 0x7fffffff;
+
+template <bool COUNT = false>
+__device__ __forceinline__ bool trace(const SceneDev& S, const Ray& ray, float tmin, bool any, Hit& hit, int* stack,
+                                      uint32_t& err, TestTally* tl = nullptr) {
     bool found = false;
     if (S.n_nodes > 0) {
         // Reciprocals of direction components clamped away from zero: the FMA slab form
@@ -298,62 +309,63 @@ __device__ __forceinline__ bool traverse(const SceneDev& S, const Ray& ray, floa
         const float4* nodes = reinterpret_cast<const float4*>(S.nodes);
         const int stride = blockDim.x;
         int sp = 0;
-        int node = 0;
+        int node = 0;   // inner node index, leaf (< 0) or kSentinel
+        int leaf = 0;   // postponed leaf (< 0) or 0
         for (;;) {
-            float4 n0 = __ldg(nodes + 4 * node + 0);
-            float4 n1 = __ldg(nodes + 4 * node + 1);
-            float4 n2 = __ldg(nodes + 4 * node + 2);
-            int4 n3 = __ldg(reinterpret_cast<const int4*>(nodes) + 4 * node + 3);
-            if constexpr (COUNT) tl->node++;
-            // slab tests of both children (aabb.rs:18-56)
-            float a0 = fmaf(n0.x, ix, ox), a1 = fmaf(n0.y, ix, ox);
-            float b0 = fmaf(n0.z, iy, oy), b1 = fmaf(n0.w, iy, oy);
-            float c0 = fmaf(n2.x, iz, oz), c1 = fmaf(n2.y, iz, oz);
-            float en0 = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), tmin));
-            float ex0 = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), hit.t));
-            float d0 = fmaf(n1.x, ix, ox), d1 = fmaf(n1.y, ix, ox);
-            float e0 = fmaf(n1.z, iy, oy), e1 = fmaf(n1.w, iy, oy);
-            float f0 = fmaf(n2.z, iz, oz), f1 = fmaf(n2.w, iz, oz);
-            float en1 = fmaxf(fmaxf(fminf(d0, d1), fminf(e0, e1)), fmaxf(fminf(f0, f1), tmin));
-            float ex1 = fminf(fminf(fmaxf(d0, d1), fmaxf(e0, e1)), fminf(fmaxf(f0, f1), hit.t));
-            bool h0 = en0 < ex0, h1 = en1 < ex1;
-            if (h0 && n3.z > 0) {
-                for (int k = 0; k < n3.z; ++k) {
-                    if (test_prim<COUNT>(S, n3.x + k, ray, tmin, hit, tl)) {
-                        found = true;
-                        if (ANY) return true;
-                    }
-                }
-                h0 = false;
-            }
-            if (h1 && n3.w > 0) {
-                for (int k = 0; k < n3.w; ++k) {
-                    if (test_prim<COUNT>(S, n3.y + k, ray, tmin, hit, tl)) {
-                        found = true;
-                        if (ANY) return true;
-                    }
-                }
-                h1 = false;
-            }
-            if (h0 && h1) {
-                int nearc = en0 <= en1 ? n3.x : n3.y;
-                int farc = en0 <= en1 ? n3.y : n3.x;
-                if (sp < kStackDepth) {
-                    stack[sp * stride] = farc;
-                    ++sp;
+            while ((unsigned)node < (unsigned)kSentinel) {
+                float4 n0 = __ldg(nodes + 4 * node + 0);
+                float4 n1 = __ldg(nodes + 4 * node + 1);
+                float4 n2 = __ldg(nodes + 4 * node + 2);
+                int4 n3 = __ldg(reinterpret_cast<const int4*>(nodes) + 4 * node + 3);
+                if constexpr (COUNT) tl->node++;
+                // slab tests of both children (aabb.rs:18-56)
+                float a0 = fmaf(n0.x, ix, ox), a1 = fmaf(n0.y, ix, ox);
+                float b0 = fmaf(n0.z, iy, oy), b1 = fmaf(n0.w, iy, oy);
+                float c0 = fmaf(n2.x, iz, oz), c1 = fmaf(n2.y, iz, oz);
+                float en0 = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), tmin));
+                float ex0 = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), hit.t));
+                float d0 = fmaf(n1.x, ix, ox), d1 = fmaf(n1.y, ix, ox);
+                float e0 = fmaf(n1.z, iy, oy), e1 = fmaf(n1.w, iy, oy);
+                float f0 = fmaf(n2.z, iz, oz), f1 = fmaf(n2.w, iz, oz);
+                float en1 = fmaxf(fmaxf(fminf(d0, d1), fminf(e0, e1)), fmaxf(fminf(f0, f1), tmin));
+                float ex1 = fminf(fminf(fmaxf(d0, d1), fmaxf(e0, e1)), fminf(fmaxf(f0, f1), hit.t));
+                const bool h0 = en0 < ex0, h1 = en1 < ex1;
+                const int c0e = n3.z > 0 ? ~((n3.x << 3) | (n3.z - 1)) : n3.x;
+                const int c1e = n3.w > 0 ? ~((n3.y << 3) | (n3.w - 1)) : n3.y;
+                if (!h0 && !h1) {
+                    node = sp > 0 ? stack[--sp * stride] : kSentinel;
                 } else {
-                    err |= LUM_KERR_STACK_OVERFLOW;
+                    const bool first0 = h0 && (!h1 || en0 <= en1);
+                    node = first0 ? c0e : c1e;
+                    if (h0 && h1) {
+                        if (sp < kStackDepth) {
+                            stack[sp++ * stride] = first0 ? c1e : c0e;
+                        } else {
+                            err |= LUM_KERR_STACK_OVERFLOW;
+                        }
+                    }
                 }
-                node = nearc;
-            } else if (h0) {
-                node = n3.x;
-            } else if (h1) {
-                node = n3.y;
-            } else {
-                if (sp == 0) break;
-                --sp;
-                node = stack[sp * stride];
+                if (node < 0 && leaf == 0) {
+                    leaf = node;
+                    node = sp > 0 ? stack[--sp * stride] : kSentinel;
+                }
+                if (!__any_sync(__activemask(), leaf == 0)) break;
             }
+            while (leaf < 0) {
+                const int first = (~leaf) >> 3, cnt = ((~leaf) & 7) + 1;
+                for (int k = 0; k < cnt; ++k) {
+                    if (test_prim<COUNT>(S, first + k, ray, tmin, hit, tl)) {
+                        found = true;
+                        if (any) return true;
+                    }
+                }
+                leaf = 0;
+                if (node < 0) {
+                    leaf = node;
+                    node = sp > 0 ? stack[--sp * stride] : kSentinel;
+                }
+            }
+            if (node == kSentinel) break;
         }
     }
     for (int k = 0; k < S.n_planes; ++k) {                             // scene.rs:826-831
@@ -363,7 +375,7 @@ __device__ __forceinline__ bool traverse(const SceneDev& S, const Ray& ray, floa
             hit.t = t;
             hit.prim = -2 - k;
             found = true;
-            if (ANY) return true;
+            if (any) return true;
         }
     }
     return found;
@@ -722,22 +734,27 @@ __device__ __forceinline__ void start_path(const SceneDev& S, const RenderDev& R
     P.skip_emission = false;
 }
 
-// One segment of the path (ray_color, render.rs:1472-1537, iterative form).
-// L = sum_j B_j (e_j + d_j), B_{j+1} = B_j att_j rrw_j; returns true when the path ended.
-template <bool COUNT = false>
-__device__ __forceinline__ bool path_bounce(const SceneDev& S, const RenderDev& R, uint32_t pixel, Path& P, int* stack,
-                                            uint32_t& err, uint32_t& n_seg, uint32_t& n_shadow,
-                                            TestTally* tl = nullptr) {
-    if (P.bounce >= R.max_depth) return true;                         // depth == 0 -> black
-    const uint32_t depth = R.max_depth - P.bounce;
-    Hit h;
-    h.t = CUDART_INF_F;
-    h.prim = -1;
-    ++n_seg;
-    if (!traverse<false, COUNT>(S, P.ray, 0.001f, h, stack, err, tl)) {
+// Path states of the megakernel lanes.
+enum : int { ST_IDLE = 0, ST_CLOSEST = 1, ST_SHADOW = 2, ST_DONE = 3 };
+
+// NEE shadow query pending after a bounce: direction from the new hit point, its t range
+// end, and the contribution B_j * (E albedo cos cos' A N / (pi d^2)) added if unoccluded.
+struct Pending {
+    V dir;
+    float tmax;
+    V contrib;
+};
+
+// Shading after the closest hit of segment j (ray_color, render.rs:1472-1537, iterative):
+// L += B_j e_j now, B_{j+1} = B_j att_j rrw_j, the NEE term B_j d_j once its shadow ray is
+// known to be unoccluded.  Returns the lane's next state.
+__device__ __forceinline__ int shade(const SceneDev& S, const RenderDev& R, uint32_t pixel, Path& P, bool found,
+                                     const Hit& h, Pending& pend) {
+    if (!found) {
         P.L = P.L + mul(P.beta, background(R, P.ray));
-        return true;
+        return ST_DONE;
     }
+    const uint32_t depth = R.max_depth - P.bounce;
     Surface sf = surface_of(S, P.ray, h);
     const MatDev& m = S.mats[sf.mat];
     V e = P.skip_emission ? mk(0.f, 0.f, 0.f) : emitted(m, sf.p);
@@ -745,39 +762,36 @@ __device__ __forceinline__ bool path_bounce(const SceneDev& S, const RenderDev& 
     Scatter sc;
     if (!scatter(m, P.ray, sf, h.t, su, R, pixel, P.stratum, P.bounce, sc)) {
         P.L = P.L + mul(P.beta, e);
-        return true;
+        return ST_DONE;
     }
     float4 nu = draw4(R.key0, R.key1, pixel, P.stratum, P.bounce, CALL_NEE);
     float surv = fminf(fmaxf(fmaxf(fmaxf(sc.att.x, sc.att.y), sc.att.z), 0.05f), 1.0f);
-    if (depth < 47 && nu.x > surv) {
+    if (depth < 47 && nu.x > surv) {                                   // Russian roulette
         P.L = P.L + mul(P.beta, e);
-        return true;
+        return ST_DONE;
     }
     float rrw = depth < 47 ? 1.0f / surv : 1.0f;
+    V nb = mul(P.beta, sc.att) * rrw;
+    if (has_nan(e) || has_nan(nb)) return ST_DONE;                     // render.rs:1526-1531
+    P.L = P.L + mul(P.beta, e);
     bool use_nee = !m.specular && S.n_lights > 0;
-    V dl = mk(0.f, 0.f, 0.f);
+    bool shadow = false;
     if (use_nee) {
-        Ray shadow;
-        float stmax;
+        Ray sr;
         V contrib;
-        if (sample_light(S, sf.p, sf.n, sc.att, nu, shadow, stmax, contrib)) {
-            Hit sh;
-            sh.t = stmax;
-            sh.prim = -1;
-            ++n_shadow;
-            if (!traverse<true, COUNT>(S, shadow, 0.001f, sh, stack, err, tl)) dl = contrib;
+        if (sample_light(S, sf.p, sf.n, sc.att, nu, sr, pend.tmax, contrib)) {
+            pend.dir = sr.d;
+            pend.contrib = mul(P.beta, contrib);
+            shadow = !has_nan(pend.contrib);
         }
     }
-    V term = e + dl;
-    V nb = mul(P.beta, sc.att) * rrw;
-    if (has_nan(term) || has_nan(nb)) return true;                     // render.rs:1526-1531
-    P.L = P.L + mul(P.beta, term);
     P.beta = nb;
     P.skip_emission = use_nee;
     P.ray.o = sf.p;
     P.ray.d = sc.dir;
     ++P.bounce;
-    return false;
+    if (shadow) return ST_SHADOW;
+    return P.bounce >= R.max_depth ? ST_DONE : ST_CLOSEST;             // depth == 0 -> black
 }
 
 }  // namespace lum
