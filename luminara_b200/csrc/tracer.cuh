@@ -756,11 +756,24 @@ __device__ __forceinline__ int shade(const SceneDev& S, const RenderDev& R, uint
     }
     const uint32_t depth = R.max_depth - P.bounce;
     Surface sf = surface_of(S, P.ray, h);
+    // A non-finite hit point (e.g. a fog hit at t = inf along a zero-length direction, where
+    // the reference's distance test compares against NaN) makes this level's result NaN in
+    // the reference, which its guard turns into zero for the level and everything deeper
+    // (render.rs:1526-1531).  Ending the path here drops the same terms and keeps NaN rays
+    // (whose slab tests pass every box) out of the traversal.
+    if (!isfinite(sf.p.x) || !isfinite(sf.p.y) || !isfinite(sf.p.z)) return ST_DONE;
     const MatDev& m = S.mats[sf.mat];
     V e = P.skip_emission ? mk(0.f, 0.f, 0.f) : emitted(m, sf.p);
     float4 su = draw4(R.key0, R.key1, pixel, P.stratum, P.bounce, CALL_SCATTER);
     Scatter sc;
     if (!scatter(m, P.ray, sf, h.t, su, R, pixel, P.stratum, P.bounce, sc)) {
+        P.L = P.L + mul(P.beta, e);
+        return ST_DONE;
+    }
+    // A zero or non-finite scatter direction (in_unit_sphere at radius 0) would make the
+    // next level NaN in the reference (its unit vectors divide by zero): end the path.
+    const float dl2 = len2(sc.dir);
+    if (!(dl2 > 0.0f) || !isfinite(dl2)) {
         P.L = P.L + mul(P.beta, e);
         return ST_DONE;
     }
