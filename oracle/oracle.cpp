@@ -1522,9 +1522,16 @@ V3 ray_color_keyed(const orc_scene& sc, const lum_render_params& p, Ray r, Sampl
             L += hadamard(B, background(p, r));
             break;
         }
+        // Non-finite vertex: the recursion's NaN guard zeroes this level and deeper.
+        if (!std::isfinite(h.p.x) || !std::isfinite(h.p.y) || !std::isfinite(h.p.z)) break;
         V3 e = skip || !h.mat ? v3(0, 0, 0) : h.mat->emitted(h.u, h.v, h.p);
         Scatter scat;
         if (!h.mat || !h.mat->scatter(r, h, s, scat)) {
+            L += hadamard(B, e);
+            break;
+        }
+        double dl2 = length_squared(scat.ray.d);
+        if (!(dl2 > 0.0) || !std::isfinite(dl2)) {   // zero-radius in-sphere draw: next level is NaN
             L += hadamard(B, e);
             break;
         }
