@@ -312,6 +312,27 @@ lum_status lum_render(lum_scene* scene, const lum_render_params* params, float* 
 lum_status lum_render_device(lum_scene* scene, const lum_render_params* params,
                              float* d_out_rgb, void* stream, lum_stats* stats);
 
+/* Allocation-free render.  Same image as lum_render into the same caller-owned HOST buffer,
+ * but it allocates no device memory, ever: the device image and the kernel's work counters
+ * live in one fixed array of LUM_NOALLOC_MAX_PIXELS * 12 + 256 bytes (12 MiB) that every GPU
+ * loading the library reserves until the process exits.  It is for callers that cannot call
+ * cudaMalloc at render time -- services that reserve all device memory at start-up, or whose
+ * free memory is held by another allocator's pool, where a render-time cudaMalloc would fail
+ * or stall on device-wide synchronisation.  lum_render, by contrast, allocates its device image
+ * on first use and whenever the image grows.
+ *   - Images of more than LUM_NOALLOC_MAX_PIXELS pixels (after crop) are rejected with
+ *     LUM_ERR_TOO_LARGE.
+ *   - The first call on a device looks up the array's device address (cudaGetSymbolAddress);
+ *     make that first call before any stream capture.
+ *   - All calls share the one array: calls that overlap on the GPU (e.g. from several host
+ *     threads at once) race on it.  Each call clears the counters it needs and overwrites the
+ *     image region it returns.
+ *   - stats->kernel_ms is 0 (no events are created); total_ms is the host wall time.
+ * No counterpart in the reference. */
+#define LUM_NOALLOC_MAX_PIXELS (1u << 20)
+lum_status lum_render_noalloc(lum_scene* scene, const lum_render_params* params, float* out_rgb,
+                              lum_stats* stats);
+
 /* Diagnostics: runs the counter build of the render kernel for `params` (output discarded)
  * and returns its test counts.  No counterpart in the reference, which counts only paths
  * (src/render.rs:1704). */

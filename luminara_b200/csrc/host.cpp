@@ -22,6 +22,7 @@
 #include "bvh_build.h"
 #include "device_scene.h"
 #include "kernels.h"
+#include "scene_access.h"
 
 namespace {
 
@@ -820,3 +821,23 @@ lum_status lum_occluded(lum_scene* s, const lum_ray* rays, uint32_t n, int32_t* 
 }
 
 }  // extern "C"
+
+// ----------------------------------------------------------------------------- internal access
+namespace lum {
+
+lum_status set_error(lum_status code, const char* msg) { return fail(code, "%s", msg); }
+
+lum_status prepare_render(lum_scene* s, const lum_render_params* params, SceneDev& dev, RenderDev& R,
+                          cudaStream_t& stream) {
+    if (!s) return fail(LUM_ERR_INVALID_ARGUMENT, "scene is null");
+    lum_status st = check_params(params);
+    if (st != LUM_OK) return st;
+    st = make_render_dev(s, *params, R);
+    if (st != LUM_OK) return st;
+    CU(cudaSetDevice(s->device), "cudaSetDevice");
+    dev = s->dev;
+    stream = s->stream;
+    return LUM_OK;
+}
+
+}  // namespace lum

@@ -6,7 +6,13 @@
 //   k_occluded    any hit of a ray set (the NEE shadow query, render.rs:1457-1460).
 #include <cuda_runtime.h>
 
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
 #include "kernels.h"
+#include "scene_access.h"
 #include "tracer.cuh"
 
 namespace lum {
@@ -275,3 +281,100 @@ cudaError_t launch_occluded(const SceneDev& S, const lum_ray* rays, uint32_t n, 
 }
 
 }  // namespace lum
+
+// ------------------------------------------------------------------ allocation-free render
+// lum_render_noalloc (include/luminara_gpu.h): the megakernel writes into a fixed device
+// array instead of device memory obtained from cudaMalloc.  Layout: WorkCounters in the
+// first 256 bytes, then up to LUM_NOALLOC_MAX_PIXELS RGB float pixels.  In host code
+// g_noalloc_scratch names a host-side stand-in, not the device array, so its device address
+// is looked up per device with cudaGetSymbolAddress and passed to the kernel.
+namespace {
+
+constexpr size_t kNoAllocCounterBytes = 256;
+constexpr size_t kNoAllocBytes = kNoAllocCounterBytes + (size_t)LUM_NOALLOC_MAX_PIXELS * 3 * sizeof(float);
+static_assert(sizeof(lum::WorkCounters) <= kNoAllocCounterBytes, "counters must fit the header slot");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device (looked up once per device).
+lum_status noalloc_scratch(void** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return lum::set_error(LUM_ERR_CUDA, cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices) return lum::set_error(LUM_ERR_TOO_LARGE, "device ordinal above 63");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* ptr = nullptr;
+        e = cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr) {
+            char msg[256];
+            snprintf(msg, sizeof msg, "cudaGetSymbolAddress of the no-alloc scratch failed: %s", cudaGetErrorString(e));
+            return lum::set_error(LUM_ERR_CUDA, msg);
+        }
+        g_noalloc_addr[dev] = ptr;
+    }
+    *out = g_noalloc_addr[dev];
+    return LUM_OK;
+}
+
+lum_status noalloc_cuda(cudaError_t e, const char* what) {
+    char msg[256];
+    snprintf(msg, sizeof msg, "%s: %s", what, cudaGetErrorString(e));
+    return lum::set_error(LUM_ERR_CUDA, msg);
+}
+
+}  // namespace
+
+extern "C" lum_status lum_render_noalloc(lum_scene* scene, const lum_render_params* params, float* out_rgb,
+                                         lum_stats* stats) {
+    auto t0 = std::chrono::steady_clock::now();
+    if (!scene || !params || !out_rgb) return lum::set_error(LUM_ERR_INVALID_ARGUMENT, "null argument");
+    lum::SceneDev dev;
+    lum::RenderDev R;
+    cudaStream_t stream;
+    lum_status st = lum::prepare_render(scene, params, dev, R, stream);
+    if (st != LUM_OK) return st;
+    const size_t pixels = (size_t)R.w * R.h;
+    if (pixels > LUM_NOALLOC_MAX_PIXELS) {
+        char msg[256];
+        snprintf(msg, sizeof msg, "lum_render_noalloc: a %u x %u image needs %zu pixels of scratch; the maximum is %u",
+                 R.w, R.h, pixels, (unsigned)LUM_NOALLOC_MAX_PIXELS);
+        return lum::set_error(LUM_ERR_TOO_LARGE, msg);
+    }
+    if (stats) std::memset(stats, 0, sizeof *stats);
+    if (pixels == 0) return LUM_OK;
+    void* base = nullptr;
+    st = noalloc_scratch(&base);
+    if (st != LUM_OK) return st;
+    auto* wc = reinterpret_cast<lum::WorkCounters*>(base);
+    float* image = reinterpret_cast<float*>(static_cast<unsigned char*>(base) + kNoAllocCounterBytes);
+    const size_t bytes = pixels * 3 * sizeof(float);
+    cudaError_t e = cudaMemsetAsync(wc, 0, sizeof(lum::WorkCounters), stream);   // counters start at zero
+    if (e != cudaSuccess) return noalloc_cuda(e, "cudaMemsetAsync");
+    if (R.n_tasks > 0 && R.s_end > R.s_begin) {
+        e = lum::launch_render(dev, R, image, wc, stream, 0);
+        if (e != cudaSuccess) return noalloc_cuda(e, "render launch");
+    } else {
+        e = cudaMemsetAsync(image, 0, bytes, stream);
+        if (e != cudaSuccess) return noalloc_cuda(e, "cudaMemsetAsync");
+    }
+    lum::WorkCounters counters{};
+    if ((e = cudaMemcpyAsync(out_rgb, image, bytes, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(&counters, wc, sizeof counters, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(stream)) != cudaSuccess)
+        return noalloc_cuda(e, "lum_render_noalloc");
+    if (stats) {
+        stats->paths = (uint64_t)pixels * (R.s_end - R.s_begin);
+        stats->segments = counters.segments;
+        stats->shadow_rays = counters.shadow_rays;
+        stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        stats->error_flags = counters.error_flags;
+    }
+    if (counters.error_flags) return lum::set_error(LUM_ERR_KERNEL, "render kernel reported error flags");
+    return LUM_OK;
+}
+

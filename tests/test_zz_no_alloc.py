@@ -1,0 +1,73 @@
+"""GPU test of lum_render_noalloc, the allocation-free render entry point.
+
+Some callers cannot call cudaMalloc while rendering: services that reserve the device's
+memory at start-up, or whose free memory is held by another allocator's pool, where a
+render-time allocation would fail or stall on device-wide synchronisation.  For them
+lum_render_noalloc keeps the device image and the kernel's counters in one fixed array
+(LUM_NOALLOC_MAX_PIXELS pixels) instead of allocating.  This file checks, through the C ABI,
+that two calls in a row return the same image as lum_render (same kernel and seeds; the
+tolerance of the other render tests' exact comparisons, rtol 1e-6), that the shared array is
+reused cleanly by a call with another scene and size, and that images beyond the maximum are
+rejected.  It is named to be collected last.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import luminara_b200 as L
+from luminara_b200 import abi
+from luminara_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _noalloc():
+    f = L.lib().lum_render_noalloc
+    f.argtypes = [C.c_void_p, C.POINTER(abi.LumRenderParams), C.c_void_p, C.POINTER(abi.LumStats)]
+    f.restype = C.c_int32
+    return f
+
+
+def _call(scene, cfg):
+    p = cfg.to_c()
+    out = np.full(cfg.out_shape(), np.nan, dtype=np.float32)
+    st = abi.LumStats()
+    rc = _noalloc()(scene.h, C.byref(p), out.ctypes.data, C.byref(st))
+    return rc, out, st
+
+
+def test_noalloc_matches_render_on_two_calls_in_a_row():
+    world, cfg = W.box_room(width=96, height=64, spp=16)
+    world.camera.aspect_ratio = 96 / 64
+    sc = L.GpuScene(world)
+    ref, ref_st = sc.render(cfg)
+    for _ in range(2):
+        rc, out, st = _call(sc, cfg)
+        assert rc == abi.LUM_OK, L.lib().lum_last_error()
+        np.testing.assert_allclose(out, ref, rtol=1e-6, atol=1e-7)
+        assert st.paths == ref_st.paths == 96 * 64 * 16
+        assert st.segments == ref_st.segments and st.error_flags == 0
+
+
+def test_noalloc_reuses_the_shared_array_across_scenes_and_sizes():
+    world, cfg = W.random_spheres(width=128, height=72, spp=4)
+    world.camera.aspect_ratio = 128 / 72
+    sc = L.GpuScene(world)
+    ref, _ = sc.render(cfg)
+    rc, out, _ = _call(sc, cfg)
+    assert rc == abi.LUM_OK, L.lib().lum_last_error()
+    np.testing.assert_allclose(out, ref, rtol=1e-6, atol=1e-7)
+    cfg.crop = (10, 5, 40, 30)                 # smaller region after a larger one
+    ref2, _ = sc.render(cfg)
+    rc, out2, _ = _call(sc, cfg)
+    assert rc == abi.LUM_OK, L.lib().lum_last_error()
+    np.testing.assert_allclose(out2, ref2, rtol=1e-6, atol=1e-7)
+
+
+def test_noalloc_rejects_images_beyond_the_maximum():
+    world, cfg = W.box_room(width=2048, height=1024, spp=1)   # 2^21 pixels > 2^20
+    sc = L.GpuScene(world)
+    rc, _, _ = _call(sc, cfg)
+    assert rc == abi.LUM_ERR_TOO_LARGE
+    assert b"maximum" in L.lib().lum_last_error()
