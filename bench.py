@@ -390,10 +390,85 @@ def run_ours(args):
     return 0
 
 
+# ------------------------------------------------------------------------------ batched
+def run_batched(args):
+    """The batched uneven workload: 64 seeded scenes rendered (a) one after another with the
+    megakernel and (b) together by the persistent wavefront tracer; reports both."""
+    import torch
+
+    import luminara_b200 as L
+    from luminara_b200 import workloads as W
+
+    torch.cuda.set_device(0)
+    items = W.batched()
+    scenes = [L.GpuScene(w) for w, _ in items]
+    cfgs = [c for _, c in items]
+    paths = sum(c.out_shape()[0] * c.out_shape()[1] * strata(c) for c in cfgs)
+    outs = [torch.empty(c.out_shape(), dtype=torch.float32, device="cuda") for c in cfgs]
+    stream = torch.cuda.current_stream()
+    t0 = time.perf_counter()
+    tuned, tune_ms = L.autotune(scenes, cfgs)
+    tune_s = time.perf_counter() - t0
+    batch = L.Batch(scenes, cfgs)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def seq():
+        for s, c, o in zip(scenes, cfgs, outs):
+            s.render_device(c, o.data_ptr(), stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        seq()
+        batch.render_device([o.data_ptr() for o in outs])
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        seq()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    seq_s = ev0.elapsed_time(ev1) / 1e3
+    seq_imgs = [o.clone() for o in outs]
+    done_all, bstats = [], []
+    ev0.record(stream)
+    for _ in range(args.steps):
+        done, st = batch.render_device([o.data_ptr() for o in outs])
+        done_all.append(done)
+        bstats.append(st)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    bat_s = ev0.elapsed_time(ev1) / 1e3
+    clock_info = clocks.stop()
+    max_rel = max(float(((a - b).abs() / (b.abs() + 1e-3)).max()) for a, b in zip(outs, seq_imgs))
+    value = paths * args.steps / bat_s / 1e6
+    done_ms = done_all[-1]
+    line = {
+        "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": bat_s * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+        "config": {"workload": f"batched: {len(cfgs)} uneven scenes, {paths} paths per step",
+                   "scenes": len(cfgs), "prims": sum(w.n_prims() for w, _ in items),
+                   "l2": "working set of the batch exceeds L2 (pool, queues, 64 scenes)"},
+        "sequential_megakernel": {"value": paths * args.steps / seq_s / 1e6, "unit": "Mpaths/s",
+                                  "ms_per_step": seq_s * 1e3 / args.steps},
+        "speedup_vs_sequential": seq_s / bat_s,
+        "max_rel_diff_vs_megakernel": max_rel,
+        "autotune": {"config": tuned, "best_ms": tune_ms, "seconds": tune_s},
+        "scene_done_ms": {"min": min(done_ms), "median": statistics.median(done_ms), "max": max(done_ms)},
+        "iterations": bstats[-1].iterations, "graph_launches": bstats[-1].graph_launches,
+        "gpu_launches": None, "clocks": clock_info,
+    }
+    print(json.dumps(line), flush=True)
+    batch.close()
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.config == "batched":
+        return run_batched(args)
     return run_ours(args)
 
 

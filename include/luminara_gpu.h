@@ -346,6 +346,58 @@ lum_status lum_intersect(lum_scene* scene, const lum_ray* rays, uint32_t n, lum_
  * Some.  HOST arrays. */
 lum_status lum_occluded(lum_scene* scene, const lum_ray* rays, uint32_t n, int32_t* occluded);
 
+/* ------------------------------------------------------------------------------------
+ * Batched wavefront rendering: many scenes per launch sequence.
+ *
+ * The reference renders one scene per render() call (src/render.rs:1557); a batch is the
+ * same as n independent render() calls (one lum_render_params per scene), traced together by
+ * a persistent wavefront tracer with material-sorted queues under a captured CUDA graph.
+ * Images equal lum_render's up to float rounding of the per-pixel sum (the batch sums in 64-bit
+ * fixed point, independent of completion order).
+ * ---------------------------------------------------------------------------------- */
+typedef struct lum_batch_config {
+    uint32_t pool_paths;      /* path slots in flight (1024 .. 2^24) */
+    uint32_t block_threads;   /* 128 or 256 */
+    uint32_t sort_threshold;  /* extend queues shorter than this shade in one generic kernel */
+    uint32_t iters_per_graph; /* wavefront iterations captured per CUDA graph launch (1 .. 64) */
+    uint32_t reserved[4];
+} lum_batch_config;
+
+typedef struct lum_batch_stats {
+    uint64_t paths;
+    uint64_t segments;
+    uint64_t shadow_rays;
+    double device_ms;         /* CUDA-event time from the first kernel to the last */
+    double total_ms;          /* host wall time of the call */
+    uint32_t graph_launches;
+    uint32_t iterations;
+    uint32_t error_flags;     /* LUM_KERR_* */
+    uint32_t reserved;
+} lum_batch_stats;
+
+typedef struct lum_batch lum_batch; /* opaque; references its scenes, which must outlive it */
+
+lum_status lum_batch_default_config(lum_batch_config* cfg);
+/* Times candidate configurations (pool size, block size, sort threshold) on a calibration
+ * run of the batch (about 1/8 of each scene's strata) and returns the fastest; results are
+ * cached per device and batch signature in $LUM_AUTOTUNE_CACHE (default
+ * ~/.cache/luminara_b200_autotune.txt).  best_ms may be NULL; it is -1 on a cache hit. */
+lum_status lum_batch_autotune(lum_scene* const* scenes, const lum_render_params* params, uint32_t n,
+                              lum_batch_config* out, double* best_ms);
+/* cfg NULL = autotuned.  Allocates the path pool, queues and accumulators and captures the
+ * iteration graph. */
+lum_status lum_batch_create(lum_scene* const* scenes, const lum_render_params* params, uint32_t n,
+                            const lum_batch_config* cfg, lum_batch** out);
+lum_status lum_batch_config_of(const lum_batch* batch, lum_batch_config* cfg);
+/* Renders every scene into caller-owned HOST buffers outs[s] (W*H*3 floats each).
+ * scene_done_ms (n entries, may be NULL) receives each scene's completion time from the start
+ * of the batch. */
+lum_status lum_batch_render(lum_batch* batch, float* const* outs, double* scene_done_ms, lum_batch_stats* stats);
+/* Same into caller-owned DEVICE buffers. */
+lum_status lum_batch_render_device(lum_batch* batch, float* const* d_outs, double* scene_done_ms,
+                                   lum_batch_stats* stats);
+lum_status lum_batch_destroy(lum_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

@@ -66,8 +66,20 @@ def lib():
     L.lum_count_tests.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.POINTER(abi.LumTestCounts)]
     L.lum_intersect.argtypes = [vp, vp, C.c_uint32, vp]
     L.lum_occluded.argtypes = [vp, vp, C.c_uint32, vp]
+    PP = C.POINTER(C.c_void_p)
+    L.lum_batch_default_config.argtypes = [C.POINTER(abi.LumBatchConfig)]
+    L.lum_batch_autotune.argtypes = [PP, C.POINTER(abi.LumRenderParams), C.c_uint32, C.POINTER(abi.LumBatchConfig),
+                                     C.POINTER(C.c_double)]
+    L.lum_batch_create.argtypes = [PP, C.POINTER(abi.LumRenderParams), C.c_uint32, C.POINTER(abi.LumBatchConfig),
+                                   C.POINTER(vp)]
+    L.lum_batch_config_of.argtypes = [vp, C.POINTER(abi.LumBatchConfig)]
+    L.lum_batch_render.argtypes = [vp, PP, C.POINTER(C.c_double), C.POINTER(abi.LumBatchStats)]
+    L.lum_batch_render_device.argtypes = [vp, PP, C.POINTER(C.c_double), C.POINTER(abi.LumBatchStats)]
+    L.lum_batch_destroy.argtypes = [vp]
     for name in ("lum_scene_create", "lum_scene_destroy", "lum_scene_info", "lum_render", "lum_render_device",
-                 "lum_count_tests", "lum_intersect", "lum_occluded"):
+                 "lum_count_tests", "lum_intersect", "lum_occluded", "lum_batch_default_config",
+                 "lum_batch_autotune", "lum_batch_create", "lum_batch_config_of", "lum_batch_render",
+                 "lum_batch_render_device", "lum_batch_destroy"):
         getattr(L, name).restype = C.c_int32
     if L.lum_abi_version() != abi.LUM_ABI_VERSION:
         raise ImportError("libluminara_b200.so ABI version mismatch")
@@ -138,6 +150,76 @@ class GpuScene:
         occ = np.zeros(rays.shape[0], dtype=np.int32)
         check(lib().lum_occluded(self.h, rays.ctypes.data, rays.shape[0], occ.ctypes.data))
         return occ
+
+
+class Batch:
+    """Many scenes rendered together by the persistent wavefront tracer (lum_batch_*).
+
+    `scenes` are GpuScene objects (kept alive by the batch), `configs` one RenderConfig per
+    scene.  `config` is None (autotuned, cached per device and batch), "default", or a dict
+    with pool_paths / block_threads / sort_threshold / iters_per_graph."""
+
+    def __init__(self, scenes, configs, config=None):
+        self.scenes = list(scenes)
+        self.configs = list(configs)
+        n = len(self.scenes)
+        self._handles = (C.c_void_p * n)(*[s.h.value for s in self.scenes])
+        self._params = (abi.LumRenderParams * n)(*[c.to_c() for c in self.configs])
+        cfg_ptr = None
+        if config is not None:
+            cfg = abi.LumBatchConfig()
+            check(lib().lum_batch_default_config(C.byref(cfg)))
+            if isinstance(config, dict):
+                for k, v in config.items():
+                    setattr(cfg, k, int(v))
+            cfg_ptr = C.byref(cfg)
+        h = C.c_void_p()
+        check(lib().lum_batch_create(C.cast(self._handles, C.POINTER(C.c_void_p)), self._params, n, cfg_ptr,
+                                     C.byref(h)))
+        self.h = h
+
+    def config(self):
+        c = abi.LumBatchConfig()
+        check(lib().lum_batch_config_of(self.h, C.byref(c)))
+        return {"pool_paths": c.pool_paths, "block_threads": c.block_threads, "sort_threshold": c.sort_threshold,
+                "iters_per_graph": c.iters_per_graph}
+
+    def render(self):
+        """Returns (images, per-scene completion ms, lum_batch_stats)."""
+        n = len(self.scenes)
+        imgs = [np.empty(c.out_shape(), dtype=np.float32) for c in self.configs]
+        ptrs = (C.c_void_p * n)(*[im.ctypes.data for im in imgs])
+        done = (C.c_double * n)()
+        st = abi.LumBatchStats()
+        check(lib().lum_batch_render(self.h, C.cast(ptrs, C.POINTER(C.c_void_p)), done, C.byref(st)))
+        return imgs, list(done), st
+
+    def render_device(self, d_ptrs):
+        n = len(self.scenes)
+        ptrs = (C.c_void_p * n)(*d_ptrs)
+        done = (C.c_double * n)()
+        st = abi.LumBatchStats()
+        check(lib().lum_batch_render_device(self.h, C.cast(ptrs, C.POINTER(C.c_void_p)), done, C.byref(st)))
+        return list(done), st
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().lum_batch_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+
+def autotune(scenes, configs):
+    """Runs (or reads from cache) the batch autotuner; returns (config dict, best ms or -1)."""
+    n = len(scenes)
+    handles = (C.c_void_p * n)(*[s.h.value for s in scenes])
+    params = (abi.LumRenderParams * n)(*[c.to_c() for c in configs])
+    cfg = abi.LumBatchConfig()
+    ms = C.c_double()
+    check(lib().lum_batch_autotune(C.cast(handles, C.POINTER(C.c_void_p)), params, n, C.byref(cfg), C.byref(ms)))
+    return ({"pool_paths": cfg.pool_paths, "block_threads": cfg.block_threads, "sort_threshold": cfg.sort_threshold,
+             "iters_per_graph": cfg.iters_per_graph}, ms.value)
 
 
 @dataclass

@@ -230,6 +230,30 @@ class LumTestCounts(C.Structure):
                                           "paths")]
 
 
+class LumBatchConfig(C.Structure):
+    _fields_ = [
+        ("pool_paths", C.c_uint32),
+        ("block_threads", C.c_uint32),
+        ("sort_threshold", C.c_uint32),
+        ("iters_per_graph", C.c_uint32),
+        ("reserved", C.c_uint32 * 4),
+    ]
+
+
+class LumBatchStats(C.Structure):
+    _fields_ = [
+        ("paths", C.c_uint64),
+        ("segments", C.c_uint64),
+        ("shadow_rays", C.c_uint64),
+        ("device_ms", C.c_double),
+        ("total_ms", C.c_double),
+        ("graph_launches", C.c_uint32),
+        ("iterations", C.c_uint32),
+        ("error_flags", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
 # numpy dtypes of the ray/hit records (for bulk arrays)
 def ray_dtype():
     import numpy as np
@@ -269,4 +293,6 @@ STRUCT_SIZES = {
     "lum_ray": C.sizeof(LumRay),
     "lum_hit": C.sizeof(LumHit),
     "lum_test_counts": C.sizeof(LumTestCounts),
+    "lum_batch_config": C.sizeof(LumBatchConfig),
+    "lum_batch_stats": C.sizeof(LumBatchStats),
 }

@@ -840,4 +840,15 @@ lum_status prepare_render(lum_scene* s, const lum_render_params* params, SceneDe
     return LUM_OK;
 }
 
+lum_status scene_view(lum_scene* s, const lum_render_params* params, SceneDev& dev, RenderDev& R, int& device) {
+    if (!s) return fail(LUM_ERR_INVALID_ARGUMENT, "scene is null");
+    lum_status st = check_params(params);
+    if (st != LUM_OK) return st;
+    st = make_render_dev(s, *params, R);
+    if (st != LUM_OK) return st;
+    dev = s->dev;
+    device = s->device;
+    return LUM_OK;
+}
+
 }  // namespace lum

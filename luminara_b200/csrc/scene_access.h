@@ -16,4 +16,8 @@ lum_status set_error(lum_status code, const char* msg);
 lum_status prepare_render(lum_scene* s, const lum_render_params* params, SceneDev& dev, RenderDev& R,
                           cudaStream_t& stream);
 
+// Device view, owning device ordinal and render description of a scene for `params`
+// (validated), without touching the scene's stream.
+lum_status scene_view(lum_scene* s, const lum_render_params* params, SceneDev& dev, RenderDev& R, int& device);
+
 }  // namespace lum

@@ -482,10 +482,13 @@ struct Scatter {
 };
 
 // Material::scatter; draws s = (s0..s3) of CALL_SCATTER, extra for dispersion.
+// KIND >= 0 fixes the material kind at compile time (the material-sorted shading kernels of
+// the wavefront tracer); KIND = -1 dispatches on m.kind.  Both run the same arithmetic.
+template <int KIND = -1>
 __device__ __forceinline__ bool scatter(const MatDev& m, const Ray& ray, const Surface& sf, float hit_t, float4 s,
                                         const RenderDev& R, uint32_t pixel, uint32_t stratum, uint32_t bounce,
                                         Scatter& out) {
-    switch (m.kind) {
+    switch (KIND >= 0 ? KIND : m.kind) {
         case 1: {                                                      // material.rs:59-71
             V d = sf.n + unit_vector(s.x, s.y);
             if (near_zero(d)) d = sf.n;
@@ -748,6 +751,7 @@ struct Pending {
 // Shading after the closest hit of segment j (ray_color, render.rs:1472-1537, iterative):
 // L += B_j e_j now, B_{j+1} = B_j att_j rrw_j, the NEE term B_j d_j once its shadow ray is
 // known to be unoccluded.  Returns the lane's next state.
+template <int KIND = -1>
 __device__ __forceinline__ int shade(const SceneDev& S, const RenderDev& R, uint32_t pixel, Path& P, bool found,
                                      const Hit& h, Pending& pend) {
     if (!found) {
@@ -766,7 +770,7 @@ __device__ __forceinline__ int shade(const SceneDev& S, const RenderDev& R, uint
     V e = P.skip_emission ? mk(0.f, 0.f, 0.f) : emitted(m, sf.p);
     float4 su = draw4(R.key0, R.key1, pixel, P.stratum, P.bounce, CALL_SCATTER);
     Scatter sc;
-    if (!scatter(m, P.ray, sf, h.t, su, R, pixel, P.stratum, P.bounce, sc)) {
+    if (!scatter<KIND>(m, P.ray, sf, h.t, su, R, pixel, P.stratum, P.bounce, sc)) {
         P.L = P.L + mul(P.beta, e);
         return ST_DONE;
     }

@@ -313,11 +313,27 @@ class RenderConfig:
 # --------------------------------------------------------------------------------------
 # World -> lum_scene_desc
 # --------------------------------------------------------------------------------------
+OBJECT_DTYPE = np.dtype([("kind", "<i4"), ("material", "<i4"), ("transform", "<i4"), ("reserved", "<i4"),
+                         ("p", "<f8", 12)])
+MATERIAL_DTYPE = np.dtype([("kind", "<i4"), ("texture", "<i4"), ("color", "<f8", 3), ("color2", "<f8", 3),
+                           ("tex_scale", "<f8"), ("fuzz", "<f8"), ("ior", "<f8"), ("roughness", "<f8"),
+                           ("metallic", "<f8"), ("intensity", "<f8"), ("dispersion", "<f8"), ("tint", "<f8", 3)])
+
+
+def material_array(n: int) -> np.ndarray:
+    """n zeroed lum_material records (tint (1,1,1), checker scale 1)."""
+    m = np.zeros(n, dtype=MATERIAL_DTYPE)
+    m["tint"] = 1.0
+    m["tex_scale"] = 1.0
+    return m
+
+
 class World:
     """An ordered object list (HittableList) plus NEE lights and camera.
 
     ``add`` keeps insertion order, which fixes primitive ids: one id per object (six for a
-    box), then mesh triangles in mesh order.
+    box), then mesh triangles in mesh order.  ``add_bulk`` appends many untransformed objects
+    at once from structured arrays laid out as lum_object / lum_material.
     """
 
     def __init__(self):
@@ -326,7 +342,15 @@ class World:
         self.lights: List[LightInfo] = []
         self.materials: List[Material] = []
         self._mat_index = {}
+        self._bulk = []          # (insert position in objects, object array, material array)
         self.camera = CameraConfig()
+
+    def add_bulk(self, objects: np.ndarray, materials: np.ndarray) -> int:
+        """Appends objects (OBJECT_DTYPE, material = index into `materials`, transform -1)."""
+        first = self.n_prims()
+        self._bulk.append((len(self.objects), np.ascontiguousarray(objects, dtype=OBJECT_DTYPE),
+                           np.ascontiguousarray(materials, dtype=MATERIAL_DTYPE)))
+        return first
 
     def material_index(self, m: Optional[Material]) -> int:
         if m is None:
@@ -356,6 +380,7 @@ class World:
 
     def n_prims(self) -> int:
         n = sum(6 if o.kind == abi.OBJ_BOX else 1 for o in self.objects)
+        n += sum(int(((b["kind"] == abi.OBJ_BOX) * 5 + 1).sum()) for _, b, _ in self._bulk)
         return n + sum(int(m.indices.shape[0]) for m in self.meshes)
 
     def desc(self) -> "SceneDesc":
@@ -368,6 +393,8 @@ class SceneDesc:
     def __init__(self, world: World):
         objs = []
         xforms = []
+        for o in world.objects:
+            world.material_index(o.material)
         for o in world.objects:
             lo = abi.LumObject()
             lo.kind = o.kind
@@ -386,7 +413,34 @@ class SceneDesc:
                 lo.transform = len(xforms)
                 xforms.append(t)
             objs.append(lo)
-        self._objects = (abi.LumObject * max(len(objs), 1))(*objs)
+        n_mat_regular = len(world.materials)
+        if world._bulk:
+            # interleave the bulk chunks at their insertion positions; their material indices
+            # follow the regular materials
+            obj_np = np.zeros(len(objs), dtype=OBJECT_DTYPE)
+            if objs:
+                obj_np[:] = np.frombuffer((abi.LumObject * len(objs))(*objs), dtype=OBJECT_DTYPE)
+            parts, mats_np, last, mat_base = [], [], 0, n_mat_regular
+            for pos, bobj, bmat in world._bulk:
+                parts.append(obj_np[last:pos])
+                chunk = bobj.copy()
+                chunk["material"] += mat_base
+                chunk["transform"] = -1
+                parts.append(chunk)
+                mats_np.append(bmat)
+                mat_base += len(bmat)
+                last = pos
+            parts.append(obj_np[last:])
+            all_obj = np.concatenate(parts) if parts else np.zeros(0, dtype=OBJECT_DTYPE)
+            self._obj_np = np.ascontiguousarray(all_obj)
+            self._objects = (abi.LumObject * max(len(all_obj), 1)).from_buffer(
+                self._obj_np if len(all_obj) else np.zeros(1, dtype=OBJECT_DTYPE))
+            n_objects = len(all_obj)
+            self._bulk_mats = np.concatenate(mats_np)
+        else:
+            self._objects = (abi.LumObject * max(len(objs), 1))(*objs)
+            n_objects = len(objs)
+            self._bulk_mats = None
         self._xforms = (abi.LumTransform * max(len(xforms), 1))(*xforms)
         self._keep = []
         meshes = []
@@ -411,16 +465,25 @@ class SceneDesc:
             meshes.append(lm)
         self._meshes = (abi.LumMesh * max(len(meshes), 1))(*meshes)
         mats = [m.to_c() for m in world.materials]
-        self._materials = (abi.LumMaterial * max(len(mats), 1))(*mats)
+        if self._bulk_mats is not None:
+            reg = np.zeros(len(mats), dtype=MATERIAL_DTYPE)
+            if mats:
+                reg[:] = np.frombuffer((abi.LumMaterial * len(mats))(*mats), dtype=MATERIAL_DTYPE)
+            self._mat_np = np.ascontiguousarray(np.concatenate([reg, self._bulk_mats]))
+            self._materials = (abi.LumMaterial * len(self._mat_np)).from_buffer(self._mat_np)
+            n_materials = len(self._mat_np)
+        else:
+            self._materials = (abi.LumMaterial * max(len(mats), 1))(*mats)
+            n_materials = len(mats)
         lights = [l.to_c() for l in world.lights]
         self._lights = (abi.LumLight * max(len(lights), 1))(*lights)
         d = abi.LumSceneDesc()
         d.objects = self._objects
-        d.n_objects = len(objs)
+        d.n_objects = n_objects
         d.meshes = self._meshes
         d.n_meshes = len(meshes)
         d.materials = self._materials
-        d.n_materials = len(mats)
+        d.n_materials = n_materials
         d.transforms = self._xforms
         d.n_transforms = len(xforms)
         d.lights = self._lights
@@ -428,7 +491,7 @@ class SceneDesc:
         d.camera = world.camera.to_c()
         self.c = d
         self.n_prims = world.n_prims()
-        self.n_materials = len(mats)
+        self.n_materials = n_materials
 
     def ref(self):
         return C.byref(self.c)

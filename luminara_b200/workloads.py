@@ -197,6 +197,84 @@ def diff_quads(width=512, height=512, spp=64, max_depth=6, seed=31337, scene_see
     return w, cfg
 
 
+def uneven_scene(rng, n_prims, width, height, spp, max_depth=8, seed=31337):
+    """One scene of the batched workload: n_prims random spheres, quads and triangles with
+    mixed Lambertian / Metal / Dielectric / GGX materials over a ground quad, lit by a sky and
+    one or two NEE lights (built with vectorized bulk arrays)."""
+    w = S.World()
+    w.add(S.Quad((-20, 0, -20), (40, 0, 0), (0, 0, 40), S.Lambertian((0.5, 0.5, 0.5))))
+    extent = max(1.5, 0.25 * n_prims ** (1 / 3))
+    size = 0.6 * extent / max(1.0, n_prims ** (1 / 3))
+    kinds = rng.integers(0, 3, n_prims)
+    r = rng.random(n_prims)
+    centers = rng.uniform(-extent, extent, (n_prims, 3))
+    centers[:, 1] = rng.uniform(0.1, 2 * extent, n_prims)
+    mats = S.material_array(n_prims)
+    lam, met, die = r < 0.5, (r >= 0.5) & (r < 0.7), (r >= 0.7) & (r < 0.8)
+    ggx = r >= 0.8
+    mats["kind"] = np.select([lam, met, die, ggx], [abi.MAT_LAMBERTIAN, abi.MAT_METAL, abi.MAT_DIELECTRIC,
+                                                    abi.MAT_MICROFACET])
+    mats["color"] = rng.random((n_prims, 3)) * 0.8 + 0.1
+    mats["color"][met] = 0.5 + 0.5 * rng.random((int(met.sum()), 3))
+    mats["fuzz"] = np.where(met, 0.3 * rng.random(n_prims), 0.0)
+    mats["ior"] = 1.5
+    mats["roughness"] = np.where(ggx, rng.uniform(0.05, 0.7, n_prims), 0.0)
+    mats["metallic"] = np.where(ggx, rng.random(n_prims), 0.0)
+    sz = size * rng.uniform(0.5, 1.5, n_prims)
+    a = rng.normal(size=(n_prims, 3))
+    a /= np.linalg.norm(a, axis=1, keepdims=True)
+    b = rng.normal(size=(n_prims, 3))
+    b -= a * (a * b).sum(1, keepdims=True)
+    b /= np.linalg.norm(b, axis=1, keepdims=True)
+    objs = np.zeros(n_prims, dtype=S.OBJECT_DTYPE)
+    objs["material"] = np.arange(n_prims)
+    objs["transform"] = -1
+    sph, quad, tri = kinds == 0, kinds == 1, kinds == 2
+    objs["kind"] = np.select([sph, quad, tri], [abi.OBJ_SPHERE, abi.OBJ_QUAD, abi.OBJ_TRIANGLE])
+    p = objs["p"]
+    p[sph, 0:3] = centers[sph]
+    p[sph, 3] = sz[sph]
+    s2 = (2 * sz)[:, None]
+    q = centers - sz[:, None] * (a + b)
+    p[quad, 0:3] = q[quad]
+    p[quad, 3:6] = (s2 * a)[quad]
+    p[quad, 6:9] = (s2 * b)[quad]
+    p[tri, 0:3] = centers[tri]
+    p[tri, 3:6] = (centers + s2 * a)[tri]
+    p[tri, 6:9] = (centers + s2 * b)[tri]
+    w.add_bulk(objs, mats)
+    for k in range(int(rng.integers(1, 3))):
+        e = float(rng.uniform(5, 20))
+        if rng.random() < 0.5:
+            c = (float(rng.uniform(-extent, extent)), 3.0 * extent, float(rng.uniform(-extent, extent)))
+            rad = 0.3 * extent
+            w.add(S.Sphere(c, rad, S.Emissive((1, 1, 1), e)))
+            w.add_light(S.LightInfo.Sphere(c, rad, (e, e, e)))
+        else:
+            qq, u, v = (-0.5 * extent, 3.0 * extent, -0.5 * extent), (extent, 0, 0), (0, 0, extent)
+            w.add(S.Quad(qq, u, v, S.Emissive((1, 1, 1), e)))
+            w.add_light(S.LightInfo.Rect(qq, u, v, (0, -1, 0), (e, e, e)))
+    w.camera = S.CameraConfig(look_from=(0.0, 1.5 * extent, 3.5 * extent), look_at=(0, 0.5 * extent, 0),
+                              vfov_degrees=45.0, aspect_ratio=width / height)
+    cfg = S.RenderConfig(width=width, height=height, samples_per_pixel=spp, max_depth=max_depth, seed=seed,
+                         background=abi.BG_SKY)
+    return w, cfg
+
+
+def batched(n_scenes=64, seed=3, res_choices=(128, 256, 512, 1024), spp_choices=(16, 64, 256), min_prims=10,
+            max_prims=50000, max_depth=8):
+    """The batched uneven workload: n_scenes seeded scenes with primitive counts log-uniform in
+    [min_prims, max_prims], square resolutions and spp drawn from the given sets."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_scenes):
+        n = int(round(np.exp(rng.uniform(np.log(min_prims), np.log(max_prims)))))
+        r = int(rng.choice(res_choices))
+        spp = int(rng.choice(spp_choices))
+        out.append(uneven_scene(rng, n, r, r, spp, max_depth=max_depth, seed=31337 + i))
+    return out
+
+
 CONFIGS = {
     "box_room": box_room,
     "random_spheres": random_spheres,

@@ -1,0 +1,103 @@
+"""GPU tests of the batched wavefront tracer (lum_batch_*).
+
+The wavefront traces the same keyed paths as the megakernel (same device functions), so
+each scene's image must equal lum_render's up to the float rounding of the per-pixel sum
+(f32 running sum in the megakernel, 64-bit fixed point in the batch): >= 99% of pixels
+within rtol 1e-5 / atol 1e-6 (a path whose discrete decision flips on a last-bit difference
+may differ), image means within 1e-4 relative.
+"""
+import numpy as np
+import pytest
+
+import luminara_b200 as L
+from luminara_b200 import abi
+from luminara_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def small_batch():
+    rng = np.random.default_rng(11)
+    items = [W.uneven_scene(rng, n, w, h, spp) for n, w, h, spp in
+             [(12, 32, 24, 4), (300, 48, 32, 16), (2000, 40, 40, 9), (50, 24, 24, 64)]]
+    w, c = W.box_room(width=40, height=40, spp=16)
+    items.append((w, c))
+    w, c = W.random_spheres(width=48, height=27, spp=16)
+    w.camera.aspect_ratio = 48 / 27
+    items.append((w, c))
+    w, c = W.dense_mesh(level=4, width=32, height=18, spp=4)
+    w.camera.aspect_ratio = 32 / 18
+    items.append((w, c))
+    return items
+
+
+def compare(img, ref):
+    close = np.abs(img - ref) <= 1e-5 * np.abs(ref) + 1e-6
+    assert close.all(axis=2).mean() >= 0.99, close.all(axis=2).mean()
+    assert np.allclose(img.mean(), ref.mean(), rtol=1e-4, atol=1e-7)
+
+
+@pytest.mark.parametrize("sort_threshold", [0, 1 << 16, 0xFFFFFFFF])
+def test_batch_matches_megakernel(sort_threshold):
+    items = small_batch()
+    scenes = [L.GpuScene(w) for w, _ in items]
+    cfgs = [c for _, c in items]
+    refs = [s.render(c)[0] for s, c in zip(scenes, cfgs)]
+    b = L.Batch(scenes, cfgs, config={"pool_paths": 1 << 16, "block_threads": 128,
+                                      "sort_threshold": sort_threshold, "iters_per_graph": 4})
+    imgs, done, st = b.render()
+    assert st.error_flags == 0
+    assert st.paths == sum(int(np.prod(c.out_shape()[:2])) * int(np.ceil(np.sqrt(c.samples_per_pixel))) ** 2
+                           for c in cfgs)
+    for img, ref in zip(imgs, refs):
+        compare(img, ref)
+    assert all(0 < t <= st.device_ms + 1e-3 for t in done)
+    b.close()
+
+
+def test_batch_is_deterministic_and_refills_a_small_pool():
+    items = small_batch()
+    scenes = [L.GpuScene(w) for w, _ in items]
+    cfgs = [c for _, c in items]
+    b = L.Batch(scenes, cfgs, config={"pool_paths": 4096, "block_threads": 256, "sort_threshold": 1024,
+                                      "iters_per_graph": 8})
+    a, _, st1 = b.render()
+    c, _, st2 = b.render()
+    for x, y in zip(a, c):
+        assert np.array_equal(x, y)
+    assert st1.iterations > 20 and st1.graph_launches >= 3
+    assert st1.segments == st2.segments
+    refs = [s.render(cf)[0] for s, cf in zip(scenes, cfgs)]
+    for img, ref in zip(a, refs):
+        compare(img, ref)
+
+
+def test_batch_device_outputs_and_filters():
+    import torch
+    items = small_batch()[:3]
+    for _, c in items:
+        c.pixel_filter = abi.FILTER_GAUSSIAN
+        c.exposure = 0.5
+    scenes = [L.GpuScene(w) for w, _ in items]
+    cfgs = [c for _, c in items]
+    refs = [s.render(c)[0] for s, c in zip(scenes, cfgs)]
+    outs = [torch.empty(c.out_shape(), dtype=torch.float32, device="cuda") for c in cfgs]
+    b = L.Batch(scenes, cfgs, config="default")
+    b.render_device([o.data_ptr() for o in outs])
+    for o, ref in zip(outs, refs):
+        compare(o.cpu().numpy(), ref)
+
+
+def test_autotuner_picks_and_caches(tmp_path, monkeypatch):
+    monkeypatch.setenv("LUM_AUTOTUNE_CACHE", str(tmp_path / "tune.txt"))
+    items = small_batch()[:4]
+    scenes = [L.GpuScene(w) for w, _ in items]
+    cfgs = [c for _, c in items]
+    cfg, ms = L.autotune(scenes, cfgs)
+    assert ms > 0 and cfg["pool_paths"] in (1 << 19, 1 << 20, 1 << 21) and cfg["block_threads"] in (128, 256)
+    cfg2, ms2 = L.autotune(scenes, cfgs)
+    assert cfg2 == cfg and ms2 == -1.0
+    b = L.Batch(scenes, cfgs)            # autotuned (cache hit)
+    assert b.config() == cfg
+    imgs, _, st = b.render()
+    assert st.error_flags == 0
