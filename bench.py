@@ -54,6 +54,9 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--scenes", type=int, default=64, help="batched workload: number of scenes")
+    ap.add_argument("--max-res", type=int, default=1024, help="batched workload: largest resolution")
+    ap.add_argument("--batch-config", default="auto", help="batched workload: auto | default | k=v,k=v")
     return ap.parse_args()
 
 
@@ -400,16 +403,22 @@ def run_batched(args):
     from luminara_b200 import workloads as W
 
     torch.cuda.set_device(0)
-    items = W.batched()
+    res = tuple(r for r in (128, 256, 512, 1024) if r <= args.max_res)
+    items = W.batched(n_scenes=args.scenes, res_choices=res)
     scenes = [L.GpuScene(w) for w, _ in items]
     cfgs = [c for _, c in items]
     paths = sum(c.out_shape()[0] * c.out_shape()[1] * strata(c) for c in cfgs)
     outs = [torch.empty(c.out_shape(), dtype=torch.float32, device="cuda") for c in cfgs]
     stream = torch.cuda.current_stream()
     t0 = time.perf_counter()
-    tuned, tune_ms = L.autotune(scenes, cfgs)
+    if args.batch_config == "auto":
+        tuned, tune_ms = L.autotune(scenes, cfgs)
+        batch = L.Batch(scenes, cfgs)
+    else:
+        kv = {} if args.batch_config == "default" else dict(x.split("=") for x in args.batch_config.split(","))
+        batch = L.Batch(scenes, cfgs, config=kv or "default")
+        tuned, tune_ms = batch.config(), None
     tune_s = time.perf_counter() - t0
-    batch = L.Batch(scenes, cfgs)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
     def seq():
@@ -449,6 +458,7 @@ def run_batched(args):
         "config": {"workload": f"batched: {len(cfgs)} uneven scenes, {paths} paths per step",
                    "scenes": len(cfgs), "prims": sum(w.n_prims() for w, _ in items),
                    "l2": "working set of the batch exceeds L2 (pool, queues, 64 scenes)"},
+        "batch_mode": "megakernel" if batch.config().get("mode") == 1 else "wavefront",
         "sequential_megakernel": {"value": paths * args.steps / seq_s / 1e6, "unit": "Mpaths/s",
                                   "ms_per_step": seq_s * 1e3 / args.steps},
         "speedup_vs_sequential": seq_s / bat_s,

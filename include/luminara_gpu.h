@@ -355,12 +355,17 @@ lum_status lum_occluded(lum_scene* scene, const lum_ray* rays, uint32_t n, int32
  * Images equal lum_render's up to float rounding of the per-pixel sum (the batch sums in 64-bit
  * fixed point, independent of completion order).
  * ---------------------------------------------------------------------------------- */
+enum {
+    LUM_BATCH_WAVEFRONT = 0,  /* path pool, material-sorted queues, graph-captured iterations */
+    LUM_BATCH_MEGAKERNEL = 1  /* one persistent megakernel whose tile queue spans all scenes */
+};
 typedef struct lum_batch_config {
-    uint32_t pool_paths;      /* path slots in flight (1024 .. 2^24) */
-    uint32_t block_threads;   /* 128 or 256 */
-    uint32_t sort_threshold;  /* extend queues shorter than this shade in one generic kernel */
-    uint32_t iters_per_graph; /* wavefront iterations captured per CUDA graph launch (1 .. 64) */
-    uint32_t reserved[4];
+    uint32_t pool_paths;      /* wavefront: path slots in flight (1024 .. 2^24) */
+    uint32_t block_threads;   /* wavefront: 128 or 256 */
+    uint32_t sort_threshold;  /* wavefront: extend queues shorter than this shade in one generic kernel */
+    uint32_t iters_per_graph; /* wavefront: iterations captured per CUDA graph launch (1 .. 64) */
+    uint32_t mode;            /* LUM_BATCH_* */
+    uint32_t reserved[3];
 } lum_batch_config;
 
 typedef struct lum_batch_stats {
@@ -378,7 +383,7 @@ typedef struct lum_batch_stats {
 typedef struct lum_batch lum_batch; /* opaque; references its scenes, which must outlive it */
 
 lum_status lum_batch_default_config(lum_batch_config* cfg);
-/* Times candidate configurations (pool size, block size, sort threshold) on a calibration
+/* Times candidate configurations (mode; pool size, block size, sort threshold) on a calibration
  * run of the batch (about 1/8 of each scene's strata) and returns the fastest; results are
  * cached per device and batch signature in $LUM_AUTOTUNE_CACHE (default
  * ~/.cache/luminara_b200_autotune.txt).  best_ms may be NULL; it is -1 on a cache hit. */

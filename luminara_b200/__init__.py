@@ -182,7 +182,7 @@ class Batch:
         c = abi.LumBatchConfig()
         check(lib().lum_batch_config_of(self.h, C.byref(c)))
         return {"pool_paths": c.pool_paths, "block_threads": c.block_threads, "sort_threshold": c.sort_threshold,
-                "iters_per_graph": c.iters_per_graph}
+                "iters_per_graph": c.iters_per_graph, "mode": c.mode}
 
     def render(self):
         """Returns (images, per-scene completion ms, lum_batch_stats)."""
@@ -219,7 +219,7 @@ def autotune(scenes, configs):
     ms = C.c_double()
     check(lib().lum_batch_autotune(C.cast(handles, C.POINTER(C.c_void_p)), params, n, C.byref(cfg), C.byref(ms)))
     return ({"pool_paths": cfg.pool_paths, "block_threads": cfg.block_threads, "sort_threshold": cfg.sort_threshold,
-             "iters_per_graph": cfg.iters_per_graph}, ms.value)
+             "iters_per_graph": cfg.iters_per_graph, "mode": cfg.mode}, ms.value)
 
 
 @dataclass

@@ -66,6 +66,9 @@ FILTER_TRIANGLE = 1
 FILTER_GAUSSIAN = 2
 FILTER_MITCHELL = 3
 
+BATCH_WAVEFRONT = 0
+BATCH_MEGAKERNEL = 1
+
 KERR_STACK_OVERFLOW = 1 << 0
 KERR_QUEUE_OVERFLOW = 1 << 1
 KERR_ITERATION_CAP = 1 << 2
@@ -236,7 +239,8 @@ class LumBatchConfig(C.Structure):
         ("block_threads", C.c_uint32),
         ("sort_threshold", C.c_uint32),
         ("iters_per_graph", C.c_uint32),
-        ("reserved", C.c_uint32 * 4),
+        ("mode", C.c_uint32),
+        ("reserved", C.c_uint32 * 3),
     ]
 
 

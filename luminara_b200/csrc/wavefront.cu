@@ -338,6 +338,102 @@ __global__ void k_finalize(Tables T, float* const* outs) {
     }
 }
 
+// Batched megakernel: the megakernel's per-pixel path-regeneration loop (k_render) over a
+// warp-task queue that spans every scene's 8x4 tiles, one persistent launch for the batch.
+// Each scene's image is the f32 per-pixel sum k_render produces for it.
+__global__ void __launch_bounds__(128, 5) k_render_multi(Tables T, const unsigned long long* tile_prefix,
+                                                         float* const* outs, Ctl* ctl, uint32_t* next_task) {
+    extern __shared__ int s_stack[];
+    int* stack = s_stack + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const unsigned long long total = tile_prefix[T.n];
+    uint32_t err = 0, nseg = 0, nsh = 0;
+    for (;;) {
+        uint32_t task = 0;
+        if (lane == 0) task = atomicAdd(next_task, 1u);
+        task = __shfl_sync(kFullMask, task, 0);
+        if (task >= total) break;
+        uint32_t lo = 0, hi = T.n;
+        while (hi - lo > 1) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (tile_prefix[mid] <= task) lo = mid; else hi = mid;
+        }
+        const uint32_t s = lo;
+        const SceneDev S = T.scenes[s];
+        const RenderDev R = T.renders[s];
+        const uint32_t t = task - (uint32_t)tile_prefix[s];
+        const uint32_t i = (t % R.tiles_x) * 8 + (lane & 7);
+        const uint32_t j = (t / R.tiles_x) * 4 + (lane >> 3);
+        const bool valid = i < R.w && j < R.h;
+        const uint32_t gi = i + R.crop_x, gj = j + R.crop_y;
+        const uint32_t pixel = gj * R.full_w + gi;
+        V acc = mk(0.f, 0.f, 0.f);
+        float wsum = 0.0f;
+        uint32_t st = R.s_begin;
+        int state = ST_IDLE;
+        Path P;
+        Pending pend;
+        for (;;) {
+            if (state == ST_IDLE && valid && st < R.s_end) {
+                start_path(S, R, gi, gj, pixel, st, P);
+                ++st;
+                state = R.max_depth > 0 ? ST_CLOSEST : ST_DONE;
+            }
+            if (!__any_sync(kFullMask, state != ST_IDLE)) break;
+            if (state == ST_CLOSEST || state == ST_SHADOW) {
+                const bool shadow = state == ST_SHADOW;
+                Ray r;
+                r.o = P.ray.o;
+                r.d = shadow ? pend.dir : P.ray.d;
+                r.time = shadow ? 0.0f : P.ray.time;
+                Hit h;
+                h.t = shadow ? pend.tmax : CUDART_INF_F;
+                h.prim = -1;
+                h.b1 = h.b2 = 0.0f;
+                const bool found = trace(S, r, 0.001f, shadow, h, stack, err);
+                if (shadow) {
+                    ++nsh;
+                    if (!found) P.L = P.L + pend.contrib;
+                    state = P.bounce >= R.max_depth ? ST_DONE : ST_CLOSEST;
+                } else {
+                    ++nseg;
+                    state = shade(S, R, pixel, P, found, h, pend);
+                }
+            }
+            if (state == ST_DONE) {
+                float lum = 0.2126f * P.L.x + 0.7152f * P.L.y + 0.0722f * P.L.z;
+                V cl = lum > 100.0f ? P.L * (100.0f / lum) : P.L;
+                float w = filter_weight(R.pixel_filter, P.jx - 0.5f, P.jy - 0.5f);
+                acc = fma3(cl, w, acc);
+                wsum += w;
+                state = ST_IDLE;
+            }
+        }
+        if (valid) {
+            V px = wsum > 0.0f ? acc * (1.0f / wsum) : acc;
+            float* o = outs[s] + 3 * ((size_t)j * R.w + i);
+            o[0] = px.x * R.exposure;
+            o[1] = px.y * R.exposure;
+            o[2] = px.z * R.exposure;
+        }
+        if (lane == 0) {
+            unsigned long long k = atomicAdd(T.done_count + s, 1ull) + 1ull;
+            if (k == tile_prefix[s + 1] - tile_prefix[s]) T.finish_ns[s] = globaltimer();
+        }
+    }
+    unsigned long long a = nseg, b = nsh;
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(kFullMask, a, o);
+        b += __shfl_xor_sync(kFullMask, b, o);
+        err |= __shfl_xor_sync(kFullMask, err, o);
+    }
+    if (lane == 0) {
+        atomicAdd(&ctl->segments, a);
+        atomicAdd(&ctl->shadow_rays, b);
+        if (err) atomicOr(&ctl->error_flags, err);
+    }
+}
+
 }  // namespace wf
 }  // namespace lum
 
@@ -392,6 +488,9 @@ struct lum_batch {
     uint32_t* h_done = nullptr;                 // pinned
     int grid_queue = 0, grid_trace = 0, block = 128;
     size_t stack_bytes = 0;
+    unsigned long long* d_tile_prefix = nullptr;   // megakernel mode
+    uint32_t* d_next_task = nullptr;
+    int grid_mega = 0;
 };
 
 namespace {
@@ -427,6 +526,35 @@ lum_status run_batch(lum_batch* b, float* const* d_outs, double* scene_done_ms, 
     c.free_n = b->pool.Q;
     WF(cudaMemcpyAsync(b->ctl, &c, sizeof c, cudaMemcpyHostToDevice, b->stream), "ctl");
     WF(cudaEventRecord(b->ev0, b->stream), "event");
+    if (b->cfg.mode == LUM_BATCH_MEGAKERNEL) {
+        WF(cudaMemsetAsync(b->d_next_task, 0, sizeof(uint32_t), b->stream), "memset");
+        k_init<<<1, 32, 0, b->stream>>>(b->pool, b->ctl);             // t0 only (pool is empty)
+        WF(cudaGraphLaunch(b->exec, b->stream), "cudaGraphLaunch");
+        WF(cudaEventRecord(b->ev1, b->stream), "event");
+        Ctl out{};
+        std::vector<unsigned long long> fin(b->n);
+        WF(cudaMemcpyAsync(&out, b->ctl, sizeof out, cudaMemcpyDeviceToHost, b->stream), "ctl");
+        WF(cudaMemcpyAsync(fin.data(), b->T.finish_ns, sizeof(unsigned long long) * b->n, cudaMemcpyDeviceToHost,
+                           b->stream), "finish");
+        WF(cudaStreamSynchronize(b->stream), "batch");
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+        if (scene_done_ms)
+            for (uint32_t s = 0; s < b->n; ++s)
+                scene_done_ms[s] = fin[s] ? (double)(fin[s] - out.t0_ns) * 1e-6 : -1.0;
+        if (stats) {
+            stats->paths = b->total_work;
+            stats->segments = out.segments;
+            stats->shadow_rays = out.shadow_rays;
+            stats->device_ms = ms;
+            stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            stats->graph_launches = 1;
+            stats->iterations = 1;
+            stats->error_flags = out.error_flags;
+        }
+        if (out.error_flags) return lum::set_error(LUM_ERR_KERNEL, "batched megakernel reported error flags");
+        return LUM_OK;
+    }
     k_init<<<b->grid_queue, b->block, 0, b->stream>>>(b->pool, b->ctl);
     WF(cudaGetLastError(), "init launch");
     // Every graph launch runs iters_per_graph iterations; each pass retires at least one
@@ -514,13 +642,20 @@ lum_status create_batch(lum_scene* const* scenes, const lum_render_params* param
         b->total_pixels += px;
     }
     b->total_work = prefix[n];
-    const uint32_t Q = cfg.pool_paths;
+    const bool mega = cfg.mode == LUM_BATCH_MEGAKERNEL;
+    if (cfg.mode != LUM_BATCH_WAVEFRONT && !mega)
+        return fail_out(lum::set_error(LUM_ERR_INVALID_ARGUMENT, "unknown batch mode"));
+    std::vector<unsigned long long> tile_prefix(n + 1, 0);
+    for (uint32_t s = 0; s < n; ++s)
+        tile_prefix[s + 1] = tile_prefix[s] + ((b->R[s].s_end > b->R[s].s_begin) ? b->R[s].n_tasks : 0);
+    if (tile_prefix[n] > 0xFFFFFFFFull) return fail_out(lum::set_error(LUM_ERR_TOO_LARGE, "too many tiles in batch"));
+    const uint32_t Q = mega ? 1024u : cfg.pool_paths;
     if (Q < 1024 || Q > (1u << 24)) return fail_out(lum::set_error(LUM_ERR_INVALID_ARGUMENT, "pool_paths out of range"));
-    if (cfg.block_threads != 128 && cfg.block_threads != 256)
+    if (!mega && cfg.block_threads != 128 && cfg.block_threads != 256)
         return fail_out(lum::set_error(LUM_ERR_INVALID_ARGUMENT, "block_threads must be 128 or 256"));
-    if (cfg.iters_per_graph < 1 || cfg.iters_per_graph > 64)
+    if (!mega && (cfg.iters_per_graph < 1 || cfg.iters_per_graph > 64))
         return fail_out(lum::set_error(LUM_ERR_INVALID_ARGUMENT, "iters_per_graph out of range"));
-    b->block = (int)cfg.block_threads;
+    b->block = mega ? 128 : (int)cfg.block_threads;
     b->stack_bytes = (size_t)lum::kStackDepth * b->block * sizeof(int);
 
     // one allocation: pool SoA, queues, tables, accumulators, staging images
@@ -540,6 +675,7 @@ lum_status create_batch(lum_scene* const* scenes, const lum_render_params* param
     size_t o_done = take(8ull * n), o_total = take(8ull * n), o_fin = take(8ull * n), o_finit = take(4ull * n);
     size_t o_ctl = take(sizeof(Ctl)), o_outs = take(sizeof(float*) * n);
     size_t o_stage = take(12ull * b->total_pixels);
+    size_t o_tpre = take(8ull * (n + 1)), o_next = take(4);
     cudaError_t e = cudaSetDevice(b->device);
     if (e != cudaSuccess) return fail_out(wf_cuda(e, "cudaSetDevice"));
     if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess ||
@@ -571,11 +707,14 @@ lum_status create_batch(lum_scene* const* scenes, const lum_render_params* param
     b->ctl = (Ctl*)(m + o_ctl);
     b->d_out_table = (float**)(m + o_outs);
     b->d_staging = (float*)(m + o_stage);
+    b->d_tile_prefix = (unsigned long long*)(m + o_tpre);
+    b->d_next_task = (uint32_t*)(m + o_next);
     if ((e = cudaMemcpy(m + o_scenes, S.data(), sizeof(lum::SceneDev) * n, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(m + o_renders, b->R.data(), sizeof(lum::RenderDev) * n, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(m + o_prefix, prefix.data(), 8ull * (n + 1), cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(m + o_accoff, b->acc_off.data(), 8ull * n, cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemcpy(m + o_total, b->scene_total.data(), 8ull * n, cudaMemcpyHostToDevice)) != cudaSuccess)
+        (e = cudaMemcpy(m + o_total, b->scene_total.data(), 8ull * n, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(m + o_tpre, tile_prefix.data(), 8ull * (n + 1), cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail_out(wf_cuda(e, "batch upload"));
 
     // grids: persistent-style, sized to the SM count and the kernels' occupancy
@@ -588,10 +727,23 @@ lum_status create_batch(lum_scene* const* scenes, const lum_render_params* param
     b->grid_queue = sms * std::max(occ_q, 1);
     b->grid_trace = sms * std::max(occ_t, 1);
 
-    // capture iters_per_graph iterations into one graph
+    int occ_m = 0;
+    cudaFuncSetAttribute(k_render_multi, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)((size_t)lum::kStackDepth * 128 * sizeof(int)));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_m, k_render_multi, 128,
+                                                  (size_t)lum::kStackDepth * 128 * sizeof(int));
+    b->grid_mega = sms * std::max(occ_m, 1);
+
+    // capture the batch's kernels into one graph: iters_per_graph wavefront iterations, or
+    // the single persistent megakernel launch
     if ((e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
         return fail_out(wf_cuda(e, "cudaStreamBeginCapture"));
-    for (uint32_t g = 0; g < cfg.iters_per_graph; ++g) enqueue_iteration(b);
+    if (mega) {
+        k_render_multi<<<b->grid_mega, 128, (size_t)lum::kStackDepth * 128 * sizeof(int), b->stream>>>(
+            b->T, b->d_tile_prefix, b->d_out_table, b->ctl, b->d_next_task);
+    } else {
+        for (uint32_t g = 0; g < cfg.iters_per_graph; ++g) enqueue_iteration(b);
+    }
     e = cudaStreamEndCapture(b->stream, &b->graph);
     if (e != cudaSuccess) return fail_out(wf_cuda(e, "cudaStreamEndCapture"));
     if ((e = cudaGraphInstantiate(&b->exec, b->graph, 0)) != cudaSuccess)
@@ -639,12 +791,14 @@ bool tune_lookup(const std::string& key, lum_batch_config& cfg) {
     bool found = false;
     while (fgets(line, sizeof line, f)) {
         char k[384];
-        unsigned q, blk, thr, it;
-        if (sscanf(line, "%383s %u %u %u %u", k, &q, &blk, &thr, &it) == 5 && key == k) {
+        unsigned q, blk, thr, it, mode;
+        if (sscanf(line, "%383s %u %u %u %u %u", k, &q, &blk, &thr, &it, &mode) == 6 && key == k) {
+            std::memset(&cfg, 0, sizeof cfg);
             cfg.pool_paths = q;
             cfg.block_threads = blk;
             cfg.sort_threshold = thr;
             cfg.iters_per_graph = it;
+            cfg.mode = mode;
             found = true;
         }
     }
@@ -658,8 +812,8 @@ void tune_store(const std::string& key, const lum_batch_config& cfg, double ms) 
     if (slash != std::string::npos && slash > 0) mkdir(path.substr(0, slash).c_str(), 0755);   // may exist
     FILE* f = fopen(path.c_str(), "a");
     if (!f) return;
-    fprintf(f, "%s %u %u %u %u %.3f\n", key.c_str(), cfg.pool_paths, cfg.block_threads, cfg.sort_threshold,
-            cfg.iters_per_graph, ms);
+    fprintf(f, "%s %u %u %u %u %u %.3f\n", key.c_str(), cfg.pool_paths, cfg.block_threads, cfg.sort_threshold,
+            cfg.iters_per_graph, cfg.mode, ms);
     fclose(f);
 }
 
@@ -674,6 +828,7 @@ lum_status lum_batch_default_config(lum_batch_config* cfg) {
     cfg->block_threads = 128;
     cfg->sort_threshold = 1u << 16;
     cfg->iters_per_graph = 8;
+    cfg->mode = LUM_BATCH_WAVEFRONT;
     return LUM_OK;
 }
 
@@ -704,8 +859,13 @@ lum_status lum_batch_autotune(lum_scene* const* scenes, const lum_render_params*
     const uint32_t pools[] = {1u << 19, 1u << 20, 1u << 21};
     const uint32_t blocks[] = {128, 256};
     const uint32_t thresholds[] = {0u, 1u << 16, 0xFFFFFFFFu};
-    lum_batch_config best{};
-    double best_t = 1e30;
+    std::vector<lum_batch_config> cands;
+    {
+        lum_batch_config c{};
+        lum_batch_default_config(&c);
+        c.mode = LUM_BATCH_MEGAKERNEL;
+        cands.push_back(c);
+    }
     for (uint32_t q : pools)
         for (uint32_t blk : blocks)
             for (uint32_t thr : thresholds) {
@@ -714,6 +874,14 @@ lum_status lum_batch_autotune(lum_scene* const* scenes, const lum_render_params*
                 c.block_threads = blk;
                 c.sort_threshold = thr;
                 c.iters_per_graph = 8;
+                c.mode = LUM_BATCH_WAVEFRONT;
+                cands.push_back(c);
+            }
+    lum_batch_config best{};
+    double best_t = 1e30;
+    for (const lum_batch_config& cand : cands) {
+            {
+                const lum_batch_config& c = cand;
                 lum_batch* b = nullptr;
                 if (create_batch(scenes, cal.data(), n, c, &b) != LUM_OK) continue;
                 lum_batch_stats st{};
@@ -732,6 +900,7 @@ lum_status lum_batch_autotune(lum_scene* const* scenes, const lum_render_params*
                     best = c;
                 }
             }
+    }
     if (best_t >= 1e30) return lum::set_error(LUM_ERR_CUDA, "autotune: no configuration ran");
     *out = best;
     if (best_ms) *best_ms = best_t;

@@ -72,6 +72,19 @@ def test_batch_is_deterministic_and_refills_a_small_pool():
         compare(img, ref)
 
 
+def test_batched_megakernel_mode_equals_lum_render():
+    items = small_batch()
+    scenes = [L.GpuScene(w) for w, _ in items]
+    cfgs = [c for _, c in items]
+    refs = [s.render(c)[0] for s, c in zip(scenes, cfgs)]
+    b = L.Batch(scenes, cfgs, config={"mode": abi.BATCH_MEGAKERNEL})
+    imgs, done, st = b.render()
+    assert st.error_flags == 0 and st.segments > 0
+    for img, ref in zip(imgs, refs):
+        np.testing.assert_allclose(img, ref, rtol=1e-6, atol=1e-7)
+    assert all(0 < t <= st.device_ms + 1e-3 for t in done)
+
+
 def test_batch_device_outputs_and_filters():
     import torch
     items = small_batch()[:3]
@@ -94,7 +107,8 @@ def test_autotuner_picks_and_caches(tmp_path, monkeypatch):
     scenes = [L.GpuScene(w) for w, _ in items]
     cfgs = [c for _, c in items]
     cfg, ms = L.autotune(scenes, cfgs)
-    assert ms > 0 and cfg["pool_paths"] in (1 << 19, 1 << 20, 1 << 21) and cfg["block_threads"] in (128, 256)
+    assert ms > 0 and cfg["mode"] in (abi.BATCH_WAVEFRONT, abi.BATCH_MEGAKERNEL)
+    assert cfg["mode"] == abi.BATCH_MEGAKERNEL or cfg["pool_paths"] in (1 << 19, 1 << 20, 1 << 21)
     cfg2, ms2 = L.autotune(scenes, cfgs)
     assert cfg2 == cfg and ms2 == -1.0
     b = L.Batch(scenes, cfgs)            # autotuned (cache hit)
