@@ -347,6 +347,26 @@ lum_status lum_intersect(lum_scene* scene, const lum_ray* rays, uint32_t n, lum_
 lum_status lum_occluded(lum_scene* scene, const lum_ray* rays, uint32_t n, int32_t* occluded);
 
 /* ------------------------------------------------------------------------------------
+ * Differentiable rendering: a forward/backward pair.  No counterpart in the reference (it
+ * renders only); the estimator differentiated is the reference's (render.rs:1472-1537).
+ * ---------------------------------------------------------------------------------- */
+
+/* The forward render (same as lum_render). */
+lum_status lum_forward(lum_scene* scene, const lum_render_params* params, float* out_rgb, lum_stats* stats);
+
+/* Path-replay adjoint: given dL/d(image) (HOST, W*H*3 floats, the layout lum_forward
+ * returns), writes dL/d(albedo) (3 per material: Lambertian/Metal/Microfacet colour),
+ * dL/d(roughness) (1 per material: Microfacet) and dL/d(emission) (3 per material: the
+ * Emissive colour * intensity) into HOST arrays sized by the scene's material count.
+ * light_material[k] names the material whose emission light k carries (NEE), or -1; NULL =
+ * none.  Each path is re-traced from its RNG key (no path storage).  Russian roulette and the
+ * microfacet lobe choice are treated as constants (unbiased); visibility changes are not
+ * differentiated.  max_depth <= 16. */
+lum_status lum_backward(lum_scene* scene, const lum_render_params* params, const float* dL_dimage,
+                        const int32_t* light_material, float* d_albedo, float* d_roughness, float* d_emission,
+                        lum_stats* stats);
+
+/* ------------------------------------------------------------------------------------
  * Batched wavefront rendering: many scenes per launch sequence.
  *
  * The reference renders one scene per render() call (src/render.rs:1557); a batch is the

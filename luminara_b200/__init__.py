@@ -64,6 +64,8 @@ def lib():
     L.lum_render.argtypes = [vp, C.POINTER(abi.LumRenderParams), vp, C.POINTER(abi.LumStats)]
     L.lum_render_device.argtypes = [vp, C.POINTER(abi.LumRenderParams), vp, vp, C.POINTER(abi.LumStats)]
     L.lum_count_tests.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.POINTER(abi.LumTestCounts)]
+    L.lum_forward.argtypes = [vp, C.POINTER(abi.LumRenderParams), vp, C.POINTER(abi.LumStats)]
+    L.lum_backward.argtypes = [vp, C.POINTER(abi.LumRenderParams), vp, vp, vp, vp, vp, C.POINTER(abi.LumStats)]
     L.lum_intersect.argtypes = [vp, vp, C.c_uint32, vp]
     L.lum_occluded.argtypes = [vp, vp, C.c_uint32, vp]
     PP = C.POINTER(C.c_void_p)
@@ -77,7 +79,8 @@ def lib():
     L.lum_batch_render_device.argtypes = [vp, PP, C.POINTER(C.c_double), C.POINTER(abi.LumBatchStats)]
     L.lum_batch_destroy.argtypes = [vp]
     for name in ("lum_scene_create", "lum_scene_destroy", "lum_scene_info", "lum_render", "lum_render_device",
-                 "lum_count_tests", "lum_intersect", "lum_occluded", "lum_batch_default_config",
+                 "lum_count_tests", "lum_intersect", "lum_occluded", "lum_forward", "lum_backward",
+                 "lum_batch_default_config",
                  "lum_batch_autotune", "lum_batch_create", "lum_batch_config_of", "lum_batch_render",
                  "lum_batch_render_device", "lum_batch_destroy"):
         getattr(L, name).restype = C.c_int32
@@ -131,6 +134,32 @@ class GpuScene:
         st = abi.LumStats()
         check(lib().lum_render_device(self.h, C.byref(p), C.c_void_p(d_out), C.c_void_p(stream), C.byref(st)))
         return st
+
+    def forward(self, cfg: RenderConfig):
+        """lum_forward: the image (H, W, 3) and stats."""
+        p = cfg.to_c()
+        out = np.empty(cfg.out_shape(), dtype=np.float32)
+        st = abi.LumStats()
+        check(lib().lum_forward(self.h, C.byref(p), out.ctypes.data, C.byref(st)))
+        return out, st
+
+    def backward(self, cfg: RenderConfig, dl_dimage: np.ndarray, light_material=None):
+        """lum_backward: gradients of the loss w.r.t. per-material albedo (n, 3), roughness
+        (n,) and emission (n, 3), given dL/d(image) of shape (H, W, 3)."""
+        p = cfg.to_c()
+        g = np.ascontiguousarray(dl_dimage, dtype=np.float32)
+        assert g.shape == cfg.out_shape()
+        n = self.desc.n_materials
+        da = np.zeros((n, 3), np.float32)
+        dr = np.zeros(n, np.float32)
+        de = np.zeros((n, 3), np.float32)
+        lm = None
+        if light_material is not None:
+            lm = np.ascontiguousarray(light_material, dtype=np.int32)
+        st = abi.LumStats()
+        check(lib().lum_backward(self.h, C.byref(p), g.ctypes.data, lm.ctypes.data if lm is not None else None,
+                                 da.ctypes.data, dr.ctypes.data, de.ctypes.data, C.byref(st)))
+        return da, dr, de, st
 
     def count_tests(self, cfg: RenderConfig) -> abi.LumTestCounts:
         """Node/primitive test counts of this render (counter build of the render kernel)."""

@@ -343,6 +343,7 @@ class World:
         self.materials: List[Material] = []
         self._mat_index = {}
         self._bulk = []          # (insert position in objects, object array, material array)
+        self.light_materials: List[Optional[Material]] = []
         self.camera = CameraConfig()
 
     def add_bulk(self, objects: np.ndarray, materials: np.ndarray) -> int:
@@ -375,8 +376,14 @@ class World:
             self.material_index(mesh.material)
         return first
 
-    def add_light(self, light: LightInfo) -> None:
+    def add_light(self, light: LightInfo, material: Optional[Material] = None) -> None:
+        """Adds an NEE light; `material` is the emissive material whose emission it carries
+        (used by the adjoint to route light-emission gradients)."""
         self.lights.append(light)
+        self.light_materials.append(material)
+
+    def light_material_indices(self):
+        return [self.material_index(m) if m is not None else -1 for m in self.light_materials]
 
     def n_prims(self) -> int:
         n = sum(6 if o.kind == abi.OBJ_BOX else 1 for o in self.objects)

@@ -184,12 +184,13 @@ def diff_quads(width=512, height=512, spp=64, max_depth=6, seed=31337, scene_see
         w.add(S.Quad(tuple(q), tuple(su * a), tuple(sv * b), m))
     for k in range(4):
         x, z = (-3 + 6 * (k % 2)), (-3 + 6 * (k // 2))
-        e = float(rng.uniform(4.0, 8.0))
-        q, u, v = (x - 1.0, 6.0, z - 1.0), (2.0, 0, 0), (0, 0, 2.0)
-        w.add(S.Quad(q, u, v, S.Emissive((1.0, 1.0, 1.0), e)))
+        e = float(rng.uniform(15.0, 30.0))
+        q, u, v = (x - 1.5, 6.0, z - 1.5), (3.0, 0, 0), (0, 0, 3.0)
+        em = S.Emissive((1.0, 1.0, 1.0), e)
+        w.add(S.Quad(q, u, v, em))
         nrm = np.cross(u, v)
         nrm = nrm / np.linalg.norm(nrm)
-        w.add_light(S.LightInfo.Rect(q, u, v, tuple(nrm), (e, e, e)))
+        w.add_light(S.LightInfo.Rect(q, u, v, tuple(nrm), (e, e, e)), material=em)
     w.camera = S.CameraConfig(look_from=(0, 2, 14), look_at=(0, 0, 0), vfov_degrees=40.0,
                               aspect_ratio=width / height)
     cfg = S.RenderConfig(width=width, height=height, samples_per_pixel=spp, max_depth=max_depth, seed=seed,

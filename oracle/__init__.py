@@ -62,6 +62,7 @@ def lib():
         L.orc_render.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.c_int, C.c_int, dp, C.POINTER(OrcStats)]
         L.orc_render_rows.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.c_int, C.c_int, C.c_uint32,
                                       C.c_uint32, dp, C.POINTER(OrcStats)]
+        L.orc_adjoint.argtypes = [vp, C.POINTER(abi.LumRenderParams), dp, vp, C.c_int, C.c_int, dp, dp, dp, dp]
         L.orc_scatter.argtypes = [C.POINTER(abi.LumMaterial), dp, dp, dp, C.c_double, C.c_double, C.c_double,
                                   C.c_uint64, C.c_int, dp]
         L.orc_schlick.argtypes = [C.c_double, C.c_double]
@@ -139,6 +140,24 @@ class OracleScene:
         if rc != 0:
             raise RuntimeError(f"orc_render failed: {rc}")
         return out, st
+
+    def adjoint(self, cfg, dl_dimage, light_material=None, detach=True, threads=0):
+        """f64 adjoint of the keyed estimator: (d_albedo (n,3), d_roughness (n,), d_emission (n,3),
+        primal image)."""
+        p = cfg.to_c()
+        g = np.ascontiguousarray(dl_dimage, dtype=np.float64)
+        assert g.shape == cfg.out_shape()
+        n = self.desc.n_materials
+        da, dr, de = np.zeros((n, 3)), np.zeros(n), np.zeros((n, 3))
+        img = np.zeros(cfg.out_shape())
+        lm = None if light_material is None else np.ascontiguousarray(light_material, dtype=np.int32)
+        dp_ = C.POINTER(C.c_double)
+        rc = lib().orc_adjoint(self.h, C.byref(p), g.ctypes.data_as(dp_), lm.ctypes.data if lm is not None else None,
+                               1 if detach else 0, threads, da.ctypes.data_as(dp_), dr.ctypes.data_as(dp_),
+                               de.ctypes.data_as(dp_), img.ctypes.data_as(dp_))
+        if rc != 0:
+            raise RuntimeError(f"orc_adjoint failed: {rc}")
+        return da, dr, de, img
 
     def sample_direct_light(self, p, n, albedo, seed, n_iter):
         out = np.zeros((n_iter, 3))

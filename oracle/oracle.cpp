@@ -261,6 +261,7 @@ struct HitRecord {
     const Material* mat = nullptr;
     int32_t prim_id = -1;
     int32_t mat_index = -1;
+    bool flat = false;   // planar primitive (used by the adjoint's hit-point derivative)
 };
 // hit.rs:19-43
 inline void set_face(HitRecord& h, const Ray& r, V3 outward) {
@@ -470,10 +471,12 @@ struct Leaf : Hittable {
     const Material* mat = nullptr;
     int32_t prim_id = -1;
     int32_t mat_index = -1;
+    bool flat = false;
     void tag(HitRecord& h) const {
         h.mat = mat;
         h.prim_id = prim_id;
         h.mat_index = mat_index;
+        h.flat = flat;
     }
 };
 
@@ -547,6 +550,7 @@ struct MovingSphere : Leaf {                                            // spher
 };
 
 struct Quad : Leaf {                                                    // quad.rs:20-72
+    Quad() { flat = true; }
     V3 q, u, v, n, w;
     double d;
     void init() {
@@ -583,6 +587,7 @@ struct Quad : Leaf {                                                    // quad.
 
 // rect.rs:7-125: axis 0 = XY (z=k), 1 = XZ (y=k), 2 = YZ (x=k).
 struct AxisRect : Leaf {
+    AxisRect() { flat = true; }
     int plane;
     double a0, a1, b0, b1, k;
     bool hit(const Ray& ray, double tmin, double tmax, HitRecord& rec) const override {
@@ -614,6 +619,7 @@ struct AxisRect : Leaf {
 };
 
 struct Triangle : Leaf {                       // triangle.rs:21-64, obj.rs:259-313
+    Triangle() { flat = true; }
     V3 v0, v1, v2;
     bool has_normals = false;
     V3 n0, n1, n2;
@@ -648,6 +654,7 @@ struct Triangle : Leaf {                       // triangle.rs:21-64, obj.rs:259-
 };
 
 struct Disk : Leaf {                                                    // disk.rs:16-65
+    Disk() { flat = true; }
     V3 c, n;
     double r;
     bool hit(const Ray& ray, double tmin, double tmax, HitRecord& rec) const override {
@@ -676,6 +683,7 @@ struct Disk : Leaf {                                                    // disk.
 };
 
 struct Plane : Leaf {                                                   // plane.rs:18-74
+    Plane() { flat = true; }
     V3 p0, n, ua, va;
     void init(V3 point, V3 normal) {
         p0 = point;
@@ -1757,6 +1765,395 @@ void orc_xoshiro_from_state(const uint64_t state[4], uint32_t n, uint64_t* out) 
 void orc_seed_state(uint64_t seed, uint64_t out[4]) {
     Xoshiro r(seed);
     for (int i = 0; i < 4; ++i) out[i] = r.s[i];
+}
+
+}  // extern "C"
+
+// =======================================================================================
+// f64 adjoint of the keyed estimator (the checker for the device's lum_backward).
+//
+// Forward-mode dual numbers over groups of 16 material parameters at a time.  Each
+// path is re-traced in f64 and the primal values take every branch (Russian roulette, the
+// microfacet lobe, the primitive hit, shadow visibility), so the result is the derivative of
+// the estimator with those decisions held.  With detach = 1 the Russian-roulette survival and
+// the microfacet lobe probability are constants (the device adjoint's estimator: the terms
+// their derivatives add have zero mean); detach = 0 keeps them, which is the plain derivative
+// of the per-sample image and is what a tiny-step finite difference of orc_render measures.
+// The hit point moves on the tangent plane of a flat primitive and is held on curved ones;
+// shading normals are constant.  Parameters: albedo of Lambertian / Metal / Microfacet (the
+// texel used), Microfacet roughness, and emission (colour * intensity) of Emissive materials
+// and of the NEE lights that carry them (light_material).  Metal, Dielectric and Isotropic
+// scatter directions, and sphere-light NEE terms as functions of the shading point, are held.
+// =======================================================================================
+namespace {
+
+constexpr int ND = 16;
+struct Dd {
+    double v = 0.0;
+    double d[ND] = {};
+};
+inline Dd dcst(double x) {
+    Dd r;
+    r.v = x;
+    return r;
+}
+inline Dd operator+(const Dd& a, const Dd& b) {
+    Dd r;
+    r.v = a.v + b.v;
+    for (int k = 0; k < ND; ++k) r.d[k] = a.d[k] + b.d[k];
+    return r;
+}
+inline Dd operator-(const Dd& a, const Dd& b) {
+    Dd r;
+    r.v = a.v - b.v;
+    for (int k = 0; k < ND; ++k) r.d[k] = a.d[k] - b.d[k];
+    return r;
+}
+inline Dd operator-(const Dd& a) {
+    Dd r;
+    r.v = -a.v;
+    for (int k = 0; k < ND; ++k) r.d[k] = -a.d[k];
+    return r;
+}
+inline Dd operator*(const Dd& a, const Dd& b) {
+    Dd r;
+    r.v = a.v * b.v;
+    for (int k = 0; k < ND; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k];
+    return r;
+}
+inline Dd operator*(const Dd& a, double s) {
+    Dd r;
+    r.v = a.v * s;
+    for (int k = 0; k < ND; ++k) r.d[k] = a.d[k] * s;
+    return r;
+}
+inline Dd operator*(double s, const Dd& a) { return a * s; }
+inline Dd operator+(const Dd& a, double s) {
+    Dd r = a;
+    r.v += s;
+    return r;
+}
+inline Dd operator+(double s, const Dd& a) { return a + s; }
+inline Dd operator-(const Dd& a, double s) { return a + (-s); }
+inline Dd operator-(double s, const Dd& a) { return (-a) + s; }
+inline Dd operator/(const Dd& a, const Dd& b) {
+    Dd r;
+    r.v = a.v / b.v;
+    for (int k = 0; k < ND; ++k) r.d[k] = (a.d[k] - r.v * b.d[k]) / b.v;
+    return r;
+}
+inline Dd operator/(const Dd& a, double s) { return a * (1.0 / s); }
+inline Dd operator/(double s, const Dd& b) { return dcst(s) / b; }
+inline Dd dsqrt(const Dd& a) {
+    Dd r;
+    r.v = std::sqrt(a.v);
+    double h = r.v > 0.0 ? 0.5 / r.v : 0.0;
+    for (int k = 0; k < ND; ++k) r.d[k] = a.d[k] * h;
+    return r;
+}
+inline Dd dmax(const Dd& a, double lo) { return a.v >= lo ? a : dcst(lo); }
+inline Dd dclamp(const Dd& a, double lo, double hi) { return a.v < lo ? dcst(lo) : (a.v > hi ? dcst(hi) : a); }
+inline Dd dabs(const Dd& a) { return a.v >= 0.0 ? a : -a; }
+inline Dd dmax3(const Dd& a, const Dd& b, const Dd& c) {
+    const Dd& m = a.v >= b.v ? a : b;
+    return m.v >= c.v ? m : c;
+}
+
+struct DV {
+    Dd x, y, z;
+};
+inline DV dv(V3 a) { return {dcst(a.x), dcst(a.y), dcst(a.z)}; }
+inline V3 val(const DV& a) { return {a.x.v, a.y.v, a.z.v}; }
+inline DV operator+(const DV& a, const DV& b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline DV operator-(const DV& a, const DV& b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline DV operator-(const DV& a) { return {-a.x, -a.y, -a.z}; }
+inline DV operator*(const DV& a, const Dd& s) { return {a.x * s, a.y * s, a.z * s}; }
+inline DV operator*(const DV& a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+inline DV operator*(V3 a, const Dd& s) { return {s * a.x, s * a.y, s * a.z}; }
+inline DV had(const DV& a, const DV& b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+inline Dd ddot(const DV& a, const DV& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline Dd ddot(V3 a, const DV& b) { return b.x * a.x + b.y * a.y + b.z * a.z; }
+inline DV dunit(const DV& a) { return a * (1.0 / dsqrt(ddot(a, a))); }
+inline bool dnan(const DV& a) { return std::isnan(a.x.v) || std::isnan(a.y.v) || std::isnan(a.z.v); }
+
+// Parameter layout: albedo 3*m+c, roughness 3*n+m, emission 4*n+3*m+c (n materials).
+struct AdjCtx {
+    const orc_scene* sc;
+    const lum_render_params* p;
+    const int32_t* light_mat;
+    int n_mat;
+    int begin;
+    bool detach;
+    Dd param(double v, int idx) const {
+        Dd r = dcst(v);
+        int k = idx - begin;
+        if (k >= 0 && k < ND) r.d[k] = 1.0;
+        return r;
+    }
+    DV albedo(int m, V3 a) const { return {param(a.x, 3 * m), param(a.y, 3 * m + 1), param(a.z, 3 * m + 2)}; }
+    Dd rough(int m, double r) const { return param(r, 3 * n_mat + m); }
+    DV emission(int m, V3 e) const {
+        if (m < 0) return dv(e);
+        return {param(e.x, 4 * n_mat + 3 * m), param(e.y, 4 * n_mat + 3 * m + 1), param(e.z, 4 * n_mat + 3 * m + 2)};
+    }
+};
+
+inline DV dfresnel(const Dd& cos_theta, const DV& f0) {                // material.rs:291-294
+    Dd m = dmax(1.0 - cos_theta, 0.0);
+    Dd t = m * m * m * m * m;
+    return {f0.x * (1.0 - t) + t, f0.y * (1.0 - t) + t, f0.z * (1.0 - t) + t};
+}
+
+// Attenuation and outgoing direction of a scatter whose primal outcome is `sc` (material.rs).
+void scatter_dual(const AdjCtx& C, const Material& m, int mi, const HitRecord& h, const DV& d_in, Sampler& s,
+                  const Scatter& sc, DV& att, DV& dir) {
+    dir = dv(sc.ray.d);
+    switch (m.kind) {
+        case LUM_MAT_LAMBERTIAN:
+            att = C.albedo(mi, m.tex.value(h.u, h.v, h.p));
+            return;
+        case LUM_MAT_METAL:
+            att = C.albedo(mi, m.albedo);
+            return;
+        case LUM_MAT_MICROFACET: {                                     // material.rs:328-390
+            V3 n = h.n;
+            DV alb = C.albedo(mi, m.tex.value(h.u, h.v, h.p));
+            Dd rr = C.rough(mi, m.roughness);
+            DV v = dunit(-d_in);
+            Dd ndv = dmax(ddot(n, v), 0.001);
+            DV f0 = DV{dcst(0.04 * (1.0 - m.metallic)), dcst(0.04 * (1.0 - m.metallic)), dcst(0.04 * (1.0 - m.metallic))} +
+                    alb * m.metallic;
+            DV fw = dfresnel(ndv, f0);
+            Dd sp = dclamp((fw.x + fw.y + fw.z) / 3.0, 0.1, 0.9);
+            if (C.detach) sp = dcst(sp.v);
+            if (s.draw(CALL_SCATTER, 0) < sp.v) {
+                double r1 = s.draw(CALL_SCATTER, 1), r2 = s.draw(CALL_SCATTER, 2);
+                Dd alpha = rr * rr;
+                Dd tan2 = alpha * alpha * (r1 / (1.0 - r1 + 1e-10));     // tan^2 of atan(...) (material.rs:297-319)
+                Dd ct = 1.0 / dsqrt(1.0 + tan2);
+                Dd st = dsqrt(tan2) * ct;
+                double phi = 2.0 * PI * r2;
+                V3 up = std::fabs(n.y) < 0.999 ? v3(0, 1, 0) : v3(1, 0, 0);
+                V3 tg = unit(cross(up, n));
+                V3 bt = cross(n, tg);
+                DV hh = dunit(tg * (st * std::cos(phi)) + bt * (st * std::sin(phi)) + n * ct);
+                Dd vh = ddot(v, hh);
+                dir = hh * (vh * 2.0) - v;
+                Dd ndl = ddot(n, dir);
+                Dd ndh = dmax(ddot(n, hh), 0.0);
+                Dd vdh = dmax(vh, 0.0);
+                Dd k = (rr + 1.0) * (rr + 1.0) / 8.0;                    // material.rs:280-288
+                Dd g = (ndv / (ndv * (1.0 - k) + k)) * (ndl / (ndl * (1.0 - k) + k));
+                DV f = dfresnel(vdh, f0);
+                if (ndh.v > 0.001) {
+                    Dd c = g * vdh / (ndv * ndh) / sp;
+                    att = f * c;
+                } else {
+                    att = dv(v3(0, 0, 0));
+                }
+                return;
+            }
+            DV kd = DV{1.0 - fw.x, 1.0 - fw.y, 1.0 - fw.z} * (1.0 - m.metallic);
+            att = had(kd, alb) * (1.0 / (1.0 - sp));
+            return;
+        }
+        default:
+            att = dv(sc.att);
+            return;
+    }
+}
+
+// render.rs:1346-1466 with the shading point as a dual; the light point, visibility and the
+// early-outs come from the primal.
+DV nee_dual(const AdjCtx& C, const DV& hp, V3 normal, const DV& att, Sampler& s, Counters& cnt) {
+    const orc_scene& sc = *C.sc;
+    const auto& lights = sc.lights;
+    V3 hv = val(hp);
+    V3 prim = sample_direct_light(sc, hv, normal, val(att), s, cnt);
+    if (prim.x == 0.0 && prim.y == 0.0 && prim.z == 0.0) return dv(v3(0, 0, 0));
+    uint64_t idx = as_usize(s.draw(CALL_NEE, 1) * (double)lights.size());
+    idx = std::min<uint64_t>(idx, lights.size() - 1);
+    const Light& L = lights[idx];
+    DV em = C.emission(C.light_mat ? C.light_mat[idx] : -1, L.e);
+    if (L.kind == LUM_LIGHT_SPHERE) {
+        // held constant in the shading point: the primal factor prim / (em * att)
+        V3 a = val(att);
+        double gx = em.x.v * a.x != 0.0 ? prim.x / (em.x.v * a.x) : 0.0;
+        double gy = em.y.v * a.y != 0.0 ? prim.y / (em.y.v * a.y) : 0.0;
+        double gz = em.z.v * a.z != 0.0 ? prim.z / (em.z.v * a.z) : 0.0;
+        DV ea = had(em, att);
+        return {ea.x * gx, ea.y * gy, ea.z * gz};
+    }
+    V3 lp;
+    double area;
+    if (L.kind == LUM_LIGHT_RECT) {
+        double a = s.draw(CALL_NEE, 2), b = s.draw(CALL_NEE, 3);
+        lp = L.p0 + L.u * a + L.v * b;
+        area = length(cross(L.u, L.v));
+    } else {
+        double r1 = s.draw(CALL_NEE, 2), r2 = s.draw(CALL_NEE, 3);
+        double r = std::sqrt(r1) * L.r;
+        double th = 2.0 * PI * r2;
+        V3 w = L.n;
+        V3 av = std::fabs(w.x) > 0.9 ? v3(0, 1, 0) : v3(1, 0, 0);
+        V3 ut = unit(cross(w, av));
+        V3 vt = cross(w, ut);
+        lp = L.p0 + ut * (r * std::cos(th)) + vt * (r * std::sin(th));
+        area = PI * L.r * L.r;
+    }
+    DV tl = dv(lp) - hp;
+    Dd d2 = ddot(tl, tl);
+    Dd dist = dsqrt(d2);
+    DV dir = tl * (1.0 / dist);
+    Dd ct = ddot(normal, dir);
+    Dd ctl = dabs(ddot(-L.n, dir));
+    Dd gterm = ct * ctl * (area * (double)lights.size() / PI) / d2;
+    return had(em, att) * gterm;
+}
+
+// One keyed path (ray_color_keyed above) with dual radiance.
+DV path_dual(const AdjCtx& C, Ray r, Sampler& s, uint32_t max_depth, Counters& cnt) {
+    const orc_scene& sc = *C.sc;
+    DV L = dv(v3(0, 0, 0)), B = dv(v3(1, 1, 1));
+    DV o = dv(r.o), d = dv(r.d);
+    bool skip = false;
+    for (uint32_t b = 0; b < max_depth; ++b) {
+        uint32_t depth = max_depth - b;
+        s.begin_bounce(b);
+        HitRecord h;
+        cnt.segments++;
+        if (!sc.hit(r, 0.001, INF, h)) {
+            L = L + had(B, dv(background(*C.p, r)));
+            break;
+        }
+        if (!std::isfinite(h.p.x) || !std::isfinite(h.p.y) || !std::isfinite(h.p.z)) break;
+        DV P = dv(h.p);
+        if (h.flat) {                     // intersection with the hit primitive's plane
+            Dd nd = ddot(h.n, d);
+            if (std::fabs(nd.v) > 1e-12) {
+                Dd t = ddot(h.n, dv(h.p) - o) / nd;
+                P = o + d * t;
+                P.x.v = h.p.x;
+                P.y.v = h.p.y;
+                P.z.v = h.p.z;
+            }
+        }
+        DV e = dv(v3(0, 0, 0));
+        if (!skip && h.mat && h.mat->kind == LUM_MAT_EMISSIVE) e = C.emission(h.mat_index, h.mat->emitted(h.u, h.v, h.p));
+        Scatter scat;
+        if (!h.mat || !h.mat->scatter(r, h, s, scat)) {
+            L = L + had(B, e);
+            break;
+        }
+        double dl2 = length_squared(scat.ray.d);
+        if (!(dl2 > 0.0) || !std::isfinite(dl2)) {
+            L = L + had(B, e);
+            break;
+        }
+        DV att, dir;
+        scatter_dual(C, *h.mat, h.mat_index, h, d, s, scat, att, dir);
+        double mc = std::fmax(std::fmax(scat.att.x, scat.att.y), scat.att.z);
+        double surv = rclamp(mc, 0.05, 1.0);
+        if (depth < 47 && s.draw(CALL_NEE, 0) > surv) {
+            L = L + had(B, e);
+            break;
+        }
+        Dd rrw = dcst(1.0);
+        if (depth < 47) rrw = C.detach ? dcst(1.0 / surv) : 1.0 / dclamp(dmax3(att.x, att.y, att.z), 0.05, 1.0);
+        bool use_nee = !h.mat->is_specular() && !sc.lights.empty();
+        DV dl = use_nee ? nee_dual(C, P, h.n, att, s, cnt) : dv(v3(0, 0, 0));
+        DV term = e + dl;
+        DV nb = had(B, att) * rrw;
+        if (dnan(term) || dnan(nb)) break;
+        L = L + had(B, term);
+        B = nb;
+        skip = use_nee;
+        r = scat.ray;
+        o = P;
+        d = dir;
+    }
+    return L;
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_adjoint(const orc_scene* sc, const lum_render_params* pp, const double* dl_dimage, const int32_t* light_material,
+                int detach, int threads, double* d_albedo, double* d_roughness, double* d_emission, double* out_rgb) {
+    if (!sc || !pp || !dl_dimage || !d_albedo || !d_roughness || !d_emission) return 1;
+    const lum_render_params& p = *pp;
+    Frame f = frame_of(p);
+    const int n_mat = (int)sc->mats.size();
+    const int n_par = 7 * n_mat;
+    std::vector<double> grad((size_t)n_par, 0.0);
+#ifdef _OPENMP
+    int nt = threads > 0 ? threads : omp_get_max_threads();
+#else
+    int nt = 1;
+    (void)threads;
+#endif
+    for (int begin = 0; begin < std::max(n_par, 1); begin += ND) {
+        AdjCtx C{sc, pp, light_material, n_mat, begin, detach != 0};
+        const bool write_img = out_rgb && begin == 0;
+#pragma omp parallel num_threads(nt)
+        {
+            double gl[ND] = {};
+#pragma omp for schedule(dynamic, 1)
+            for (int64_t j = 0; j < (int64_t)f.h; ++j) {
+                size_t gj = (size_t)j + f.crop_y;
+                Sampler s;
+                s.mode = ORC_MODE_KEYED;
+                s.stream = nullptr;
+                s.key[0] = (uint32_t)p.seed;
+                s.key[1] = (uint32_t)(p.seed >> 32);
+                double y = (double)(f.full_h - 1 - gj);
+                Counters cnt;
+                for (size_t i = 0; i < f.w; ++i) {
+                    size_t gi = i + f.crop_x;
+                    DV color = dv(v3(0, 0, 0));
+                    double tw = 0.0;
+                    s.pixel = (uint32_t)(gj * f.full_w + gi);
+                    for (uint32_t st = f.s_begin; st < f.s_end; ++st) {
+                        uint32_t sx = st % f.sqrt_spp, sy = st / f.sqrt_spp;
+                        s.stratum = st;
+                        s.begin_bounce(0);
+                        double jx = ((double)sx + s.draw(CALL_CAMERA, 0)) / (double)f.sqrt_spp;
+                        double jy = ((double)sy + s.draw(CALL_CAMERA, 1)) / (double)f.sqrt_spp;
+                        double uc = ((double)gi + jx) / (double)(f.full_w - 1);
+                        double vc = (y + jy) / (double)(f.full_h - 1);
+                        Ray ray = sc->cam.get_ray(uc, vc, s);
+                        DV smp = path_dual(C, ray, s, p.max_depth, cnt);
+                        Dd lum = 0.2126 * smp.x + 0.7152 * smp.y + 0.0722 * smp.z;   // render.rs:1692-1697
+                        DV cl = lum.v > 100.0 ? smp * (100.0 / lum) : smp;
+                        double w = filter_weight(p.pixel_filter, jx - 0.5, jy - 0.5);
+                        color = color + cl * w;
+                        tw += w;
+                    }
+                    DV px = tw > 0.0 ? color * (1.0 / tw) : color;
+                    const double* g = dl_dimage + ((size_t)j * f.w + i) * 3;
+                    for (int k = 0; k < ND; ++k)
+                        gl[k] += p.exposure * (g[0] * px.x.d[k] + g[1] * px.y.d[k] + g[2] * px.z.d[k]);
+                    if (write_img) {
+                        double* o = out_rgb + ((size_t)j * f.w + i) * 3;
+                        o[0] = px.x.v * p.exposure;
+                        o[1] = px.y.v * p.exposure;
+                        o[2] = px.z.v * p.exposure;
+                    }
+                }
+            }
+#pragma omp critical
+            for (int k = 0; k < ND && begin + k < n_par; ++k) grad[(size_t)begin + k] += gl[k];
+        }
+    }
+    for (int m = 0; m < n_mat; ++m) {
+        for (int c = 0; c < 3; ++c) {
+            d_albedo[3 * m + c] = grad[(size_t)3 * m + c];
+            d_emission[3 * m + c] = grad[(size_t)4 * n_mat + 3 * m + c];
+        }
+        d_roughness[m] = grad[(size_t)3 * n_mat + m];
+    }
+    return 0;
 }
 
 }  // extern "C"

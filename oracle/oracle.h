@@ -91,6 +91,14 @@ void orc_reflect(const double v[3], const double n[3], double out[3]);
 /* RNG pins: SmallRng stream outputs and Philox4x32-10 blocks. */
 void orc_stream_u64(uint64_t seed, uint32_t n, uint64_t* out);
 void orc_stream_f64(uint64_t seed, uint32_t n, double* out);
+/* f64 adjoint of the keyed estimator for a given dL/d(image) (W*H*3 doubles): gradients with
+ * respect to per-material albedo (3/material), roughness (1/material) and emission
+ * (3/material).  detach = 1: Russian-roulette survival and microfacet lobe probabilities held
+ * constant (the device adjoint's estimator); 0: the plain per-sample derivative.  out_rgb (may
+ * be NULL) receives the primal image. */
+int orc_adjoint(const orc_scene* s, const lum_render_params* p, const double* dl_dimage,
+                const int32_t* light_material, int detach, int threads, double* d_albedo,
+                double* d_roughness, double* d_emission, double* out_rgb);
 void orc_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 /* xoshiro256++ outputs from a raw state, and the SplitMix64-expanded state of a u64 seed. */
 void orc_xoshiro_from_state(const uint64_t state[4], uint32_t n, uint64_t* out);
