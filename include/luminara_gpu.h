@@ -361,7 +361,9 @@ lum_status lum_forward(lum_scene* scene, const lum_render_params* params, float*
  * light_material[k] names the material whose emission light k carries (NEE), or -1; NULL =
  * none.  Each path is re-traced from its RNG key (no path storage).  Russian roulette and the
  * microfacet lobe choice are treated as constants (unbiased); visibility changes are not
- * differentiated.  max_depth <= 16. */
+ * differentiated.  max_depth <= 16.  Pixels whose dL/d(image) is zero are not replayed.  The
+ * call stages one chunk of replayed paths at a time in device memory (at most 8 GiB or a
+ * quarter of the free memory, 48 + 64 * max_depth bytes per path). */
 lum_status lum_backward(lum_scene* scene, const lum_render_params* params, const float* dL_dimage,
                         const int32_t* light_material, float* d_albedo, float* d_roughness, float* d_emission,
                         lum_stats* stats);
