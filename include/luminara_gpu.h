@@ -359,11 +359,14 @@ lum_status lum_forward(lum_scene* scene, const lum_render_params* params, float*
  * dL/d(roughness) (1 per material: Microfacet) and dL/d(emission) (3 per material: the
  * Emissive colour * intensity) into HOST arrays sized by the scene's material count.
  * light_material[k] names the material whose emission light k carries (NEE), or -1; NULL =
- * none.  Each path is re-traced from its RNG key (no path storage).  Russian roulette and the
- * microfacet lobe choice are treated as constants (unbiased); visibility changes are not
- * differentiated.  max_depth <= 16.  Pixels whose dL/d(image) is zero are not replayed.  The
- * call stages one chunk of replayed paths at a time in device memory (at most 8 GiB or a
- * quarter of the free memory, 48 + 64 * max_depth bytes per path). */
+ * none.  Each path is re-traced from its RNG key (no path storage).  Russian-roulette and
+ * microfacet-lobe probabilities are held constant in the weights they divide, and the NEE term
+ * (which the reference adds only on surviving paths, undivided by the survival probability)
+ * carries a survival score term, so the gradient is an unbiased estimate of the derivative of
+ * the expected image; visibility changes are not differentiated.  max_depth <= 16.  Pixels
+ * whose dL/d(image) is zero are not replayed.  The call stages one chunk of replayed paths at
+ * a time in device memory (at most 8 GiB or a quarter of the free memory, 48 + 64 * max_depth
+ * bytes per path). */
 lum_status lum_backward(lum_scene* scene, const lum_render_params* params, const float* dL_dimage,
                         const int32_t* light_material, float* d_albedo, float* d_roughness, float* d_emission,
                         lum_stats* stats);

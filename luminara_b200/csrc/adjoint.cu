@@ -14,9 +14,12 @@
 //   grad(E_L)  += w_j (.) att_j G_j vis_j     emission of the light's material
 //   abar_j      = w_j (.) (rrw_j S_{j+1} + E_L G_j vis_j)      S_{j+1}: the suffix sum
 //   grad(albedo, roughness) += abar_j . d att_j / d(albedo, roughness)
-// Russian-roulette survival and the microfacet lobe probability are treated as constants:
-// the expectation of the estimator does not depend on them, so these per-path derivatives are
-// unbiased.  Roughness also moves the GGX-sampled direction; that dependence is carried to
+// Russian-roulette survival and the microfacet lobe probability are held constant in the
+// weights they divide (those weights make the expectation independent of them).  The one
+// exception is the NEE term, which the reference adds only on paths that survive Russian
+// roulette without dividing by the survival probability, so its expectation is surv * term;
+// its derivative gets the score term (surv'/surv) * term with surv' in full.  The result is an
+// unbiased estimate of the derivative of the expected image.  Roughness also moves the GGX-sampled direction; that dependence is carried to
 // later vertices by reverse-mode adjoints of the vertex position and direction:
 //   - att_j and the specular direction l_j as functions of (incoming direction, roughness),
 //     differentiated with 4-wide forward-mode duals,
@@ -174,7 +177,7 @@ __device__ __forceinline__ VDn<N> dunit(VDn<N> a) {
 // d att / d albedo (diagonal, values).
 template <int N>
 __device__ void microfacet_dual(V n, V d, float r, V rho, float m, float u1, float u2, bool spec, float sp, VDn<N>& att,
-                                VDn<N>& l, V& drho) {
+                                VDn<N>& l, V& drho, float& dsp_dalb, V& dsp_dd) {
     VDn<N> dd = vd<N>(d);
     if constexpr (N == 4) {
         dd.x.d[0] = 1.0f;
@@ -185,6 +188,17 @@ __device__ void microfacet_dual(V n, V d, float r, V rho, float m, float u1, flo
     VDn<N> v = dunit(VDn<N>{-dd.x, -dd.y, -dd.z});
     Dn<N> ndv = dmax(ddot(n, v), 0.001f);
     float f0[3] = {0.04f * (1.0f - m) + rho.x * m, 0.04f * (1.0f - m) + rho.y * m, 0.04f * (1.0f - m) + rho.z * m};
+    {   // the lobe probability sp = clamp(mean Fresnel(ndv, f0), 0.1, 0.9) and its derivatives
+        Dn<N> omn = dmax(1.0f - ndv, 0.0f);
+        Dn<N> omn2 = omn * omn;
+        Dn<N> tn = omn2 * omn2 * omn;
+        Dn<N> spr = (tn * (3.0f - f0[0] - f0[1] - f0[2]) + (f0[0] + f0[1] + f0[2])) * (1.0f / 3.0f);
+        const bool active = spr.v > 0.1f && spr.v < 0.9f;
+        dsp_dalb = active ? m * (1.0f - tn.v) * (1.0f / 3.0f) : 0.0f;
+        dsp_dd = mk(0.f, 0.f, 0.f);
+        if constexpr (N == 4)
+            if (active) dsp_dd = mk(spr.d[0], spr.d[1], spr.d[2]);
+    }
     if (spec) {
         Dn<N> alpha = rr * rr;
         Dn<N> tan2 = alpha * alpha * (u1 / (1.0f - u1 + 1e-10f));
@@ -228,13 +242,15 @@ __device__ void microfacet_dual(V n, V d, float r, V rho, float m, float u1, flo
 }
 
 // Diffuse-lobe microfacet att and d att / d albedo as plain values (no direction adjoint).
-__device__ __forceinline__ V microfacet_diffuse(V n, V d, V rho, float m, float sp, V& drho) {
+__device__ __forceinline__ V microfacet_diffuse(V n, V d, V rho, float m, float sp, V& drho, float& dsp_dalb) {
     float ndv = fmaxf(dot(n, unit(-d)), 0.001f);
     float om = fmaxf(1.0f - ndv, 0.0f);
     float om2 = om * om;
     float t = om2 * om2 * om;
     float s = (1.0f - m) / (1.0f - sp);
     V f0 = mk(0.04f, 0.04f, 0.04f) * (1.0f - m) + rho * m;
+    const float spr = (t * (3.0f - f0.x - f0.y - f0.z) + (f0.x + f0.y + f0.z)) * (1.0f / 3.0f);
+    dsp_dalb = spr > 0.1f && spr < 0.9f ? m * (1.0f - t) * (1.0f / 3.0f) : 0.0f;
     V F = f0 * (1.0f - t) + mk(t, t, t);
     drho = mk(s * ((1.0f - F.x) - rho.x * m * (1.0f - t)), s * ((1.0f - F.y) - rho.y * m * (1.0f - t)),
               s * ((1.0f - F.z) - rho.z * m * (1.0f - t)));
@@ -414,14 +430,16 @@ __device__ void sweep_path(const SceneDev& S, const RenderDev& R, const PathHead
             const float4 su = draw4(R.key0, R.key1, pixel, st, (uint32_t)j, CALL_SCATTER);
             const bool spec = (vx.flags & VF_SPEC) != 0;
             V att_v, drho = mk(0.f, 0.f, 0.f);
-            V datt[4] = {};               // d att / d (d_in.x, d_in.y, d_in.z, roughness)
+            V datt[4] = {};               // d att / d (d_in.x, d_in.y, d_in.z, roughness), sp held
             V dl[4] = {};                 // d l / d (same), specular lobe
+            float dsp_dalb = 0.0f;        // d sp / d albedo (each channel), microfacet
+            V dsp_dd = mk(0.f, 0.f, 0.f); // d sp / d d_in
             if (m.kind == 5) {
                 V alb = tex_value(m, vx.p);
                 if (geo) {
                     VDn<4> att, l;
                     microfacet_dual<4>(vx.n, vx.d_in, m.roughness, alb, m.metallic, su.y, su.z, spec, vx.sp, att, l,
-                                       drho);
+                                       drho, dsp_dalb, dsp_dd);
                     att_v = mk(att.x.v, att.y.v, att.z.v);
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
@@ -430,13 +448,14 @@ __device__ void sweep_path(const SceneDev& S, const RenderDev& R, const PathHead
                     }
                 } else if (spec) {
                     VDn<1> att, l;
+                    V unused;
                     microfacet_dual<1>(vx.n, vx.d_in, m.roughness, alb, m.metallic, su.y, su.z, true, vx.sp, att, l,
-                                       drho);
+                                       drho, dsp_dalb, unused);
                     att_v = mk(att.x.v, att.y.v, att.z.v);
                     datt[3] = mk(att.x.d[0], att.y.d[0], att.z.d[0]);
                     dl[3] = mk(l.x.d[0], l.y.d[0], l.z.d[0]);
                 } else {
-                    att_v = microfacet_diffuse(vx.n, vx.d_in, alb, m.metallic, vx.sp, drho);
+                    att_v = microfacet_diffuse(vx.n, vx.d_in, alb, m.metallic, vx.sp, drho, dsp_dalb);
                 }
             } else if (m.kind == 1 || m.kind == 2) {
                 att_v = m.kind == 1 ? tex_value(m, vx.p) : mk(m.color);
@@ -449,6 +468,7 @@ __device__ void sweep_path(const SceneDev& S, const RenderDev& R, const PathHead
             float surv = fminf(fmaxf(fmaxf(fmaxf(att_v.x, att_v.y), att_v.z), 0.05f), 1.0f);
             float rrw = depth < 47 ? 1.0f / surv : 1.0f;
             V abar = mul(w, S_next * rrw);
+            V nee = mk(0.f, 0.f, 0.f);
             if ((vx.flags & VF_NEE) && (vx.flags & VF_VIS)) {
                 const float4 nu = draw4(R.key0, R.key1, pixel, st, (uint32_t)j, CALL_NEE);
                 int li;
@@ -457,7 +477,8 @@ __device__ void sweep_path(const SceneDev& S, const RenderDev& R, const PathHead
                 bool ok = geo ? nee_term<true>(S, vx, att_v, nu, li, EL, Gv, gradG)
                               : nee_term<false>(S, vx, att_v, nu, li, EL, Gv, gradG);
                 if (ok) {
-                    c = c + mul(EL, att_v) * Gv;
+                    nee = mul(EL, att_v) * Gv;
+                    c = c + nee;
                     abar = abar + mul(w, EL) * Gv;
                     int lm = light_mat ? light_mat[li] : -1;
                     V gE = mul(w, att_v) * Gv;
@@ -467,16 +488,41 @@ __device__ void sweep_path(const SceneDev& S, const RenderDev& R, const PathHead
                     if (geo) PbarJ = PbarJ + gradG * dot(mul(w, EL), att_v);
                 }
             }
+            // The NEE term is added only on paths that survive Russian roulette and is not divided
+            // by the survival probability (render.rs:1497-1524): its expectation carries surv(att),
+            // so the unbiased derivative adds (surv'/surv) * (NEE contribution), surv' taken with
+            // the lobe probability's own dependence on albedo and direction.
+            V ga = mul(abar, drho);                          // albedo gradient of this vertex
+            float gr_score = 0.0f;
+            V dscore = mk(0.f, 0.f, 0.f);                    // its incoming-direction part
+            const float mx = fmaxf(fmaxf(att_v.x, att_v.y), att_v.z);
+            if (depth < 47 && mx > 0.05f && mx < 1.0f && (nee.x != 0.0f || nee.y != 0.0f || nee.z != 0.0f)) {
+                const int cs = att_v.x == mx ? 0 : (att_v.y == mx ? 1 : 2);
+                const float coef = dot(w, nee) / mx;
+                if (m.kind == 1 || m.kind == 2) {
+                    ga = ga + mk(cs == 0 ? coef : 0.f, cs == 1 ? coef : 0.f, cs == 2 ? coef : 0.f);
+                } else if (m.kind == 5) {
+                    // d att_c / d albedo_k = drho_c [c == k] + att_c * (-1/sp | 1/(1-sp)) * dsp/dalbedo_k
+                    const float sl = (spec ? -1.0f / vx.sp : 1.0f / (1.0f - vx.sp)) * mx;
+                    const float dc = cs == 0 ? drho.x : (cs == 1 ? drho.y : drho.z);
+                    const float common = coef * sl * dsp_dalb;
+                    ga = ga + mk(common + (cs == 0 ? coef * dc : 0.f), common + (cs == 1 ? coef * dc : 0.f),
+                                 common + (cs == 2 ? coef * dc : 0.f));
+                    auto comp = [cs](V v) { return cs == 0 ? v.x : (cs == 1 ? v.y : v.z); };
+                    gr_score = coef * comp(datt[3]);
+                    if (geo) dscore = (mk(comp(datt[0]), comp(datt[1]), comp(datt[2])) + dsp_dd * sl) * coef;
+                }
+            }
             // albedo / roughness through att
-            add_grad(smem, n_mat, G, vx.mat, 0, abar.x * drho.x);
-            add_grad(smem, n_mat, G, vx.mat, 1, abar.y * drho.y);
-            add_grad(smem, n_mat, G, vx.mat, 2, abar.z * drho.z);
+            add_grad(smem, n_mat, G, vx.mat, 0, ga.x);
+            add_grad(smem, n_mat, G, vx.mat, 1, ga.y);
+            add_grad(smem, n_mat, G, vx.mat, 2, ga.z);
             if (m.kind == 5) {
-                float gr = dot(abar, datt[3]);
+                float gr = dot(abar, datt[3]) + gr_score;
                 if (spec) gr += dot(Dbar, dl[3]);            // outgoing direction l(d_in, r)
                 add_grad(smem, n_mat, G, vx.mat, 3, gr);
                 if (geo) {
-                    DbarIn = mk(dot(abar, datt[0]), dot(abar, datt[1]), dot(abar, datt[2]));
+                    DbarIn = mk(dot(abar, datt[0]), dot(abar, datt[1]), dot(abar, datt[2])) + dscore;
                     if (spec) DbarIn = DbarIn + mk(dot(Dbar, dl[0]), dot(Dbar, dl[1]), dot(Dbar, dl[2]));
                 }
             }

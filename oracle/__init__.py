@@ -63,6 +63,7 @@ def lib():
         L.orc_render_rows.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.c_int, C.c_int, C.c_uint32,
                                       C.c_uint32, dp, C.POINTER(OrcStats)]
         L.orc_adjoint.argtypes = [vp, C.POINTER(abi.LumRenderParams), dp, vp, C.c_int, C.c_int, dp, dp, dp, dp]
+        L.orc_adjoint_dir.argtypes = [vp, C.POINTER(abi.LumRenderParams), dp, vp, C.c_int, C.c_int, dp, dp]
         L.orc_scatter.argtypes = [C.POINTER(abi.LumMaterial), dp, dp, dp, C.c_double, C.c_double, C.c_double,
                                   C.c_uint64, C.c_int, dp]
         L.orc_schlick.argtypes = [C.c_double, C.c_double]
@@ -153,11 +154,28 @@ class OracleScene:
         lm = None if light_material is None else np.ascontiguousarray(light_material, dtype=np.int32)
         dp_ = C.POINTER(C.c_double)
         rc = lib().orc_adjoint(self.h, C.byref(p), g.ctypes.data_as(dp_), lm.ctypes.data if lm is not None else None,
-                               1 if detach else 0, threads, da.ctypes.data_as(dp_), dr.ctypes.data_as(dp_),
+                               int(detach), threads, da.ctypes.data_as(dp_), dr.ctypes.data_as(dp_),
                                de.ctypes.data_as(dp_), img.ctypes.data_as(dp_))
         if rc != 0:
             raise RuntimeError(f"orc_adjoint failed: {rc}")
         return da, dr, de, img
+
+    def adjoint_dir(self, cfg, dl_dimage, direction, light_material=None, detach=True, threads=0):
+        """Directional derivative of sum(dl_dimage * image) along `direction` (7n parameters).
+        detach: 0/False plain, 1/True probabilities held with the survival score term, 2 held
+        without it."""
+        p = cfg.to_c()
+        g = np.ascontiguousarray(dl_dimage, dtype=np.float64)
+        d = np.ascontiguousarray(direction, dtype=np.float64)
+        assert d.shape == (7 * self.desc.n_materials,)
+        lm = None if light_material is None else np.ascontiguousarray(light_material, dtype=np.int32)
+        out = C.c_double()
+        dp_ = C.POINTER(C.c_double)
+        rc = lib().orc_adjoint_dir(self.h, C.byref(p), g.ctypes.data_as(dp_), lm.ctypes.data if lm is not None else None,
+                                   int(detach), threads, d.ctypes.data_as(dp_), C.byref(out))
+        if rc != 0:
+            raise RuntimeError(f"orc_adjoint_dir failed: {rc}")
+        return out.value
 
     def sample_direct_light(self, p, n, albedo, seed, n_iter):
         out = np.zeros((n_iter, 3))

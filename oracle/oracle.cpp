@@ -1884,8 +1884,14 @@ struct AdjCtx {
     int n_mat;
     int begin;
     bool detach;
+    bool score;                // with detach: add the NEE survival score term
+    const double* direction;   // non-null: one slot, seeded with this direction over all parameters
     Dd param(double v, int idx) const {
         Dd r = dcst(v);
+        if (direction) {
+            r.d[0] = direction[idx];
+            return r;
+        }
         int k = idx - begin;
         if (k >= 0 && k < ND) r.d[k] = 1.0;
         return r;
@@ -1905,15 +1911,18 @@ inline DV dfresnel(const Dd& cos_theta, const DV& f0) {                // materi
 }
 
 // Attenuation and outgoing direction of a scatter whose primal outcome is `sc` (material.rs).
+// att uses the lobe probability as the context says (held or not); att_full never holds it.
 void scatter_dual(const AdjCtx& C, const Material& m, int mi, const HitRecord& h, const DV& d_in, Sampler& s,
-                  const Scatter& sc, DV& att, DV& dir) {
+                  const Scatter& sc, DV& att, DV& att_full, DV& dir) {
     dir = dv(sc.ray.d);
     switch (m.kind) {
         case LUM_MAT_LAMBERTIAN:
             att = C.albedo(mi, m.tex.value(h.u, h.v, h.p));
+            att_full = att;
             return;
         case LUM_MAT_METAL:
             att = C.albedo(mi, m.albedo);
+            att_full = att;
             return;
         case LUM_MAT_MICROFACET: {                                     // material.rs:328-390
             V3 n = h.n;
@@ -1924,8 +1933,8 @@ void scatter_dual(const AdjCtx& C, const Material& m, int mi, const HitRecord& h
             DV f0 = DV{dcst(0.04 * (1.0 - m.metallic)), dcst(0.04 * (1.0 - m.metallic)), dcst(0.04 * (1.0 - m.metallic))} +
                     alb * m.metallic;
             DV fw = dfresnel(ndv, f0);
-            Dd sp = dclamp((fw.x + fw.y + fw.z) / 3.0, 0.1, 0.9);
-            if (C.detach) sp = dcst(sp.v);
+            Dd sp_full = dclamp((fw.x + fw.y + fw.z) / 3.0, 0.1, 0.9);
+            Dd sp = C.detach ? dcst(sp_full.v) : sp_full;
             if (s.draw(CALL_SCATTER, 0) < sp.v) {
                 double r1 = s.draw(CALL_SCATTER, 1), r2 = s.draw(CALL_SCATTER, 2);
                 Dd alpha = rr * rr;
@@ -1946,19 +1955,21 @@ void scatter_dual(const AdjCtx& C, const Material& m, int mi, const HitRecord& h
                 Dd g = (ndv / (ndv * (1.0 - k) + k)) * (ndl / (ndl * (1.0 - k) + k));
                 DV f = dfresnel(vdh, f0);
                 if (ndh.v > 0.001) {
-                    Dd c = g * vdh / (ndv * ndh) / sp;
-                    att = f * c;
+                    Dd c = g * vdh / (ndv * ndh);
+                    att = f * (c / sp);
+                    att_full = f * (c / sp_full);
                 } else {
-                    att = dv(v3(0, 0, 0));
+                    att = att_full = dv(v3(0, 0, 0));
                 }
                 return;
             }
             DV kd = DV{1.0 - fw.x, 1.0 - fw.y, 1.0 - fw.z} * (1.0 - m.metallic);
             att = had(kd, alb) * (1.0 / (1.0 - sp));
+            att_full = had(kd, alb) * (1.0 / (1.0 - sp_full));
             return;
         }
         default:
-            att = dv(sc.att);
+            att = att_full = dv(sc.att);
             return;
     }
 }
@@ -2050,8 +2061,8 @@ DV path_dual(const AdjCtx& C, Ray r, Sampler& s, uint32_t max_depth, Counters& c
             L = L + had(B, e);
             break;
         }
-        DV att, dir;
-        scatter_dual(C, *h.mat, h.mat_index, h, d, s, scat, att, dir);
+        DV att, att_full, dir;
+        scatter_dual(C, *h.mat, h.mat_index, h, d, s, scat, att, att_full, dir);
         double mc = std::fmax(std::fmax(scat.att.x, scat.att.y), scat.att.z);
         double surv = rclamp(mc, 0.05, 1.0);
         if (depth < 47 && s.draw(CALL_NEE, 0) > surv) {
@@ -2062,6 +2073,15 @@ DV path_dual(const AdjCtx& C, Ray r, Sampler& s, uint32_t max_depth, Counters& c
         if (depth < 47) rrw = C.detach ? dcst(1.0 / surv) : 1.0 / dclamp(dmax3(att.x, att.y, att.z), 0.05, 1.0);
         bool use_nee = !h.mat->is_specular() && !sc.lights.empty();
         DV dl = use_nee ? nee_dual(C, P, h.n, att, s, cnt) : dv(v3(0, 0, 0));
+        // The NEE term is evaluated only on paths that survive Russian roulette and is not
+        // divided by the survival probability (render.rs:1497-1524), so its expectation carries
+        // a factor surv(theta).  With probabilities held, the unbiased derivative adds the
+        // score term (surv'/surv) * term, surv' taken in full (lobe probability included).
+        if (C.detach && C.score && use_nee && depth < 47) {
+            Dd sf = dclamp(dmax3(att_full.x, att_full.y, att_full.z), 0.05, 1.0);
+            Dd ratio = sf / sf.v;
+            dl = {dl.x * ratio, dl.y * ratio, dl.z * ratio};
+        }
         DV term = e + dl;
         DV nb = had(B, att) * rrw;
         if (dnan(term) || dnan(nb)) break;
@@ -2079,9 +2099,32 @@ DV path_dual(const AdjCtx& C, Ray r, Sampler& s, uint32_t max_depth, Counters& c
 
 extern "C" {
 
+static int adjoint_impl(const orc_scene* sc, const lum_render_params* pp, const double* dl_dimage,
+                        const int32_t* light_material, int mode, int threads, const double* direction,
+                        double* d_albedo, double* d_roughness, double* d_emission, double* out_rgb);
+
 int orc_adjoint(const orc_scene* sc, const lum_render_params* pp, const double* dl_dimage, const int32_t* light_material,
                 int detach, int threads, double* d_albedo, double* d_roughness, double* d_emission, double* out_rgb) {
     if (!sc || !pp || !dl_dimage || !d_albedo || !d_roughness || !d_emission) return 1;
+    return adjoint_impl(sc, pp, dl_dimage, light_material, detach, threads, nullptr, d_albedo, d_roughness, d_emission,
+                        out_rgb);
+}
+
+int orc_adjoint_dir(const orc_scene* sc, const lum_render_params* pp, const double* dl_dimage,
+                    const int32_t* light_material, int detach, int threads, const double* direction, double* out) {
+    if (!sc || !pp || !dl_dimage || !direction || !out) return 1;
+    const size_t n = sc->mats.size();
+    std::vector<double> da(3 * n + 1), dr(n + 1), de(3 * n + 1);
+    int rc = adjoint_impl(sc, pp, dl_dimage, light_material, detach, threads, direction, da.data(), dr.data(), de.data(),
+                          nullptr);
+    *out = da[0];
+    return rc;
+}
+
+// mode: 0 plain, 1 probabilities held with the survival score term, 2 held without it.
+static int adjoint_impl(const orc_scene* sc, const lum_render_params* pp, const double* dl_dimage,
+                        const int32_t* light_material, int mode, int threads, const double* direction,
+                        double* d_albedo, double* d_roughness, double* d_emission, double* out_rgb) {
     const lum_render_params& p = *pp;
     Frame f = frame_of(p);
     const int n_mat = (int)sc->mats.size();
@@ -2093,8 +2136,9 @@ int orc_adjoint(const orc_scene* sc, const lum_render_params* pp, const double* 
     int nt = 1;
     (void)threads;
 #endif
-    for (int begin = 0; begin < std::max(n_par, 1); begin += ND) {
-        AdjCtx C{sc, pp, light_material, n_mat, begin, detach != 0};
+    const int n_pass = direction ? 1 : std::max(n_par, 1);
+    for (int begin = 0; begin < n_pass; begin += ND) {
+        AdjCtx C{sc, pp, light_material, n_mat, begin, mode != 0, mode == 1, direction};
         const bool write_img = out_rgb && begin == 0;
 #pragma omp parallel num_threads(nt)
         {
@@ -2143,8 +2187,14 @@ int orc_adjoint(const orc_scene* sc, const lum_render_params* pp, const double* 
                 }
             }
 #pragma omp critical
-            for (int k = 0; k < ND && begin + k < n_par; ++k) grad[(size_t)begin + k] += gl[k];
+            if (direction) grad[0] += gl[0];
+            else
+                for (int k = 0; k < ND && begin + k < n_par; ++k) grad[(size_t)begin + k] += gl[k];
         }
+    }
+    if (direction) {
+        d_albedo[0] = n_par > 0 ? grad[0] : 0.0;
+        return 0;
     }
     for (int m = 0; m < n_mat; ++m) {
         for (int c = 0; c < 3; ++c) {

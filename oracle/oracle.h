@@ -99,6 +99,11 @@ void orc_stream_f64(uint64_t seed, uint32_t n, double* out);
 int orc_adjoint(const orc_scene* s, const lum_render_params* p, const double* dl_dimage,
                 const int32_t* light_material, int detach, int threads, double* d_albedo,
                 double* d_roughness, double* d_emission, double* out_rgb);
+/* Directional form of orc_adjoint: the derivative along `direction` (7 * n_materials doubles,
+ * the same parameter layout: albedo 3m+c, roughness 3n+m, emission 4n+3m+c). */
+int orc_adjoint_dir(const orc_scene* s, const lum_render_params* p, const double* dl_dimage,
+                    const int32_t* light_material, int detach, int threads, const double* direction,
+                    double* out);
 void orc_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 /* xoshiro256++ outputs from a raw state, and the SplitMix64-expanded state of a u64 seed. */
 void orc_xoshiro_from_state(const uint64_t state[4], uint32_t n, uint64_t* out);
