@@ -54,6 +54,8 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward cost block")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-workload block")
     ap.add_argument("--scenes", type=int, default=64, help="batched workload: number of scenes")
     ap.add_argument("--max-res", type=int, default=1024, help="batched workload: largest resolution")
     ap.add_argument("--batch-config", default="auto", help="batched workload: auto | default | k=v,k=v")
@@ -369,6 +371,15 @@ def run_ours(args):
                "sample": f"{rows} evenly spaced rows of the same frame ({rows * Wd * strata(cfg)} paths, {s:.1f} s), "
                          f"reference estimator restated in C++ f64 (oracle/, stream RNG), OpenMP over rows"}
 
+    adjoint = adjoint_block(L) if (rank == 0 and world_size == 1 and not args.no_adjoint) else None
+    batched = None
+    if rank == 0 and world_size == 1 and not args.no_batched:
+        b = batched_measure(args, 2, 3, with_clocks=False)
+        batched = {k: b[k] for k in ("value", "unit", "ms_per_step", "batch_mode", "sequential_megakernel",
+                                     "speedup_vs_sequential", "max_rel_diff_vs_megakernel", "autotune",
+                                     "scene_done_ms")}
+        batched["workload"] = b["config"]["workload"]
+
     if rank == 0:
         line = {
             "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": world_size, "steps": args.steps,
@@ -383,7 +394,7 @@ def run_ours(args):
             "segments_per_path": segs / (paths_per_step * args.steps),
             "shadow_rays_per_path": shadows / (paths_per_step * args.steps),
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps,
-            "clocks": clock_info,
+            "clocks": clock_info, "adjoint": adjoint, "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -393,10 +404,55 @@ def run_ours(args):
     return 0
 
 
+# ------------------------------------------------------------------------------ adjoint
+def adjoint_block(L):
+    """Cost of the path-replay adjoint against one forward render on the differentiable
+    workload (1000 GGX quads + 4 emissive quads, 512x512, 64 spp, depth 6): device time of
+    lum_forward's render kernel and of lum_backward's replay + sweep kernels, for a dense
+    dL/d(image) (every pixel replayed) and for the L2 loss against a render at perturbed
+    parameters (pixels with zero gradient are skipped)."""
+    import numpy as np
+
+    from luminara_b200 import workloads as W
+
+    world, cfg = W.diff_quads()
+    rng = np.random.default_rng(77)
+    saved = [(m, m.color, m.roughness) for m in world.materials]
+    for m in world.materials:
+        if m.kind != 4:
+            m.color = tuple(float(x) for x in np.clip(np.array(m.color) + rng.normal(0, 0.05, 3), 0, 1))
+            m.roughness = float(np.clip(m.roughness + rng.normal(0, 0.05), 0.05, 1))
+    target, _ = L.GpuScene(world).render(cfg)
+    for m, c, r in saved:
+        m.color, m.roughness = c, r
+    sc = L.GpuScene(world)
+    lm = world.light_material_indices()
+    img, _ = sc.forward(cfg)
+    grads = {"dense": np.random.default_rng(1).normal(size=img.shape).astype(np.float32),
+             "l2": (2.0 * (img - target)).astype(np.float32)}
+    fwd = []
+    bwd = {k: [] for k in grads}
+    for _ in range(4):
+        _, st = sc.forward(cfg)
+        fwd.append(st.kernel_ms)
+        for k, g in grads.items():
+            *_, st = sc.backward(cfg, g, lm)
+            assert st.error_flags == 0
+            bwd[k].append(st.kernel_ms)
+    f = min(fwd)
+    out = {"workload": "diff_quads 512x512 64spp depth 6 (1004 materials)", "forward_ms": f,
+           "paths": int(np.prod(img.shape[:2])) * 64}
+    for k, v in bwd.items():
+        out[f"backward_ms_{k}"] = min(v)
+        out[f"ratio_{k}"] = min(v) / f
+    sc.close()
+    return out
+
+
 # ------------------------------------------------------------------------------ batched
-def run_batched(args):
+def batched_measure(args, steps, warmup, with_clocks=True):
     """The batched uneven workload: 64 seeded scenes rendered (a) one after another with the
-    megakernel and (b) together by the persistent wavefront tracer; reports both."""
+    megakernel and (b) together by the batch (lum_batch_*, autotuned); returns the JSON line."""
     import torch
 
     import luminara_b200 as L
@@ -425,14 +481,15 @@ def run_batched(args):
         for s, c, o in zip(scenes, cfgs, outs):
             s.render_device(c, o.data_ptr(), stream.cuda_stream)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         seq()
         batch.render_device([o.data_ptr() for o in outs])
     torch.cuda.synchronize()
-    clocks = ClockSampler(0)
-    clocks.start()
+    clocks = ClockSampler(0) if with_clocks else None
+    if clocks:
+        clocks.start()
     ev0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         seq()
     ev1.record(stream)
     torch.cuda.synchronize()
@@ -440,27 +497,27 @@ def run_batched(args):
     seq_imgs = [o.clone() for o in outs]
     done_all, bstats = [], []
     ev0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         done, st = batch.render_device([o.data_ptr() for o in outs])
         done_all.append(done)
         bstats.append(st)
     ev1.record(stream)
     torch.cuda.synchronize()
     bat_s = ev0.elapsed_time(ev1) / 1e3
-    clock_info = clocks.stop()
+    clock_info = clocks.stop() if clocks else None
     max_rel = max(float(((a - b).abs() / (b.abs() + 1e-3)).max()) for a, b in zip(outs, seq_imgs))
-    value = paths * args.steps / bat_s / 1e6
+    value = paths * steps / bat_s / 1e6
     done_ms = done_all[-1]
     line = {
-        "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": bat_s * 1e3 / args.steps, "higher_is_better": True,
+        "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": 1, "steps": steps,
+        "warmup": warmup, "ms_per_step": bat_s * 1e3 / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
         "config": {"workload": f"batched: {len(cfgs)} uneven scenes, {paths} paths per step",
                    "scenes": len(cfgs), "prims": sum(w.n_prims() for w, _ in items),
                    "l2": "working set of the batch exceeds L2 (pool, queues, 64 scenes)"},
         "batch_mode": "megakernel" if batch.config().get("mode") == 1 else "wavefront",
-        "sequential_megakernel": {"value": paths * args.steps / seq_s / 1e6, "unit": "Mpaths/s",
-                                  "ms_per_step": seq_s * 1e3 / args.steps},
+        "sequential_megakernel": {"value": paths * steps / seq_s / 1e6, "unit": "Mpaths/s",
+                                  "ms_per_step": seq_s * 1e3 / steps},
         "speedup_vs_sequential": seq_s / bat_s,
         "max_rel_diff_vs_megakernel": max_rel,
         "autotune": {"config": tuned, "best_ms": tune_ms, "seconds": tune_s},
@@ -468,8 +525,14 @@ def run_batched(args):
         "iterations": bstats[-1].iterations, "graph_launches": bstats[-1].graph_launches,
         "gpu_launches": None, "clocks": clock_info,
     }
-    print(json.dumps(line), flush=True)
     batch.close()
+    return line
+
+
+def run_batched(args):
+    line = batched_measure(args, args.steps, args.warmup)
+    print(json.dumps(line), flush=True)
+
     return 0
 
 
