@@ -286,3 +286,6 @@ def make_rays(org, dir, tmin=0.001, tmax=np.inf, time_=0.0) -> np.ndarray:
     r["tmax"] = tmax
     r["time"] = time_
     return r
+
+
+from .toml_scene import UnsupportedSceneError, load_scene, load_scene_file  # noqa: E402  (scene files)
