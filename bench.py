@@ -371,6 +371,7 @@ def run_ours(args):
                "sample": f"{rows} evenly spaced rows of the same frame ({rows * Wd * strata(cfg)} paths, {s:.1f} s), "
                          f"reference estimator restated in C++ f64 (oracle/, stream RNG), OpenMP over rows"}
 
+    tone = tonemap_block(L, out, H, Wd, stream, hbm_peak, flush) if rank == 0 else None
     adjoint = adjoint_block(L) if (rank == 0 and world_size == 1 and not args.no_adjoint) else None
     batched = None
     if rank == 0 and world_size == 1 and not args.no_batched:
@@ -394,7 +395,7 @@ def run_ours(args):
             "segments_per_path": segs / (paths_per_step * args.steps),
             "shadow_rays_per_path": shadows / (paths_per_step * args.steps),
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps,
-            "clocks": clock_info, "adjoint": adjoint, "batched": batched,
+            "clocks": clock_info, "tonemap": tone, "adjoint": adjoint, "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -402,6 +403,39 @@ def run_ours(args):
         dist.destroy_process_group()
     sc.close()
     return 0
+
+
+# ------------------------------------------------------------------------------ LDR output
+def tonemap_block(L, hdr, H, Wd, stream, hbm_peak, flush):
+    """The LDR colour chain (lum_tonemap_device) over the frame just rendered: ACES + sRGB,
+    without and with auto-exposure (a log-luminance reduction kernel first).  Each launch is
+    timed alone with CUDA events after an L2 flush.  Algorithmic bytes per call: 12 read + 4
+    written per pixel, plus 12 read per pixel for the reduction."""
+    import torch
+
+    rgba = torch.empty((H, Wd, 4), dtype=torch.uint8, device="cuda")
+    scratch = torch.empty(L.abi.TONEMAP_SCRATCH_BYTES, dtype=torch.uint8, device="cuda")
+    out = {}
+    for name, auto in (("aces_srgb", False), ("aces_srgb_auto_exposure", True)):
+        tm = L.ToneMapConfig(auto_exposure=auto)
+        for _ in range(3):
+            L.tonemap_device(hdr.data_ptr(), Wd, H, tm, scratch.data_ptr(), rgba.data_ptr(), stream.cuda_stream)
+        times = []
+        for _ in range(20):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            L.tonemap_device(hdr.data_ptr(), Wd, H, tm, scratch.data_ptr(), rgba.data_ptr(), stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        ms = statistics.median(times)
+        nbytes = H * Wd * (16 + (12 if auto else 0))
+        out[name] = {"ms": ms, "gbs": nbytes / ms / 1e6, "frac_of_measured_hbm": nbytes / ms / 1e6 / hbm_peak,
+                     "bytes_per_call": nbytes}
+    out["pixels"] = H * Wd
+    out["l2"] = "flushed (256 MiB write) before each timed call"
+    return out
 
 
 # ------------------------------------------------------------------------------ adjoint

@@ -428,6 +428,70 @@ lum_status lum_batch_render_device(lum_batch* batch, float* const* d_outs, doubl
                                    lum_batch_stats* stats);
 lum_status lum_batch_destroy(lum_batch* batch);
 
+/* ------------------------------------------------------------------------------------
+ * LDR output: exposure, tone curve and sRGB on the GPU.
+ *
+ * Replaces the per-pixel colour pipeline of render::render (src/render.rs:2594-2625 for the
+ * exposure and auto-exposure, 3100-3260 for the per-pixel chain, 3608-3658 for the tone
+ * curves and gamma_correct): for each pixel of a linear HDR image, in this order,
+ *   exposure (times 0.18 / log-average luminance when auto_exposure), vignette, white
+ *   balance, hue shift, saturation, shadow/highlight grading, tone curve per channel,
+ *   ordered dither, sRGB (gamma <= 0) or 1/gamma power to 8 bits, brightness, contrast,
+ *   sepia, tint, colour balance, posterize;
+ * output RGBA8 (alpha 255), rows top first.  Stylisation passes and spatial filters of the
+ * reference (bloom, denoise, blur, edge effects, ...) are not part of this chain.
+ * ---------------------------------------------------------------------------------- */
+enum {
+    LUM_TONEMAP_ACES = 0,      /* src/render.rs:3608-3617 (the reference's default) */
+    LUM_TONEMAP_REINHARD = 1,  /* src/render.rs:3619-3622 */
+    LUM_TONEMAP_FILMIC = 2,    /* src/render.rs:3626-3641 (Hable / Uncharted 2) */
+    LUM_TONEMAP_NONE = 3       /* clamp to [0, 1] */
+};
+
+typedef struct lum_tonemap_params {  /* the RenderConfig fields of the pixel chain */
+    int32_t tone_map;           /* LUM_TONEMAP_* */
+    int32_t auto_exposure;      /* 0/1 */
+    double exposure;            /* lum_tonemap_device only; lum_render_ldr uses the render's */
+    double gamma;               /* <= 0: sRGB transfer function */
+    int32_t dither;             /* 0/1: 4x4 Bayer dither before quantisation */
+    int32_t posterize;          /* < 2: off */
+    double vignette;            /* <= 0: off */
+    double saturation;          /* 1: off */
+    double white_balance;       /* 0: off */
+    double hue_shift;           /* degrees, 0: off */
+    double grade_shadows[3];    /* (1,1,1): off */
+    double grade_highlights[3];
+    double brightness;          /* 0: off */
+    double contrast;            /* 1: off */
+    double sepia;               /* <= 0: off */
+    double tint[3];             /* (1,1,1): off */
+    double color_balance[3];    /* (1,1,1): off */
+    double reserved[4];
+} lum_tonemap_params;
+
+/* The reference's RenderConfig defaults for the chain (ACES, sRGB, everything else off). */
+void lum_tonemap_default(lum_tonemap_params* out);
+
+/* Device scratch that lum_tonemap_device needs when auto_exposure is set. */
+#define LUM_TONEMAP_SCRATCH_BYTES 4096
+
+/* Tone-maps a DEVICE linear image (width*height*3 floats, exposure not yet applied) into a
+ * DEVICE RGBA8 buffer (width*height*4 bytes) on `stream` (cudaStream_t as void*, NULL = the
+ * default stream).  d_scratch: LUM_TONEMAP_SCRATCH_BYTES of device memory, used only with
+ * auto_exposure (may be NULL otherwise; 8-byte aligned).  d_hdr_rgb must be 4-byte aligned,
+ * d_rgba may have any alignment (16-byte aligned buffers take the vectorised path).
+ * Allocates nothing; does not synchronise. */
+lum_status lum_tonemap_device(const float* d_hdr_rgb, uint32_t width, uint32_t height,
+                              const lum_tonemap_params* tm, void* d_scratch, uint8_t* d_rgba,
+                              void* stream);
+
+/* Renders and tone-maps in one call: the HDR image stays in device memory (rendered at
+ * exposure 1; the render's params->exposure is the chain's exposure, tm->exposure is ignored)
+ * and only the RGBA8 image (width*height*4 bytes, crop size when has_crop) is copied to the
+ * caller-owned HOST buffer.  Replaces render::render's LDR output path. */
+lum_status lum_render_ldr(lum_scene* scene, const lum_render_params* params, const lum_tonemap_params* tm,
+                          uint8_t* out_rgba, lum_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

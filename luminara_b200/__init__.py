@@ -21,7 +21,7 @@ from . import abi
 from .scene import (  # noqa: F401  (re-exported reference names)
     CameraConfig, Checker, ConstantMedium, Dielectric, Disk, Emissive, Isotropic, Lambertian, LightInfo, Mesh,
     Metal, Microfacet, MovingSphere, Plane, Quad, RenderConfig, RotateX, RotateY, RotateZ, Scale, SolidColor,
-    Sphere, Translate, Triangle, World, XyRect, XzRect, YzRect, make_box,
+    Sphere, ToneMapConfig, Translate, Triangle, World, XyRect, XzRect, YzRect, make_box,
 )
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -64,6 +64,11 @@ def lib():
     L.lum_render.argtypes = [vp, C.POINTER(abi.LumRenderParams), vp, C.POINTER(abi.LumStats)]
     L.lum_render_device.argtypes = [vp, C.POINTER(abi.LumRenderParams), vp, vp, C.POINTER(abi.LumStats)]
     L.lum_count_tests.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.POINTER(abi.LumTestCounts)]
+    L.lum_tonemap_default.argtypes = [C.POINTER(abi.LumTonemapParams)]
+    L.lum_tonemap_default.restype = None
+    L.lum_tonemap_device.argtypes = [vp, C.c_uint32, C.c_uint32, C.POINTER(abi.LumTonemapParams), vp, vp, vp]
+    L.lum_render_ldr.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.POINTER(abi.LumTonemapParams), vp,
+                                 C.POINTER(abi.LumStats)]
     L.lum_forward.argtypes = [vp, C.POINTER(abi.LumRenderParams), vp, C.POINTER(abi.LumStats)]
     L.lum_backward.argtypes = [vp, C.POINTER(abi.LumRenderParams), vp, vp, vp, vp, vp, C.POINTER(abi.LumStats)]
     L.lum_intersect.argtypes = [vp, vp, C.c_uint32, vp]
@@ -80,6 +85,7 @@ def lib():
     L.lum_batch_destroy.argtypes = [vp]
     for name in ("lum_scene_create", "lum_scene_destroy", "lum_scene_info", "lum_render", "lum_render_device",
                  "lum_count_tests", "lum_intersect", "lum_occluded", "lum_forward", "lum_backward",
+                 "lum_tonemap_device", "lum_render_ldr",
                  "lum_batch_default_config",
                  "lum_batch_autotune", "lum_batch_create", "lum_batch_config_of", "lum_batch_render",
                  "lum_batch_render_device", "lum_batch_destroy"):
@@ -134,6 +140,17 @@ class GpuScene:
         st = abi.LumStats()
         check(lib().lum_render_device(self.h, C.byref(p), C.c_void_p(d_out), C.c_void_p(stream), C.byref(st)))
         return st
+
+    def render_ldr(self, cfg: RenderConfig, tm: Optional["ToneMapConfig"] = None):
+        """lum_render_ldr: (H, W, 4) uint8 RGBA through the LDR colour chain, and stats.  The
+        render's exposure is the chain's exposure (tm.exposure is ignored)."""
+        p = cfg.to_c()
+        t = (tm or ToneMapConfig()).to_c()
+        h, w, _ = cfg.out_shape()
+        out = np.empty((h, w, 4), dtype=np.uint8)
+        st = abi.LumStats()
+        check(lib().lum_render_ldr(self.h, C.byref(p), C.byref(t), out.ctypes.data, C.byref(st)))
+        return out, st
 
     def forward(self, cfg: RenderConfig):
         """lum_forward: the image (H, W, 3) and stats."""
@@ -288,4 +305,12 @@ def make_rays(org, dir, tmin=0.001, tmax=np.inf, time_=0.0) -> np.ndarray:
     return r
 
 
-from .toml_scene import UnsupportedSceneError, load_scene, load_scene_file  # noqa: E402  (scene files)
+from .toml_scene import UnsupportedSceneError, load_scene, load_scene_file, tonemap_config  # noqa: E402,F401
+
+
+def tonemap_device(d_hdr: int, width: int, height: int, tm=None, d_scratch: int = 0, d_rgba: int = 0,
+                   stream: int = 0) -> None:
+    """lum_tonemap_device on device pointers (e.g. torch tensors' data_ptr())."""
+    t = (tm or ToneMapConfig()).to_c()
+    check(lib().lum_tonemap_device(d_hdr or None, width, height, C.byref(t), d_scratch or None, d_rgba or None,
+                                   stream or None))

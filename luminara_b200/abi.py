@@ -284,6 +284,36 @@ def hit_dtype():
     )
 
 
+TONEMAP_ACES = 0
+TONEMAP_REINHARD = 1
+TONEMAP_FILMIC = 2
+TONEMAP_NONE = 3
+TONEMAP_SCRATCH_BYTES = 4096
+
+
+class LumTonemapParams(C.Structure):
+    _fields_ = [
+        ("tone_map", C.c_int32),
+        ("auto_exposure", C.c_int32),
+        ("exposure", C.c_double),
+        ("gamma", C.c_double),
+        ("dither", C.c_int32),
+        ("posterize", C.c_int32),
+        ("vignette", C.c_double),
+        ("saturation", C.c_double),
+        ("white_balance", C.c_double),
+        ("hue_shift", C.c_double),
+        ("grade_shadows", C.c_double * 3),
+        ("grade_highlights", C.c_double * 3),
+        ("brightness", C.c_double),
+        ("contrast", C.c_double),
+        ("sepia", C.c_double),
+        ("tint", C.c_double * 3),
+        ("color_balance", C.c_double * 3),
+        ("reserved", C.c_double * 4),
+    ]
+
+
 STRUCT_SIZES = {
     "lum_object": C.sizeof(LumObject),
     "lum_transform": C.sizeof(LumTransform),
@@ -299,4 +329,5 @@ STRUCT_SIZES = {
     "lum_test_counts": C.sizeof(LumTestCounts),
     "lum_batch_config": C.sizeof(LumBatchConfig),
     "lum_batch_stats": C.sizeof(LumBatchStats),
+    "lum_tonemap_params": C.sizeof(LumTonemapParams),
 }

@@ -457,6 +457,10 @@ struct lum_scene {
     size_t d_out_cap = 0;
     void* d_rays = nullptr;
     size_t d_rays_cap = 0;
+    void* d_ldr = nullptr;      // RGBA8 image of lum_render_ldr
+    size_t d_ldr_cap = 0;
+    void* d_tone = nullptr;     // tone-map reduction scratch
+    size_t d_tone_cap = 0;
     lum::SceneDev dev{};
     uint32_t n_prims = 0, n_nodes = 0, n_lights = 0, bvh_depth = 0;
     std::mutex mu;
@@ -692,6 +696,8 @@ lum_status lum_scene_destroy(lum_scene* s) {
     if (s->d_work) cudaFree(s->d_work);
     if (s->d_out) cudaFree(s->d_out);
     if (s->d_rays) cudaFree(s->d_rays);
+    if (s->d_ldr) cudaFree(s->d_ldr);
+    if (s->d_tone) cudaFree(s->d_tone);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -740,6 +746,42 @@ lum_status lum_render(lum_scene* s, const lum_render_params* params, float* out_
     lum_status rs = run_render(s, params, s->d_out, s->stream, stats);
     if (rs != LUM_OK && rs != LUM_ERR_KERNEL) return rs;
     CU(cudaMemcpyAsync(out_rgb, s->d_out, bytes, cudaMemcpyDeviceToHost, s->stream), "cudaMemcpyAsync D2H");
+    CU(cudaStreamSynchronize(s->stream), "D2H");
+    if (stats) stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return rs;
+}
+
+lum_status lum_render_ldr(lum_scene* s, const lum_render_params* params, const lum_tonemap_params* tm,
+                          uint8_t* out_rgba, lum_stats* stats) {
+    if (!s || !out_rgba || !tm) return fail(LUM_ERR_INVALID_ARGUMENT, "null argument");
+    lum_status st = check_params(params);
+    if (st != LUM_OK) return st;
+    if (tm->tone_map < LUM_TONEMAP_ACES || tm->tone_map > LUM_TONEMAP_NONE)
+        return fail(LUM_ERR_INVALID_ARGUMENT, "unknown tone_map");
+    std::lock_guard<std::mutex> lk(s->mu);
+    CU(cudaSetDevice(s->device), "cudaSetDevice");
+    auto t0 = std::chrono::steady_clock::now();
+    lum::RenderDev R;
+    st = make_render_dev(s, *params, R);
+    if (st != LUM_OK) return st;
+    const size_t px = (size_t)R.w * R.h;
+    if (px == 0) {
+        if (stats) std::memset(stats, 0, sizeof *stats);
+        return LUM_OK;
+    }
+    st = ensure((void**)&s->d_out, &s->d_out_cap, sizeof(float) * 3 * px);
+    if (st == LUM_OK) st = ensure(&s->d_ldr, &s->d_ldr_cap, 4 * px);
+    if (st == LUM_OK) st = ensure(&s->d_tone, &s->d_tone_cap, LUM_TONEMAP_SCRATCH_BYTES);
+    if (st != LUM_OK) return st;
+    // the HDR stage at exposure 1: the chain applies the exposure (src/render.rs:2594-2608)
+    lum_render_params hp = *params;
+    hp.exposure = 1.0;
+    lum_status rs = run_render(s, &hp, s->d_out, s->stream, stats);
+    if (rs != LUM_OK && rs != LUM_ERR_KERNEL) return rs;
+    CU(lum::launch_tonemap(s->d_out, R.w, R.h, *tm, params->exposure, (double*)s->d_tone, (uint8_t*)s->d_ldr,
+                           s->stream),
+       "tone map launch");
+    CU(cudaMemcpyAsync(out_rgba, s->d_ldr, 4 * px, cudaMemcpyDeviceToHost, s->stream), "cudaMemcpyAsync D2H");
     CU(cudaStreamSynchronize(s->stream), "D2H");
     if (stats) stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return rs;

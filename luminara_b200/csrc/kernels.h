@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include "../../include/luminara_gpu.h"
 #include "device_scene.h"
 
 namespace lum {
@@ -18,5 +19,10 @@ cudaError_t launch_intersect(const SceneDev& S, const lum_ray* rays, uint32_t n,
                              cudaStream_t stream);
 cudaError_t launch_occluded(const SceneDev& S, const lum_ray* rays, uint32_t n, int32_t* occ, WorkCounters* wc,
                             cudaStream_t stream);
+
+// Linear HDR (3 floats per pixel) -> RGBA8 through the colour chain of lum_tonemap_params at
+// `exposure`; `scratch` (LUM_TONEMAP_SCRATCH_BYTES) is used with auto-exposure.
+cudaError_t launch_tonemap(const float* hdr, uint32_t w, uint32_t h, const lum_tonemap_params& tm, double exposure,
+                           double* scratch, uint8_t* rgba, cudaStream_t stream);
 
 }  // namespace lum

@@ -310,6 +310,44 @@ class RenderConfig:
         return (h, w, 3)
 
 
+@dataclass
+class ToneMapConfig:
+    """The RenderConfig fields of the LDR colour chain (src/render.rs:423-510 defaults)."""
+    tone_map: int = abi.TONEMAP_ACES
+    auto_exposure: bool = False
+    exposure: float = 1.0          # used by tonemap_device; render_ldr takes the render's exposure
+    gamma: float = 0.0
+    dither: bool = False
+    posterize: int = 0
+    vignette: float = 0.0
+    saturation: float = 1.0
+    white_balance: float = 0.0
+    hue_shift: float = 0.0
+    grade_shadows: Vec = (1.0, 1.0, 1.0)
+    grade_highlights: Vec = (1.0, 1.0, 1.0)
+    brightness: float = 0.0
+    contrast: float = 1.0
+    sepia: float = 0.0
+    tint: Vec = (1.0, 1.0, 1.0)
+    color_balance: Vec = (1.0, 1.0, 1.0)
+
+    def to_c(self) -> abi.LumTonemapParams:
+        t = abi.LumTonemapParams()
+        for f in ("tone_map", "posterize"):
+            setattr(t, f, int(getattr(self, f)))
+        for f in ("auto_exposure", "dither"):
+            setattr(t, f, 1 if getattr(self, f) else 0)
+        for f in ("exposure", "gamma", "vignette", "saturation", "white_balance", "hue_shift", "brightness",
+                  "contrast", "sepia"):
+            setattr(t, f, float(getattr(self, f)))
+        for f in ("grade_shadows", "grade_highlights", "tint", "color_balance"):
+            getattr(t, f)[:] = [float(x) for x in getattr(self, f)]
+        return t
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f in self.__dataclass_fields__}
+
+
 # --------------------------------------------------------------------------------------
 # World -> lum_scene_desc
 # --------------------------------------------------------------------------------------

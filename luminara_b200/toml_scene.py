@@ -420,3 +420,37 @@ def load_scene_file(path: str) -> Tuple[S.RenderConfig, S.World, Dict]:
     with open(path, "rb") as f:
         doc = tomllib.load(f)
     return _Loader(os.path.dirname(os.path.abspath(path))).load(doc)
+
+
+# [render] settings of the LDR colour chain (lum_render_ldr / lum_tonemap_device).
+_TONE_NAMES = {"aces": abi.TONEMAP_ACES, "reinhard": abi.TONEMAP_REINHARD, "filmic": abi.TONEMAP_FILMIC,
+               "uncharted2": abi.TONEMAP_FILMIC, "none": abi.TONEMAP_NONE}
+_CHAIN_KEYS = {"tone_map", "auto_exposure", "gamma", "dither", "posterize", "vignette", "saturation",
+               "white_balance", "hue_shift", "grade_shadows", "grade_highlights", "brightness", "contrast", "sepia",
+               "tint", "color_balance"}
+
+
+def tonemap_config(post: Dict) -> S.ToneMapConfig:
+    """The colour-chain settings of a scene file's [render] table (`post` from load_scene) as a
+    ToneMapConfig (unknown tone_map names select ACES, as in src/render.rs:1130-1137).  Any other
+    active post-processing setting (bloom, denoise, blur, stylisation passes, ...) raises
+    UnsupportedSceneError: the chain would otherwise produce a different image."""
+    tm = S.ToneMapConfig()
+    bad = []
+    for k, v in post.items():
+        if k in _CHAIN_KEYS:
+            if k == "tone_map":
+                tm.tone_map = _TONE_NAMES.get(str(v), abi.TONEMAP_ACES)
+            elif k in ("grade_shadows", "grade_highlights", "tint", "color_balance"):
+                setattr(tm, k, _v3(v))
+            elif k in ("auto_exposure", "dither"):
+                setattr(tm, k, bool(v))
+            elif k == "posterize":
+                tm.posterize = int(v)
+            else:
+                setattr(tm, k, float(v))
+        elif not (v in (False, 0, 0.0, "", None) or (k == "solarize" and float(v) < 0.0)):
+            bad.append(f"render.{k}")
+    if bad:
+        raise UnsupportedSceneError(bad)
+    return tm
