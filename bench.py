@@ -55,6 +55,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward cost block")
+    ap.add_argument("--adjoint-res", type=int, default=512, help="adjoint block: image side (workload: 512)")
+    ap.add_argument("--adjoint-spp", type=int, default=64, help="adjoint block: samples per pixel (workload: 64)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-workload block")
     ap.add_argument("--scenes", type=int, default=64, help="batched workload: number of scenes")
     ap.add_argument("--max-res", type=int, default=1024, help="batched workload: largest resolution")
@@ -372,7 +374,8 @@ def run_ours(args):
                          f"reference estimator restated in C++ f64 (oracle/, stream RNG), OpenMP over rows"}
 
     tone = tonemap_block(L, out, H, Wd, stream, hbm_peak, flush) if rank == 0 else None
-    adjoint = adjoint_block(L) if (rank == 0 and world_size == 1 and not args.no_adjoint) else None
+    adjoint = (adjoint_block(L, args.adjoint_res, args.adjoint_spp)
+               if (rank == 0 and world_size == 1 and not args.no_adjoint) else None)
     batched = None
     if rank == 0 and world_size == 1 and not args.no_batched:
         b = batched_measure(args, 2, 3, with_clocks=False)
@@ -439,7 +442,7 @@ def tonemap_block(L, hdr, H, Wd, stream, hbm_peak, flush):
 
 
 # ------------------------------------------------------------------------------ adjoint
-def adjoint_block(L):
+def adjoint_block(L, res=512, spp=64):
     """Cost of the path-replay adjoint against one forward render on the differentiable
     workload (1000 GGX quads + 4 emissive quads, 512x512, 64 spp, depth 6): device time of
     lum_forward's render kernel and of lum_backward's replay + sweep kernels, for a dense
@@ -449,7 +452,7 @@ def adjoint_block(L):
 
     from luminara_b200 import workloads as W
 
-    world, cfg = W.diff_quads()
+    world, cfg = W.diff_quads(width=res, height=res, spp=spp)
     rng = np.random.default_rng(77)
     saved = [(m, m.color, m.roughness) for m in world.materials]
     for m in world.materials:
@@ -474,8 +477,8 @@ def adjoint_block(L):
             assert st.error_flags == 0
             bwd[k].append(st.kernel_ms)
     f = min(fwd)
-    out = {"workload": "diff_quads 512x512 64spp depth 6 (1004 materials)", "forward_ms": f,
-           "paths": int(np.prod(img.shape[:2])) * 64}
+    out = {"workload": f"diff_quads {res}x{res} {spp}spp depth 6 (1004 materials)", "forward_ms": f,
+           "paths": int(np.prod(img.shape[:2])) * int(np.ceil(np.sqrt(spp))) ** 2}
     for k, v in bwd.items():
         out[f"backward_ms_{k}"] = min(v)
         out[f"ratio_{k}"] = min(v) / f
