@@ -461,6 +461,8 @@ struct lum_scene {
     size_t d_ldr_cap = 0;
     void* d_tone = nullptr;     // tone-map reduction scratch
     size_t d_tone_cap = 0;
+    void* d_part = nullptr;     // stratum-group partial sums of small frames
+    size_t d_part_cap = 0;
     lum::SceneDev dev{};
     uint32_t n_prims = 0, n_nodes = 0, n_lights = 0, bvh_depth = 0;
     std::mutex mu;
@@ -534,7 +536,15 @@ lum_status run_render(lum_scene* s, const lum_render_params* params, float* d_ou
     CU(cudaMemsetAsync(s->d_work, 0, sizeof(lum::WorkCounters), stream), "cudaMemsetAsync");
     CU(cudaEventRecord(s->ev0, stream), "cudaEventRecord");
     if (R.n_tasks > 0 && R.s_end > R.s_begin) {
-        CU(lum::launch_render(s->dev, R, d_out, s->d_work, stream, 0), "render launch");
+        // frames with fewer tiles than resident warps split their strata into groups
+        const lum::RenderGroups grp = lum::render_groups(R);
+        float4* part = nullptr;
+        if (grp.n_groups > 1) {
+            st = ensure(&s->d_part, &s->d_part_cap, sizeof(float4) * grp.n_groups * (size_t)R.w * R.h);
+            if (st != LUM_OK) return st;
+            part = (float4*)s->d_part;
+        }
+        CU(lum::launch_render_grouped(s->dev, R, d_out, s->d_work, stream, part, grp), "render launch");
     } else if (R.w > 0 && R.h > 0) {
         CU(cudaMemsetAsync(d_out, 0, sizeof(float) * 3 * (size_t)R.w * R.h, stream), "cudaMemsetAsync");
     }
@@ -698,6 +708,7 @@ lum_status lum_scene_destroy(lum_scene* s) {
     if (s->d_rays) cudaFree(s->d_rays);
     if (s->d_ldr) cudaFree(s->d_ldr);
     if (s->d_tone) cudaFree(s->d_tone);
+    if (s->d_part) cudaFree(s->d_part);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);

@@ -6,6 +6,8 @@
 //   k_occluded    any hit of a ray set (the NEE shadow query, render.rs:1457-1460).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -50,7 +52,8 @@ __device__ __forceinline__ void flush_counters(WorkCounters* wc, uint32_t err, u
 // order, so the image does not depend on scheduling.
 template <bool COUNT>
 __global__ void __launch_bounds__(kRenderThreads, LUM_RENDER_MIN_BLOCKS) k_render(SceneDev S, RenderDev R, float* __restrict__ out,
-                                                           WorkCounters* wc) {
+                                                           WorkCounters* wc, float4* __restrict__ partial,
+                                                           uint32_t n_groups, uint32_t group_strata) {
     extern __shared__ int s_stack[];
     int* stack = s_stack + threadIdx.x;
     const int lane = threadIdx.x & 31;
@@ -60,20 +63,22 @@ __global__ void __launch_bounds__(kRenderThreads, LUM_RENDER_MIN_BLOCKS) k_rende
         uint32_t task = 0;
         if (lane == 0) task = atomicAdd(&wc->next_task, 1u);
         task = __shfl_sync(kFull, task, 0);
-        if (task >= R.n_tasks) break;
-        const uint32_t i = (task % R.tiles_x) * 8 + (lane & 7);
-        const uint32_t j = (task / R.tiles_x) * 4 + (lane >> 3);
+        if (task >= R.n_tasks * n_groups) break;
+        const uint32_t tile = task / n_groups, group = task - tile * n_groups;
+        const uint32_t i = (tile % R.tiles_x) * 8 + (lane & 7);
+        const uint32_t j = (tile / R.tiles_x) * 4 + (lane >> 3);
         const bool valid = i < R.w && j < R.h;
         const uint32_t gi = i + R.crop_x, gj = j + R.crop_y;
         const uint32_t pixel = gj * R.full_w + gi;
         V acc = mk(0.f, 0.f, 0.f);
         float wsum = 0.0f;
-        uint32_t st = R.s_begin;
+        uint32_t st = R.s_begin + group * group_strata;
+        const uint32_t s_end = min(R.s_end, st + group_strata);
         int state = ST_IDLE;
         Path P;
         Pending pend;
         for (;;) {
-            if (state == ST_IDLE && valid && st < R.s_end) {
+            if (state == ST_IDLE && valid && st < s_end) {
                 start_path(S, R, gi, gj, pixel, st, P);
                 ++st;
                 state = R.max_depth > 0 ? ST_CLOSEST : ST_DONE;
@@ -109,7 +114,9 @@ __global__ void __launch_bounds__(kRenderThreads, LUM_RENDER_MIN_BLOCKS) k_rende
                 state = ST_IDLE;
             }
         }
-        if (valid) {
+        if (valid && n_groups > 1) {       // this group's share; k_combine adds the groups in order
+            partial[(size_t)group * R.w * R.h + (size_t)j * R.w + i] = make_float4(acc.x, acc.y, acc.z, wsum);
+        } else if (valid) {
             V px = wsum > 0.0f ? acc * (1.0f / wsum) : acc;                // render.rs:1705
             float* o = out + 3 * ((size_t)j * R.w + i);
             o[0] = px.x * R.exposure;
@@ -122,6 +129,26 @@ __global__ void __launch_bounds__(kRenderThreads, LUM_RENDER_MIN_BLOCKS) k_rende
         atomicAdd(&wc->tally.node, tally.node);
         for (int k = 0; k < 6; ++k) atomicAdd(&wc->tally.prim[k], tally.prim[k]);
         atomicAdd(&wc->tally.plane, tally.plane);
+    }
+}
+
+// Sum of the stratum groups of each pixel in group order (deterministic), then the filter
+// normalisation and exposure of render.rs:1705 and 2610-2624.
+__global__ void k_combine(const float4* __restrict__ partial, uint32_t n_groups, size_t n_px, float exposure,
+                          float* __restrict__ out) {
+    for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < n_px; p += (size_t)gridDim.x * blockDim.x) {
+        float4 a = partial[p];
+        for (uint32_t g = 1; g < n_groups; ++g) {
+            const float4 b = partial[(size_t)g * n_px + p];
+            a.x += b.x;
+            a.y += b.y;
+            a.z += b.z;
+            a.w += b.w;
+        }
+        const float inv = a.w > 0.0f ? 1.0f / a.w : 1.0f;
+        out[3 * p] = a.x * inv * exposure;
+        out[3 * p + 1] = a.y * inv * exposure;
+        out[3 * p + 2] = a.z * inv * exposure;
     }
 }
 
@@ -231,33 +258,67 @@ static int num_sms() {
 
 static size_t stack_bytes(int threads) { return (size_t)kStackDepth * threads * sizeof(int); }
 
-template <bool COUNT>
-static cudaError_t launch_render_t(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
-                                   cudaStream_t stream, int blocks_per_sm) {
+static int render_occupancy() {
     static int occ = -1;
     if (occ < 0) {
-        cudaFuncSetAttribute(k_render<COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_render<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)stack_bytes(kRenderThreads));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_render<COUNT>, kRenderThreads,
+        cudaFuncSetAttribute(k_render<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)stack_bytes(kRenderThreads));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_render<false>, kRenderThreads,
                                                       stack_bytes(kRenderThreads));
         if (occ <= 0) occ = 4;
     }
+    return occ;
+}
+
+RenderGroups render_groups(const RenderDev& R) {
+    RenderGroups g{1, R.s_end > R.s_begin ? R.s_end - R.s_begin : 0};
+    const uint32_t n_st = g.group_strata;
+    const uint64_t warps = (uint64_t)num_sms() * render_occupancy() * (kRenderThreads / 32);
+    if (R.n_tasks == 0 || n_st < 8 || (uint64_t)R.n_tasks >= 4 * warps) return g;
+    // enough tile x group tasks for ~4 per resident warp, groups of >= 4 strata
+    uint64_t want = (4 * warps + R.n_tasks - 1) / R.n_tasks;
+    uint32_t groups = (uint32_t)std::min<uint64_t>(want, n_st / 4);
+    if (groups <= 1) return g;
+    g.group_strata = (n_st + groups - 1) / groups;
+    g.n_groups = (n_st + g.group_strata - 1) / g.group_strata;   // no empty group
+    return g;
+}
+
+template <bool COUNT>
+static cudaError_t launch_render_t(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
+                                   cudaStream_t stream, int blocks_per_sm, float4* partial, RenderGroups grp) {
+    const int occ = render_occupancy();
     if (blocks_per_sm <= 0) blocks_per_sm = occ;
+    if (!partial || grp.n_groups < 1) grp = RenderGroups{1, R.s_end > R.s_begin ? R.s_end - R.s_begin : 0};
     int grid = num_sms() * blocks_per_sm;
-    int blocks_needed = (int)((R.n_tasks + 3) / 4);   // 4 warps per block, one tile per warp at least
+    const uint64_t tasks = (uint64_t)R.n_tasks * grp.n_groups;
+    int blocks_needed = (int)((tasks + 3) / 4);   // 4 warps per block, one task per warp at least
     if (grid > blocks_needed) grid = blocks_needed > 0 ? blocks_needed : 1;
-    k_render<COUNT><<<grid, kRenderThreads, stack_bytes(kRenderThreads), stream>>>(S, R, out, wc);
+    k_render<COUNT><<<grid, kRenderThreads, stack_bytes(kRenderThreads), stream>>>(S, R, out, wc, partial,
+                                                                                   grp.n_groups, grp.group_strata);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || grp.n_groups <= 1) return e;
+    const size_t n_px = (size_t)R.w * R.h;
+    const int cgrid = (int)std::min<size_t>((n_px + 255) / 256, (size_t)num_sms() * 8);
+    k_combine<<<cgrid, 256, 0, stream>>>(partial, grp.n_groups, n_px, R.exposure, out);
     return cudaGetLastError();
 }
 
 cudaError_t launch_render(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc, cudaStream_t stream,
                           int blocks_per_sm) {
-    return launch_render_t<false>(S, R, out, wc, stream, blocks_per_sm);
+    return launch_render_t<false>(S, R, out, wc, stream, blocks_per_sm, nullptr, RenderGroups{1, 0});
+}
+
+cudaError_t launch_render_grouped(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
+                                  cudaStream_t stream, float4* partial, RenderGroups groups) {
+    return launch_render_t<false>(S, R, out, wc, stream, 0, partial, groups);
 }
 
 cudaError_t launch_render_counted(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
                                   cudaStream_t stream) {
-    return launch_render_t<true>(S, R, out, wc, stream, 0);
+    return launch_render_t<true>(S, R, out, wc, stream, 0, nullptr, RenderGroups{1, 0});
 }
 
 cudaError_t launch_intersect(const SceneDev& S, const lum_ray* rays, uint32_t n, lum_hit* hits, WorkCounters* wc,

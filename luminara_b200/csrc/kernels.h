@@ -12,6 +12,17 @@ namespace lum {
 // picks the occupancy limit.
 cudaError_t launch_render(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc, cudaStream_t stream,
                           int blocks_per_sm);
+// Stratum groups of a megakernel launch: frames with fewer 8x4 tiles than ~4x the resident
+// warps split each tile's strata into groups, so more tasks than warps exist.
+struct RenderGroups {
+    uint32_t n_groups;      // 1 = no split
+    uint32_t group_strata;  // strata per group
+};
+RenderGroups render_groups(const RenderDev& R);
+// The megakernel with stratum groups: `partial` holds n_groups * w * h float4 partial sums,
+// which a second kernel adds in group order into `out`.
+cudaError_t launch_render_grouped(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
+                                  cudaStream_t stream, float4* partial, RenderGroups groups);
 // Counter build of the megakernel: same image, plus node/primitive test tallies in wc->tally.
 cudaError_t launch_render_counted(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
                                   cudaStream_t stream);

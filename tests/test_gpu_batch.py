@@ -81,7 +81,8 @@ def test_batched_megakernel_mode_equals_lum_render():
     imgs, done, st = b.render()
     assert st.error_flags == 0 and st.segments > 0
     for img, ref in zip(imgs, refs):
-        np.testing.assert_allclose(img, ref, rtol=1e-6, atol=1e-7)
+        # same paths; lum_render adds stratum-group sums for small frames, so f32 sums differ in order
+        np.testing.assert_allclose(img, ref, rtol=1e-5, atol=1e-6)
     assert all(0 < t <= st.device_ms + 1e-3 for t in done)
 
 

@@ -45,7 +45,9 @@ def test_noalloc_matches_render_on_two_calls_in_a_row():
     for _ in range(2):
         rc, out, st = _call(sc, cfg)
         assert rc == abi.LUM_OK, L.lib().lum_last_error()
-        np.testing.assert_allclose(out, ref, rtol=1e-6, atol=1e-7)
+        # lum_render splits the strata of this small frame into groups and adds the group sums;
+        # the allocation-free path sums each pixel in one pass: same paths, f32 sum order differs
+        np.testing.assert_allclose(out, ref, rtol=1e-5, atol=1e-6)
         assert st.paths == ref_st.paths == 96 * 64 * 16
         assert st.segments == ref_st.segments and st.error_flags == 0
 
