@@ -338,15 +338,30 @@ __global__ void k_finalize(Tables T, float* const* outs) {
     }
 }
 
-// Batched megakernel: the megakernel's per-pixel path-regeneration loop (k_render) over a
-// warp-task queue that spans every scene's 8x4 tiles, one persistent launch for the batch.
-// Each scene's image is the f32 per-pixel sum k_render produces for it.
-__global__ void __launch_bounds__(128, 5) k_render_multi(Tables T, const unsigned long long* tile_prefix,
-                                                         float* const* outs, Ctl* ctl, uint32_t* next_task) {
+// Batched megakernel: the megakernel's per-pixel path-regeneration loop (k_render) over one
+// warp-task queue that spans every scene, one persistent launch for the batch.  A task is one
+// 8x4 tile of one scene and one group of at most kGroupStrata of its strata; scenes are queued
+// heaviest task first (order[]).
+// Each task adds its per-pixel partial sums to the scene's 64-bit fixed-point accumulators
+// (order-free, hence deterministic) and k_finalize writes the images.  Scene descriptors are
+// read in place (constant or global memory) rather than copied per task.
+constexpr uint32_t kGroupStrata = 256;   // whole tiles up to 256 spp: the batch's queue is long anyway
+
+// Scene and render descriptors of batches of up to kConstScenes scenes live in constant memory,
+// indexed by a warp-uniform scene index: read through the constant cache like the plain
+// megakernel's kernel parameters.  Larger batches read them from global memory.
+constexpr uint32_t kConstScenes = 128;
+__constant__ SceneDev c_scenes[kConstScenes];
+__constant__ RenderDev c_renders[kConstScenes];
+
+template <bool CONST_TABLES>
+__global__ void __launch_bounds__(128, 5) k_render_multi(Tables T, const unsigned long long* task_prefix,
+                                                         const uint32_t* order, const uint2* groups, Ctl* ctl,
+                                                         uint32_t* next_task) {
     extern __shared__ int s_stack[];
     int* stack = s_stack + threadIdx.x;
     const int lane = threadIdx.x & 31;
-    const unsigned long long total = tile_prefix[T.n];
+    const unsigned long long total = task_prefix[T.n];
     uint32_t err = 0, nseg = 0, nsh = 0;
     for (;;) {
         uint32_t task = 0;
@@ -356,25 +371,28 @@ __global__ void __launch_bounds__(128, 5) k_render_multi(Tables T, const unsigne
         uint32_t lo = 0, hi = T.n;
         while (hi - lo > 1) {
             uint32_t mid = (lo + hi) >> 1;
-            if (tile_prefix[mid] <= task) lo = mid; else hi = mid;
+            if (task_prefix[mid] <= task) lo = mid; else hi = mid;
         }
-        const uint32_t s = lo;
-        const SceneDev S = T.scenes[s];
-        const RenderDev R = T.renders[s];
-        const uint32_t t = task - (uint32_t)tile_prefix[s];
-        const uint32_t i = (t % R.tiles_x) * 8 + (lane & 7);
-        const uint32_t j = (t / R.tiles_x) * 4 + (lane >> 3);
+        const uint32_t s = order[lo];
+        const SceneDev& S = CONST_TABLES ? c_scenes[s] : T.scenes[s];
+        const RenderDev& R = CONST_TABLES ? c_renders[s] : T.renders[s];
+        const uint2 grp = groups[s];                       // (n_groups, strata per group)
+        const uint32_t t = task - (uint32_t)task_prefix[lo];
+        const uint32_t tile = t / grp.x, group = t - tile * grp.x;
+        const uint32_t i = (tile % R.tiles_x) * 8 + (lane & 7);
+        const uint32_t j = (tile / R.tiles_x) * 4 + (lane >> 3);
         const bool valid = i < R.w && j < R.h;
         const uint32_t gi = i + R.crop_x, gj = j + R.crop_y;
         const uint32_t pixel = gj * R.full_w + gi;
         V acc = mk(0.f, 0.f, 0.f);
         float wsum = 0.0f;
-        uint32_t st = R.s_begin;
+        uint32_t st = R.s_begin + group * grp.y;
+        const uint32_t s_end = min(R.s_end, st + grp.y);
         int state = ST_IDLE;
         Path P;
         Pending pend;
         for (;;) {
-            if (state == ST_IDLE && valid && st < R.s_end) {
+            if (state == ST_IDLE && valid && st < s_end) {
                 start_path(S, R, gi, gj, pixel, st, P);
                 ++st;
                 state = R.max_depth > 0 ? ST_CLOSEST : ST_DONE;
@@ -410,15 +428,15 @@ __global__ void __launch_bounds__(128, 5) k_render_multi(Tables T, const unsigne
             }
         }
         if (valid) {
-            V px = wsum > 0.0f ? acc * (1.0f / wsum) : acc;
-            float* o = outs[s] + 3 * ((size_t)j * R.w + i);
-            o[0] = px.x * R.exposure;
-            o[1] = px.y * R.exposure;
-            o[2] = px.z * R.exposure;
+            unsigned long long* a = T.acc + 4 * (T.acc_off[s] + (size_t)j * R.w + i);
+            atomicAdd(a, (unsigned long long)fix(acc.x));
+            atomicAdd(a + 1, (unsigned long long)fix(acc.y));
+            atomicAdd(a + 2, (unsigned long long)fix(acc.z));
+            atomicAdd(a + 3, (unsigned long long)fix(wsum));
         }
         if (lane == 0) {
             unsigned long long k = atomicAdd(T.done_count + s, 1ull) + 1ull;
-            if (k == tile_prefix[s + 1] - tile_prefix[s]) T.finish_ns[s] = globaltimer();
+            if (k == task_prefix[lo + 1] - task_prefix[lo]) T.finish_ns[s] = globaltimer();
         }
     }
     unsigned long long a = nseg, b = nsh;
@@ -475,6 +493,7 @@ struct lum_batch {
     uint32_t n = 0;
     lum_batch_config cfg{};
     std::vector<lum::RenderDev> R;
+    std::vector<lum::SceneDev> S;                  // host copies (constant tables of megakernel mode)
     std::vector<unsigned long long> scene_total;
     unsigned long long total_work = 0;
     size_t total_pixels = 0;
@@ -488,8 +507,10 @@ struct lum_batch {
     uint32_t* h_done = nullptr;                 // pinned
     int grid_queue = 0, grid_trace = 0, block = 128;
     size_t stack_bytes = 0;
-    unsigned long long* d_tile_prefix = nullptr;   // megakernel mode
+    unsigned long long* d_tile_prefix = nullptr;   // megakernel mode: task prefix in queue order
     uint32_t* d_next_task = nullptr;
+    uint32_t* d_order = nullptr;                   // queue position -> scene
+    uint2* d_groups = nullptr;                     // per scene: (stratum groups, strata per group)
     int grid_mega = 0;
 };
 
@@ -513,6 +534,8 @@ lum_status enqueue_iteration(lum_batch* b) {
     return LUM_OK;
 }
 
+std::mutex g_const_mu;   // guards the constant scene tables of megakernel-mode renders
+
 lum_status run_batch(lum_batch* b, float* const* d_outs, double* scene_done_ms, lum_batch_stats* stats) {
     using namespace lum::wf;
     auto t0 = std::chrono::steady_clock::now();
@@ -527,9 +550,21 @@ lum_status run_batch(lum_batch* b, float* const* d_outs, double* scene_done_ms, 
     WF(cudaMemcpyAsync(b->ctl, &c, sizeof c, cudaMemcpyHostToDevice, b->stream), "ctl");
     WF(cudaEventRecord(b->ev0, b->stream), "event");
     if (b->cfg.mode == LUM_BATCH_MEGAKERNEL) {
+        // the constant tables are per device: one megakernel-mode render at a time uploads and
+        // uses them (this call synchronises its stream before returning)
+        std::unique_lock<std::mutex> lk(g_const_mu, std::defer_lock);
+        if (b->n <= kConstScenes) {
+            lk.lock();
+            WF(cudaMemcpyToSymbolAsync(c_scenes, b->S.data(), sizeof(lum::SceneDev) * b->n, 0, cudaMemcpyHostToDevice,
+                                       b->stream), "scene table");
+            WF(cudaMemcpyToSymbolAsync(c_renders, b->R.data(), sizeof(lum::RenderDev) * b->n, 0,
+                                       cudaMemcpyHostToDevice, b->stream), "render table");
+        }
         WF(cudaMemsetAsync(b->d_next_task, 0, sizeof(uint32_t), b->stream), "memset");
         k_init<<<1, 32, 0, b->stream>>>(b->pool, b->ctl);             // t0 only (pool is empty)
         WF(cudaGraphLaunch(b->exec, b->stream), "cudaGraphLaunch");
+        k_finalize<<<dim3(64, b->n), 256, 0, b->stream>>>(b->T, b->d_out_table);
+        WF(cudaGetLastError(), "finalize launch");
         WF(cudaEventRecord(b->ev1, b->stream), "event");
         Ctl out{};
         std::vector<unsigned long long> fin(b->n);
@@ -642,12 +677,29 @@ lum_status create_batch(lum_scene* const* scenes, const lum_render_params* param
         b->total_pixels += px;
     }
     b->total_work = prefix[n];
+    b->S = S;
     const bool mega = cfg.mode == LUM_BATCH_MEGAKERNEL;
     if (cfg.mode != LUM_BATCH_WAVEFRONT && !mega)
         return fail_out(lum::set_error(LUM_ERR_INVALID_ARGUMENT, "unknown batch mode"));
+    // megakernel mode: tasks of one tile x one group of <= kGroupStrata strata, scenes queued
+    // by decreasing task cost (strata per task x log2 of the primitive count), so the longest
+    // tasks start first and the batch ends on short ones
+    std::vector<uint2> groups(n);
+    std::vector<uint32_t> order(n);
+    std::vector<double> task_cost(n);
+    for (uint32_t s = 0; s < n; ++s) {
+        const uint32_t n_st = b->R[s].s_end > b->R[s].s_begin ? b->R[s].s_end - b->R[s].s_begin : 0;
+        const uint32_t gs = std::max(1u, std::min(n_st, kGroupStrata));
+        groups[s] = make_uint2(n_st ? (n_st + gs - 1) / gs : 0, gs);
+        task_cost[s] = (double)gs * (2.0 + std::log2(1.0 + (double)S[s].n_prims)) * std::max(1u, b->R[s].max_depth);
+        order[s] = s;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return task_cost[x] > task_cost[y]; });
     std::vector<unsigned long long> tile_prefix(n + 1, 0);
-    for (uint32_t s = 0; s < n; ++s)
-        tile_prefix[s + 1] = tile_prefix[s] + ((b->R[s].s_end > b->R[s].s_begin) ? b->R[s].n_tasks : 0);
+    for (uint32_t k = 0; k < n; ++k) {
+        const uint32_t s = order[k];
+        tile_prefix[k + 1] = tile_prefix[k] + (unsigned long long)b->R[s].n_tasks * groups[s].x;
+    }
     if (tile_prefix[n] > 0xFFFFFFFFull) return fail_out(lum::set_error(LUM_ERR_TOO_LARGE, "too many tiles in batch"));
     const uint32_t Q = mega ? 1024u : cfg.pool_paths;
     if (Q < 1024 || Q > (1u << 24)) return fail_out(lum::set_error(LUM_ERR_INVALID_ARGUMENT, "pool_paths out of range"));
@@ -675,7 +727,7 @@ lum_status create_batch(lum_scene* const* scenes, const lum_render_params* param
     size_t o_done = take(8ull * n), o_total = take(8ull * n), o_fin = take(8ull * n), o_finit = take(4ull * n);
     size_t o_ctl = take(sizeof(Ctl)), o_outs = take(sizeof(float*) * n);
     size_t o_stage = take(12ull * b->total_pixels);
-    size_t o_tpre = take(8ull * (n + 1)), o_next = take(4);
+    size_t o_tpre = take(8ull * (n + 1)), o_next = take(4), o_order = take(4ull * n), o_groups = take(8ull * n);
     cudaError_t e = cudaSetDevice(b->device);
     if (e != cudaSuccess) return fail_out(wf_cuda(e, "cudaSetDevice"));
     if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess ||
@@ -709,12 +761,16 @@ lum_status create_batch(lum_scene* const* scenes, const lum_render_params* param
     b->d_staging = (float*)(m + o_stage);
     b->d_tile_prefix = (unsigned long long*)(m + o_tpre);
     b->d_next_task = (uint32_t*)(m + o_next);
+    b->d_order = (uint32_t*)(m + o_order);
+    b->d_groups = (uint2*)(m + o_groups);
     if ((e = cudaMemcpy(m + o_scenes, S.data(), sizeof(lum::SceneDev) * n, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(m + o_renders, b->R.data(), sizeof(lum::RenderDev) * n, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(m + o_prefix, prefix.data(), 8ull * (n + 1), cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(m + o_accoff, b->acc_off.data(), 8ull * n, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(m + o_total, b->scene_total.data(), 8ull * n, cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemcpy(m + o_tpre, tile_prefix.data(), 8ull * (n + 1), cudaMemcpyHostToDevice)) != cudaSuccess)
+        (e = cudaMemcpy(m + o_tpre, tile_prefix.data(), 8ull * (n + 1), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(m + o_order, order.data(), 4ull * n, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(m + o_groups, groups.data(), 8ull * n, cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail_out(wf_cuda(e, "batch upload"));
 
     // grids: persistent-style, sized to the SM count and the kernels' occupancy
@@ -728,9 +784,10 @@ lum_status create_batch(lum_scene* const* scenes, const lum_render_params* param
     b->grid_trace = sms * std::max(occ_t, 1);
 
     int occ_m = 0;
-    cudaFuncSetAttribute(k_render_multi, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)((size_t)lum::kStackDepth * 128 * sizeof(int)));
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_m, k_render_multi, 128,
+    for (auto fn : {k_render_multi<true>, k_render_multi<false>})
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)((size_t)lum::kStackDepth * 128 * sizeof(int)));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_m, k_render_multi<true>, 128,
                                                   (size_t)lum::kStackDepth * 128 * sizeof(int));
     b->grid_mega = sms * std::max(occ_m, 1);
 
@@ -739,8 +796,12 @@ lum_status create_batch(lum_scene* const* scenes, const lum_render_params* param
     if ((e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
         return fail_out(wf_cuda(e, "cudaStreamBeginCapture"));
     if (mega) {
-        k_render_multi<<<b->grid_mega, 128, (size_t)lum::kStackDepth * 128 * sizeof(int), b->stream>>>(
-            b->T, b->d_tile_prefix, b->d_out_table, b->ctl, b->d_next_task);
+        if (n <= kConstScenes)
+            k_render_multi<true><<<b->grid_mega, 128, (size_t)lum::kStackDepth * 128 * sizeof(int), b->stream>>>(
+                b->T, b->d_tile_prefix, b->d_order, b->d_groups, b->ctl, b->d_next_task);
+        else
+            k_render_multi<false><<<b->grid_mega, 128, (size_t)lum::kStackDepth * 128 * sizeof(int), b->stream>>>(
+                b->T, b->d_tile_prefix, b->d_order, b->d_groups, b->ctl, b->d_next_task);
     } else {
         for (uint32_t g = 0; g < cfg.iters_per_graph; ++g) enqueue_iteration(b);
     }
