@@ -461,7 +461,7 @@ struct lum_scene {
     size_t d_ldr_cap = 0;
     void* d_tone = nullptr;     // tone-map reduction scratch
     size_t d_tone_cap = 0;
-    void* d_part = nullptr;     // stratum-group partial sums of small frames
+    void* d_part = nullptr;     // fixed-point pixel accumulators of grouped (small) frames
     size_t d_part_cap = 0;
     lum::SceneDev dev{};
     uint32_t n_prims = 0, n_nodes = 0, n_lights = 0, bvh_depth = 0;
@@ -538,11 +538,11 @@ lum_status run_render(lum_scene* s, const lum_render_params* params, float* d_ou
     if (R.n_tasks > 0 && R.s_end > R.s_begin) {
         // frames with fewer tiles than resident warps split their strata into groups
         const lum::RenderGroups grp = lum::render_groups(R);
-        float4* part = nullptr;
+        unsigned long long* part = nullptr;
         if (grp.n_groups > 1) {
-            st = ensure(&s->d_part, &s->d_part_cap, sizeof(float4) * grp.n_groups * (size_t)R.w * R.h);
+            st = ensure(&s->d_part, &s->d_part_cap, 32 * (size_t)R.w * R.h);
             if (st != LUM_OK) return st;
-            part = (float4*)s->d_part;
+            part = (unsigned long long*)s->d_part;
         }
         CU(lum::launch_render_grouped(s->dev, R, d_out, s->d_work, stream, part, grp), "render launch");
     } else if (R.w > 0 && R.h > 0) {

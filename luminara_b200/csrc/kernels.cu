@@ -15,6 +15,7 @@
 
 #include "kernels.h"
 #include "scene_access.h"
+#include "render_task.cuh"
 #include "tracer.cuh"
 
 namespace lum {
@@ -43,20 +44,22 @@ __device__ __forceinline__ void flush_counters(WorkCounters* wc, uint32_t err, u
     }
 }
 
-// Persistent megakernel.  Each warp takes 8x4 pixel tiles from a global counter; each lane
-// owns one pixel and walks its strata [s_begin, s_end), starting a new path as soon as the
-// previous one ends (path regeneration).  Every loop iteration runs exactly one traversal
-// per active lane -- the closest hit of a path segment or the any hit of an NEE shadow
-// ray, through the same code -- followed by that lane's shading step, so traversal stays
-// convergent across lanes at different bounces.  The per-pixel sum is taken in a fixed
-// order, so the image does not depend on scheduling.
+// Persistent megakernel.  Each warp takes tasks from a global counter: an 8x4 pixel tile and a
+// group of its strata (all of them, unless the frame is small: render_groups).  tile_task
+// (render_task.cuh) runs the task with the warp's lanes drawing (pixel, stratum) pairs from one
+// pool and adding each finished path to the tile's fixed-point pixel sums.  An ungrouped task
+// then writes its pixels; a grouped one adds its sums to the frame's fixed-point accumulators,
+// which k_fixed_finalize turns into pixels.  Integer sums make the image deterministic and the
+// same whether or not the frame was grouped.
 template <bool COUNT>
 __global__ void __launch_bounds__(kRenderThreads, LUM_RENDER_MIN_BLOCKS) k_render(SceneDev S, RenderDev R, float* __restrict__ out,
-                                                           WorkCounters* wc, float4* __restrict__ partial,
+                                                           WorkCounters* wc, unsigned long long* __restrict__ gacc,
                                                            uint32_t n_groups, uint32_t group_strata) {
     extern __shared__ int s_stack[];
+    __shared__ unsigned long long s_acc[kRenderThreads / 32][32][4];
+    __shared__ uint32_t s_next[kRenderThreads / 32];
     int* stack = s_stack + threadIdx.x;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     uint32_t err = 0, nseg = 0, nsh = 0;
     TestTally tally{};
     for (;;) {
@@ -65,64 +68,22 @@ __global__ void __launch_bounds__(kRenderThreads, LUM_RENDER_MIN_BLOCKS) k_rende
         task = __shfl_sync(kFull, task, 0);
         if (task >= R.n_tasks * n_groups) break;
         const uint32_t tile = task / n_groups, group = task - tile * n_groups;
-        const uint32_t i = (tile % R.tiles_x) * 8 + (lane & 7);
-        const uint32_t j = (tile / R.tiles_x) * 4 + (lane >> 3);
-        const bool valid = i < R.w && j < R.h;
-        const uint32_t gi = i + R.crop_x, gj = j + R.crop_y;
-        const uint32_t pixel = gj * R.full_w + gi;
-        V acc = mk(0.f, 0.f, 0.f);
-        float wsum = 0.0f;
-        uint32_t st = R.s_begin + group * group_strata;
-        const uint32_t s_end = min(R.s_end, st + group_strata);
-        int state = ST_IDLE;
-        Path P;
-        Pending pend;
-        for (;;) {
-            if (state == ST_IDLE && valid && st < s_end) {
-                start_path(S, R, gi, gj, pixel, st, P);
-                ++st;
-                state = R.max_depth > 0 ? ST_CLOSEST : ST_DONE;
-            }
-            if (!__any_sync(kFull, state != ST_IDLE)) break;
-            if (state == ST_CLOSEST || state == ST_SHADOW) {
-                const bool shadow = state == ST_SHADOW;
-                Ray r;
-                r.o = P.ray.o;
-                r.d = shadow ? pend.dir : P.ray.d;
-                r.time = shadow ? 0.0f : P.ray.time;                  // Ray::new (render.rs:1457)
-                Hit h;
-                h.t = shadow ? pend.tmax : CUDART_INF_F;
-                h.prim = -1;
-                h.b1 = h.b2 = 0.0f;
-                const bool found = trace<COUNT>(S, r, 0.001f, shadow, h, stack, err, &tally);
-                if (shadow) {
-                    ++nsh;
-                    if (!found) P.L = P.L + pend.contrib;
-                    state = P.bounce >= R.max_depth ? ST_DONE : ST_CLOSEST;
-                } else {
-                    ++nseg;
-                    state = shade(S, R, pixel, P, found, h, pend);
-                }
-            }
-            if (state == ST_DONE) {
-                // luminance clamp and filter weight (render.rs:1692-1701)
-                float lum = 0.2126f * P.L.x + 0.7152f * P.L.y + 0.0722f * P.L.z;
-                V cl = lum > 100.0f ? P.L * (100.0f / lum) : P.L;
-                float w = filter_weight(R.pixel_filter, P.jx - 0.5f, P.jy - 0.5f);
-                acc = fma3(cl, w, acc);
-                wsum += w;
-                state = ST_IDLE;
+        const uint32_t x0 = (tile % R.tiles_x) * 8, y0 = (tile / R.tiles_x) * 4;
+        const uint32_t tw = min(8u, R.w - x0), th = min(4u, R.h - y0);
+        const uint32_t s_lo = R.s_begin + group * group_strata;
+        const uint32_t s_hi = min(R.s_end, s_lo + group_strata);
+        tile_task<COUNT>(S, R, x0, y0, tw, th, s_lo, s_hi, s_acc[wid], &s_next[wid], stack, err, nseg, nsh, &tally);
+        if (lane < (int)(tw * th)) {
+            const uint32_t i = x0 + lane % tw, j = y0 + lane / tw;
+            const unsigned long long* a = s_acc[wid][lane];
+            if (n_groups > 1) {
+                unsigned long long* g = gacc + 4 * ((size_t)j * R.w + i);
+                for (int c = 0; c < 4; ++c) atomicAdd(g + c, a[c]);
+            } else {
+                fixed_pixel(a, R.exposure, out + 3 * ((size_t)j * R.w + i));
             }
         }
-        if (valid && n_groups > 1) {       // this group's share; k_combine adds the groups in order
-            partial[(size_t)group * R.w * R.h + (size_t)j * R.w + i] = make_float4(acc.x, acc.y, acc.z, wsum);
-        } else if (valid) {
-            V px = wsum > 0.0f ? acc * (1.0f / wsum) : acc;                // render.rs:1705
-            float* o = out + 3 * ((size_t)j * R.w + i);
-            o[0] = px.x * R.exposure;
-            o[1] = px.y * R.exposure;
-            o[2] = px.z * R.exposure;
-        }
+        __syncwarp(kFull);   // the sums are read before the next task clears them
     }
     flush_counters(wc, err, nseg, nsh);
     if constexpr (COUNT) {
@@ -132,24 +93,11 @@ __global__ void __launch_bounds__(kRenderThreads, LUM_RENDER_MIN_BLOCKS) k_rende
     }
 }
 
-// Sum of the stratum groups of each pixel in group order (deterministic), then the filter
-// normalisation and exposure of render.rs:1705 and 2610-2624.
-__global__ void k_combine(const float4* __restrict__ partial, uint32_t n_groups, size_t n_px, float exposure,
-                          float* __restrict__ out) {
-    for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < n_px; p += (size_t)gridDim.x * blockDim.x) {
-        float4 a = partial[p];
-        for (uint32_t g = 1; g < n_groups; ++g) {
-            const float4 b = partial[(size_t)g * n_px + p];
-            a.x += b.x;
-            a.y += b.y;
-            a.z += b.z;
-            a.w += b.w;
-        }
-        const float inv = a.w > 0.0f ? 1.0f / a.w : 1.0f;
-        out[3 * p] = a.x * inv * exposure;
-        out[3 * p + 1] = a.y * inv * exposure;
-        out[3 * p + 2] = a.z * inv * exposure;
-    }
+// Pixels of a grouped frame from its fixed-point accumulators.
+__global__ void k_fixed_finalize(const unsigned long long* __restrict__ gacc, size_t n_px, float exposure,
+                                 float* __restrict__ out) {
+    for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < n_px; p += (size_t)gridDim.x * blockDim.x)
+        fixed_pixel(gacc + 4 * p, exposure, out + 3 * p);
 }
 
 // u, v of a hit as the reference's HitRecord carries them (uv per primitive type).
@@ -292,21 +240,25 @@ RenderGroups render_groups(const RenderDev& R) {
 
 template <bool COUNT>
 static cudaError_t launch_render_t(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
-                                   cudaStream_t stream, int blocks_per_sm, float4* partial, RenderGroups grp) {
+                                   cudaStream_t stream, int blocks_per_sm, unsigned long long* gacc, RenderGroups grp) {
     const int occ = render_occupancy();
     if (blocks_per_sm <= 0) blocks_per_sm = occ;
-    if (!partial || grp.n_groups < 1) grp = RenderGroups{1, R.s_end > R.s_begin ? R.s_end - R.s_begin : 0};
+    if (!gacc || grp.n_groups < 1) grp = RenderGroups{1, R.s_end > R.s_begin ? R.s_end - R.s_begin : 0};
+    const size_t n_px = (size_t)R.w * R.h;
+    if (grp.n_groups > 1) {
+        cudaError_t e = cudaMemsetAsync(gacc, 0, 32 * n_px, stream);
+        if (e != cudaSuccess) return e;
+    }
     int grid = num_sms() * blocks_per_sm;
     const uint64_t tasks = (uint64_t)R.n_tasks * grp.n_groups;
     int blocks_needed = (int)((tasks + 3) / 4);   // 4 warps per block, one task per warp at least
     if (grid > blocks_needed) grid = blocks_needed > 0 ? blocks_needed : 1;
-    k_render<COUNT><<<grid, kRenderThreads, stack_bytes(kRenderThreads), stream>>>(S, R, out, wc, partial,
+    k_render<COUNT><<<grid, kRenderThreads, stack_bytes(kRenderThreads), stream>>>(S, R, out, wc, gacc,
                                                                                    grp.n_groups, grp.group_strata);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || grp.n_groups <= 1) return e;
-    const size_t n_px = (size_t)R.w * R.h;
     const int cgrid = (int)std::min<size_t>((n_px + 255) / 256, (size_t)num_sms() * 8);
-    k_combine<<<cgrid, 256, 0, stream>>>(partial, grp.n_groups, n_px, R.exposure, out);
+    k_fixed_finalize<<<cgrid, 256, 0, stream>>>(gacc, n_px, R.exposure, out);
     return cudaGetLastError();
 }
 
@@ -316,8 +268,8 @@ cudaError_t launch_render(const SceneDev& S, const RenderDev& R, float* out, Wor
 }
 
 cudaError_t launch_render_grouped(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
-                                  cudaStream_t stream, float4* partial, RenderGroups groups) {
-    return launch_render_t<false>(S, R, out, wc, stream, 0, partial, groups);
+                                  cudaStream_t stream, unsigned long long* gacc, RenderGroups groups) {
+    return launch_render_t<false>(S, R, out, wc, stream, 0, gacc, groups);
 }
 
 cudaError_t launch_render_counted(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,

@@ -19,10 +19,10 @@ struct RenderGroups {
     uint32_t group_strata;  // strata per group
 };
 RenderGroups render_groups(const RenderDev& R);
-// The megakernel with stratum groups: `partial` holds n_groups * w * h float4 partial sums,
-// which a second kernel adds in group order into `out`.
+// The megakernel with stratum groups: `gacc` holds 4 u64 fixed-point accumulators per pixel
+// (zeroed by the launch), which a second kernel turns into `out`.
 cudaError_t launch_render_grouped(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
-                                  cudaStream_t stream, float4* partial, RenderGroups groups);
+                                  cudaStream_t stream, unsigned long long* gacc, RenderGroups groups);
 // Counter build of the megakernel: same image, plus node/primitive test tallies in wc->tally.
 cudaError_t launch_render_counted(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
                                   cudaStream_t stream);

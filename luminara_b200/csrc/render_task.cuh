@@ -1,0 +1,101 @@
+// render_task.cuh -- one warp's render task: an 8x4 tile of one frame and a range of its strata.
+//
+// The task's (pixel, stratum) pairs form one pool that the warp's lanes draw from through a
+// shared-memory counter: a lane whose path ends takes the next pair, so no lane idles while the
+// task has paths left (a lane that owned one pixel would wait, at the end of every task, for the
+// lane with the longest paths).  Pairs are numbered stratum-major, so the warp starts on one
+// stratum of every pixel of the tile, as coherent as one path per pixel.  Every loop iteration
+// runs exactly one traversal per active lane -- the closest hit of a path segment or the any hit
+// of an NEE shadow ray, through the same code -- then that lane's shading step, so traversal
+// stays convergent across lanes at different bounces.
+//
+// Each finished path adds its clamped, filter-weighted radiance and its filter weight to the
+// tile's per-pixel sums in 64-bit fixed point (2^-32 units, shared-memory atomics): integer sums
+// do not depend on the order in which paths finish, so the image is deterministic and equal
+// whichever kernel (megakernel, batched megakernel, wavefront) traced the paths.
+#pragma once
+
+#include "tracer.cuh"
+
+namespace lum {
+
+constexpr double kFixScale = 4294967296.0;   // 2^32
+
+__device__ __forceinline__ unsigned long long to_fixed(float v) {
+    return (unsigned long long)llrint((double)v * kFixScale);
+}
+
+// Pixel value from its fixed-point sums (render.rs:1705 and the exposure of 2610-2624).
+__device__ __forceinline__ void fixed_pixel(const unsigned long long* a, float exposure, float* o) {
+    const double w = (double)(long long)a[3] / kFixScale;
+    const double inv = w > 0.0 ? 1.0 / w : 1.0;
+    for (int c = 0; c < 3; ++c) o[c] = (float)((double)(long long)a[c] / kFixScale * inv) * exposure;
+}
+
+// Runs the task; on return acc[k][0..3] (k < tw * th, pixel (k % tw, k / tw) of the tile) hold
+// the sums.  acc (32 x 4) and *next are the warp's shared memory; the call zeroes them.
+template <bool COUNT>
+__device__ __forceinline__ void tile_task(const SceneDev& S, const RenderDev& R, uint32_t x0, uint32_t y0,
+                                          uint32_t tw, uint32_t th, uint32_t s_lo, uint32_t s_hi,
+                                          unsigned long long (*acc)[4], uint32_t* next, int* stack, uint32_t& err,
+                                          uint32_t& nseg, uint32_t& nsh, TestTally* tally) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    acc[lane][0] = acc[lane][1] = acc[lane][2] = acc[lane][3] = 0ull;
+    if (lane == 0) *next = 0u;
+    __syncwarp(full);
+    const uint32_t nv = tw * th;
+    const uint32_t n_items = s_hi > s_lo ? nv * (s_hi - s_lo) : 0u;
+    int state = ST_IDLE;
+    uint32_t cur = 0, pixel = 0;
+    Path P;
+    Pending pend;
+    for (;;) {
+        if (state == ST_IDLE) {
+            const uint32_t idx = atomicAdd(next, 1u);
+            if (idx < n_items) {
+                cur = idx % nv;
+                const uint32_t st = s_lo + idx / nv;
+                const uint32_t gi = x0 + cur % tw + R.crop_x, gj = y0 + cur / tw + R.crop_y;
+                pixel = gj * R.full_w + gi;
+                start_path(S, R, gi, gj, pixel, st, P);
+                state = R.max_depth > 0 ? ST_CLOSEST : ST_DONE;
+            }
+        }
+        if (!__any_sync(full, state != ST_IDLE)) break;
+        if (state == ST_CLOSEST || state == ST_SHADOW) {
+            const bool shadow = state == ST_SHADOW;
+            Ray r;
+            r.o = P.ray.o;
+            r.d = shadow ? pend.dir : P.ray.d;
+            r.time = shadow ? 0.0f : P.ray.time;                  // Ray::new (render.rs:1457)
+            Hit h;
+            h.t = shadow ? pend.tmax : CUDART_INF_F;
+            h.prim = -1;
+            h.b1 = h.b2 = 0.0f;
+            const bool found = trace<COUNT>(S, r, 0.001f, shadow, h, stack, err, tally);
+            if (shadow) {
+                ++nsh;
+                if (!found) P.L = P.L + pend.contrib;
+                state = P.bounce >= R.max_depth ? ST_DONE : ST_CLOSEST;
+            } else {
+                ++nseg;
+                state = shade(S, R, pixel, P, found, h, pend);
+            }
+        }
+        if (state == ST_DONE) {
+            // luminance clamp and filter weight (render.rs:1692-1701)
+            const float lum = 0.2126f * P.L.x + 0.7152f * P.L.y + 0.0722f * P.L.z;
+            const V cl = lum > 100.0f ? P.L * (100.0f / lum) : P.L;
+            const float w = filter_weight(R.pixel_filter, P.jx - 0.5f, P.jy - 0.5f);
+            atomicAdd(&acc[cur][0], to_fixed(cl.x * w));
+            atomicAdd(&acc[cur][1], to_fixed(cl.y * w));
+            atomicAdd(&acc[cur][2], to_fixed(cl.z * w));
+            atomicAdd(&acc[cur][3], to_fixed(w));
+            state = ST_IDLE;
+        }
+    }
+    __syncwarp(full);
+}
+
+}  // namespace lum

@@ -33,6 +33,7 @@
 
 #include "kernels.h"
 #include "scene_access.h"
+#include "render_task.cuh"
 #include "tracer.cuh"
 
 namespace lum {
@@ -342,8 +343,9 @@ __global__ void k_finalize(Tables T, float* const* outs) {
 // warp-task queue that spans every scene, one persistent launch for the batch.  A task is one
 // 8x4 tile of one scene and one group of at most kGroupStrata of its strata; scenes are queued
 // heaviest task first (order[]).
-// Each task adds its per-pixel partial sums to the scene's 64-bit fixed-point accumulators
-// (order-free, hence deterministic) and k_finalize writes the images.  Scene descriptors are
+// Each task runs as the plain megakernel's (tile_task: the warp's lanes share the task's
+// (pixel, stratum) pairs) and adds its fixed-point pixel sums to the scene's accumulators;
+// k_finalize writes the images, equal bit for bit to lum_render's.  Scene descriptors are
 // read in place (constant or global memory) rather than copied per task.
 constexpr uint32_t kGroupStrata = 256;   // whole tiles up to 256 spp: the batch's queue is long anyway
 
@@ -359,8 +361,10 @@ __global__ void __launch_bounds__(128, 5) k_render_multi(Tables T, const unsigne
                                                          const uint32_t* order, const uint2* groups, Ctl* ctl,
                                                          uint32_t* next_task) {
     extern __shared__ int s_stack[];
+    __shared__ unsigned long long s_acc[4][32][4];
+    __shared__ uint32_t s_next[4];
     int* stack = s_stack + threadIdx.x;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const unsigned long long total = task_prefix[T.n];
     uint32_t err = 0, nseg = 0, nsh = 0;
     for (;;) {
@@ -379,61 +383,17 @@ __global__ void __launch_bounds__(128, 5) k_render_multi(Tables T, const unsigne
         const uint2 grp = groups[s];                       // (n_groups, strata per group)
         const uint32_t t = task - (uint32_t)task_prefix[lo];
         const uint32_t tile = t / grp.x, group = t - tile * grp.x;
-        const uint32_t i = (tile % R.tiles_x) * 8 + (lane & 7);
-        const uint32_t j = (tile / R.tiles_x) * 4 + (lane >> 3);
-        const bool valid = i < R.w && j < R.h;
-        const uint32_t gi = i + R.crop_x, gj = j + R.crop_y;
-        const uint32_t pixel = gj * R.full_w + gi;
-        V acc = mk(0.f, 0.f, 0.f);
-        float wsum = 0.0f;
-        uint32_t st = R.s_begin + group * grp.y;
-        const uint32_t s_end = min(R.s_end, st + grp.y);
-        int state = ST_IDLE;
-        Path P;
-        Pending pend;
-        for (;;) {
-            if (state == ST_IDLE && valid && st < s_end) {
-                start_path(S, R, gi, gj, pixel, st, P);
-                ++st;
-                state = R.max_depth > 0 ? ST_CLOSEST : ST_DONE;
-            }
-            if (!__any_sync(kFullMask, state != ST_IDLE)) break;
-            if (state == ST_CLOSEST || state == ST_SHADOW) {
-                const bool shadow = state == ST_SHADOW;
-                Ray r;
-                r.o = P.ray.o;
-                r.d = shadow ? pend.dir : P.ray.d;
-                r.time = shadow ? 0.0f : P.ray.time;
-                Hit h;
-                h.t = shadow ? pend.tmax : CUDART_INF_F;
-                h.prim = -1;
-                h.b1 = h.b2 = 0.0f;
-                const bool found = trace(S, r, 0.001f, shadow, h, stack, err);
-                if (shadow) {
-                    ++nsh;
-                    if (!found) P.L = P.L + pend.contrib;
-                    state = P.bounce >= R.max_depth ? ST_DONE : ST_CLOSEST;
-                } else {
-                    ++nseg;
-                    state = shade(S, R, pixel, P, found, h, pend);
-                }
-            }
-            if (state == ST_DONE) {
-                float lum = 0.2126f * P.L.x + 0.7152f * P.L.y + 0.0722f * P.L.z;
-                V cl = lum > 100.0f ? P.L * (100.0f / lum) : P.L;
-                float w = filter_weight(R.pixel_filter, P.jx - 0.5f, P.jy - 0.5f);
-                acc = fma3(cl, w, acc);
-                wsum += w;
-                state = ST_IDLE;
-            }
-        }
-        if (valid) {
+        const uint32_t x0 = (tile % R.tiles_x) * 8, y0 = (tile / R.tiles_x) * 4;
+        const uint32_t tw = min(8u, R.w - x0), th = min(4u, R.h - y0);
+        const uint32_t s_lo = R.s_begin + group * grp.y;
+        const uint32_t s_hi = min(R.s_end, s_lo + grp.y);
+        tile_task<false>(S, R, x0, y0, tw, th, s_lo, s_hi, s_acc[wid], &s_next[wid], stack, err, nseg, nsh, nullptr);
+        if (lane < (int)(tw * th)) {
+            const uint32_t i = x0 + lane % tw, j = y0 + lane / tw;
             unsigned long long* a = T.acc + 4 * (T.acc_off[s] + (size_t)j * R.w + i);
-            atomicAdd(a, (unsigned long long)fix(acc.x));
-            atomicAdd(a + 1, (unsigned long long)fix(acc.y));
-            atomicAdd(a + 2, (unsigned long long)fix(acc.z));
-            atomicAdd(a + 3, (unsigned long long)fix(wsum));
+            for (int c = 0; c < 4; ++c) atomicAdd(a + c, s_acc[wid][lane][c]);
         }
+        __syncwarp(kFullMask);
         if (lane == 0) {
             unsigned long long k = atomicAdd(T.done_count + s, 1ull) + 1ull;
             if (k == task_prefix[lo + 1] - task_prefix[lo]) T.finish_ns[s] = globaltimer();

@@ -1,10 +1,8 @@
-"""GPU tests of the batched wavefront tracer (lum_batch_*).
+"""GPU tests of the batched tracer (lum_batch_*), both modes.
 
-The wavefront traces the same keyed paths as the megakernel (same device functions), so
-each scene's image must equal lum_render's up to the float rounding of the per-pixel sum
-(f32 running sum in the megakernel, 64-bit fixed point in the batch): >= 99% of pixels
-within rtol 1e-5 / atol 1e-6 (a path whose discrete decision flips on a last-bit difference
-may differ), image means within 1e-4 relative.
+Every path is traced from the same RNG key by the same device functions, and every kernel adds
+finished paths to 64-bit fixed-point pixel sums (integer sums do not depend on the order in
+which paths finish), so each scene's image must equal lum_render's bit for bit.
 """
 import numpy as np
 import pytest
@@ -32,9 +30,7 @@ def small_batch():
 
 
 def compare(img, ref):
-    close = np.abs(img - ref) <= 1e-5 * np.abs(ref) + 1e-6
-    assert close.all(axis=2).mean() >= 0.99, close.all(axis=2).mean()
-    assert np.allclose(img.mean(), ref.mean(), rtol=1e-4, atol=1e-7)
+    np.testing.assert_array_equal(img, ref)
 
 
 @pytest.mark.parametrize("sort_threshold", [0, 1 << 16, 0xFFFFFFFF])
@@ -81,8 +77,7 @@ def test_batched_megakernel_mode_equals_lum_render():
     imgs, done, st = b.render()
     assert st.error_flags == 0 and st.segments > 0
     for img, ref in zip(imgs, refs):
-        # same paths; lum_render adds stratum-group sums for small frames, so f32 sums differ in order
-        np.testing.assert_allclose(img, ref, rtol=1e-5, atol=1e-6)
+        compare(img, ref)
     assert all(0 < t <= st.device_ms + 1e-3 for t in done)
 
 

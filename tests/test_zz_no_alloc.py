@@ -5,8 +5,8 @@ memory at start-up, or whose free memory is held by another allocator's pool, wh
 render-time allocation would fail or stall on device-wide synchronisation.  For them
 lum_render_noalloc keeps the device image and the kernel's counters in one fixed array
 (LUM_NOALLOC_MAX_PIXELS pixels) instead of allocating.  This file checks, through the C ABI,
-that two calls in a row return the same image as lum_render (same kernel and seeds; the
-tolerance of the other render tests' exact comparisons, rtol 1e-6), that the shared array is
+that two calls in a row return the same image as lum_render, bit for bit (same kernel and
+seeds; pixel sums in 64-bit fixed point do not depend on path order), that the shared array is
 reused cleanly by a call with another scene and size, and that images beyond the maximum are
 rejected.  It is named to be collected last.
 """
@@ -45,9 +45,9 @@ def test_noalloc_matches_render_on_two_calls_in_a_row():
     for _ in range(2):
         rc, out, st = _call(sc, cfg)
         assert rc == abi.LUM_OK, L.lib().lum_last_error()
-        # lum_render splits the strata of this small frame into groups and adds the group sums;
-        # the allocation-free path sums each pixel in one pass: same paths, f32 sum order differs
-        np.testing.assert_allclose(out, ref, rtol=1e-5, atol=1e-6)
+        # lum_render splits this small frame's strata into groups, the allocation-free path does
+        # not; both add the same paths in 64-bit fixed point, so the images are identical
+        np.testing.assert_array_equal(out, ref)
         assert st.paths == ref_st.paths == 96 * 64 * 16
         assert st.segments == ref_st.segments and st.error_flags == 0
 
@@ -59,12 +59,12 @@ def test_noalloc_reuses_the_shared_array_across_scenes_and_sizes():
     ref, _ = sc.render(cfg)
     rc, out, _ = _call(sc, cfg)
     assert rc == abi.LUM_OK, L.lib().lum_last_error()
-    np.testing.assert_allclose(out, ref, rtol=1e-6, atol=1e-7)
+    np.testing.assert_array_equal(out, ref)
     cfg.crop = (10, 5, 40, 30)                 # smaller region after a larger one
     ref2, _ = sc.render(cfg)
     rc, out2, _ = _call(sc, cfg)
     assert rc == abi.LUM_OK, L.lib().lum_last_error()
-    np.testing.assert_allclose(out2, ref2, rtol=1e-6, atol=1e-7)
+    np.testing.assert_array_equal(out2, ref2)
 
 
 def test_noalloc_rejects_images_beyond_the_maximum():
