@@ -552,7 +552,7 @@ def batched_measure(args, steps, warmup, with_clocks=True):
         "config": {"workload": f"batched: {len(cfgs)} uneven scenes, {paths} paths per step",
                    "scenes": len(cfgs), "prims": sum(w.n_prims() for w, _ in items),
                    "l2": "working set of the batch exceeds L2 (pool, queues, 64 scenes)"},
-        "batch_mode": "megakernel" if batch.config().get("mode") == 1 else "wavefront",
+        "batch_mode": {0: "wavefront", 1: "megakernel", 2: "streams"}[batch.config().get("mode")],
         "sequential_megakernel": {"value": paths * steps / seq_s / 1e6, "unit": "Mpaths/s",
                                   "ms_per_step": seq_s * 1e3 / steps},
         "speedup_vs_sequential": seq_s / bat_s,

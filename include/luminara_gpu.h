@@ -382,7 +382,9 @@ lum_status lum_backward(lum_scene* scene, const lum_render_params* params, const
  * ---------------------------------------------------------------------------------- */
 enum {
     LUM_BATCH_WAVEFRONT = 0,  /* path pool, material-sorted queues, graph-captured iterations */
-    LUM_BATCH_MEGAKERNEL = 1  /* one persistent megakernel whose tile queue spans all scenes */
+    LUM_BATCH_MEGAKERNEL = 1, /* one persistent megakernel whose tile queue spans all scenes */
+    LUM_BATCH_STREAMS = 2     /* lum_render's megakernel once per scene, heaviest first, over 4
+                                 streams: a scene's tail overlaps the next scene's start */
 };
 typedef struct lum_batch_config {
     uint32_t pool_paths;      /* wavefront: path slots in flight (1024 .. 2^24) */
@@ -408,8 +410,9 @@ typedef struct lum_batch_stats {
 typedef struct lum_batch lum_batch; /* opaque; references its scenes, which must outlive it */
 
 lum_status lum_batch_default_config(lum_batch_config* cfg);
-/* Times candidate configurations (mode; pool size, block size, sort threshold) on a calibration
- * run of the batch (about 1/8 of each scene's strata) and returns the fastest; results are
+/* Times candidate configurations (mode; pool size, block size, sort threshold) on calibration
+ * runs of the batch -- all of them on 1/8 of each scene's strata, the three fastest again on
+ * 1/4 -- and returns the fastest of the second round (best_ms is its time); results are
  * cached per device and batch signature in $LUM_AUTOTUNE_CACHE (default
  * ~/.cache/luminara_b200_autotune.txt).  best_ms may be NULL; it is -1 on a cache hit. */
 lum_status lum_batch_autotune(lum_scene* const* scenes, const lum_render_params* params, uint32_t n,

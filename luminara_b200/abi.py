@@ -68,6 +68,7 @@ FILTER_MITCHELL = 3
 
 BATCH_WAVEFRONT = 0
 BATCH_MEGAKERNEL = 1
+BATCH_STREAMS = 2
 
 KERR_STACK_OVERFLOW = 1 << 0
 KERR_QUEUE_OVERFLOW = 1 << 1

@@ -84,14 +84,11 @@ __device__ __forceinline__ void tile_task(const SceneDev& S, const RenderDev& R,
             }
         }
         if (state == ST_DONE) {
-            // luminance clamp and filter weight (render.rs:1692-1701)
-            const float lum = 0.2126f * P.L.x + 0.7152f * P.L.y + 0.0722f * P.L.z;
-            const V cl = lum > 100.0f ? P.L * (100.0f / lum) : P.L;
-            const float w = filter_weight(R.pixel_filter, P.jx - 0.5f, P.jy - 0.5f);
-            atomicAdd(&acc[cur][0], to_fixed(cl.x * w));
-            atomicAdd(&acc[cur][1], to_fixed(cl.y * w));
-            atomicAdd(&acc[cur][2], to_fixed(cl.z * w));
-            atomicAdd(&acc[cur][3], to_fixed(w));
+            const float4 v = path_sample(R, P.L, P.jx, P.jy);
+            atomicAdd(&acc[cur][0], to_fixed(v.x));
+            atomicAdd(&acc[cur][1], to_fixed(v.y));
+            atomicAdd(&acc[cur][2], to_fixed(v.z));
+            atomicAdd(&acc[cur][3], to_fixed(v.w));
             state = ST_IDLE;
         }
     }

@@ -682,20 +682,40 @@ __device__ __forceinline__ V background(const RenderDev& R, const Ray& r) {  // 
     return mk(1.f, 1.f, 1.f) * (1.0f - t) + mk(0.5f, 0.7f, 1.0f) * t;
 }
 
+// The pixel filter is written with explicitly rounded operations (no FMA contraction): the
+// compiler contracts a*b+c per call site, so the same expression could round differently in the
+// megakernel and in the wavefront kernels, and the images of both must agree bit for bit.
 __device__ __forceinline__ float mitchell_1d(float x) {                // render.rs:220-237
     x = fabsf(x);
     const float b = 1.0f / 3.0f, c = 1.0f / 3.0f;
+    const float x2 = __fmul_rn(x, x), x3 = __fmul_rn(x2, x);
     if (x < 1.0f)
-        return ((12.f - 9.f * b - 6.f * c) * x * x * x + (-18.f + 12.f * b + 6.f * c) * x * x + (6.f - 2.f * b)) / 6.f;
+        return __fdiv_rn(__fadd_rn(__fadd_rn(__fmul_rn(12.f - 9.f * b - 6.f * c, x3),
+                                             __fmul_rn(-18.f + 12.f * b + 6.f * c, x2)),
+                                   6.f - 2.f * b), 6.f);
     if (x < 2.0f)
-        return ((-b - 6.f * c) * x * x * x + (6.f * b + 30.f * c) * x * x + (-12.f * b - 48.f * c) * x + (8.f * b + 24.f * c)) / 6.f;
+        return __fdiv_rn(__fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(-b - 6.f * c, x3), __fmul_rn(6.f * b + 30.f * c, x2)),
+                                             __fmul_rn(-12.f * b - 48.f * c, x)),
+                                   8.f * b + 24.f * c), 6.f);
     return 0.0f;
 }
 __device__ __forceinline__ float filter_weight(int f, float dx, float dy) {  // render.rs:201-216
-    if (f == 1) return fmaxf(1.0f - fabsf(dx) * 2.0f, 0.0f) * fmaxf(1.0f - fabsf(dy) * 2.0f, 0.0f);
-    if (f == 2) return __expf(-(dx * dx + dy * dy) / (2.0f * 0.35f * 0.35f));
-    if (f == 3) return mitchell_1d(dx * 2.0f) * mitchell_1d(dy * 2.0f);
+    if (f == 1)
+        return __fmul_rn(fmaxf(__fsub_rn(1.0f, __fmul_rn(fabsf(dx), 2.0f)), 0.0f),
+                         fmaxf(__fsub_rn(1.0f, __fmul_rn(fabsf(dy), 2.0f)), 0.0f));
+    if (f == 2) return __expf(__fdiv_rn(-__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), 2.0f * 0.35f * 0.35f));
+    if (f == 3) return __fmul_rn(mitchell_1d(__fmul_rn(dx, 2.0f)), mitchell_1d(__fmul_rn(dy, 2.0f)));
     return 1.0f;
+}
+
+// A finished path's contribution to its pixel (render.rs:1692-1701): radiance clamped to
+// luminance 100, times the filter weight, and the weight; explicitly rounded like the filter.
+__device__ __forceinline__ float4 path_sample(const RenderDev& R, V L, float jx, float jy) {
+    const float lum = __fadd_rn(__fadd_rn(__fmul_rn(0.2126f, L.x), __fmul_rn(0.7152f, L.y)), __fmul_rn(0.0722f, L.z));
+    const float k = lum > 100.0f ? __fdiv_rn(100.0f, lum) : 1.0f;
+    const float w = filter_weight(R.pixel_filter, __fsub_rn(jx, 0.5f), __fsub_rn(jy, 0.5f));
+    if (lum > 100.0f) L = V{__fmul_rn(L.x, k), __fmul_rn(L.y, k), __fmul_rn(L.z, k)};
+    return make_float4(__fmul_rn(L.x, w), __fmul_rn(L.y, w), __fmul_rn(L.z, w), w);
 }
 
 // ------------------------------------------------------------------------------ path state

@@ -135,14 +135,12 @@ __device__ __forceinline__ long long fix(float v) { return llrint((double)v * kF
 // fixed-point accumulators of its pixel; per-scene completion bookkeeping.
 __device__ __forceinline__ void finish(const Tables& T, const Ctl* ctl, const RenderDev& R, uint32_t scene,
                                        uint32_t out_idx, const Path& P) {
-    float lum = 0.2126f * P.L.x + 0.7152f * P.L.y + 0.0722f * P.L.z;
-    V cl = lum > 100.0f ? P.L * (100.0f / lum) : P.L;
-    float w = filter_weight(R.pixel_filter, P.jx - 0.5f, P.jy - 0.5f);
+    const float4 v = path_sample(R, P.L, P.jx, P.jy);
     unsigned long long* a = T.acc + 4 * (T.acc_off[scene] + out_idx);
-    atomicAdd(a + 0, (unsigned long long)fix(cl.x * w));
-    atomicAdd(a + 1, (unsigned long long)fix(cl.y * w));
-    atomicAdd(a + 2, (unsigned long long)fix(cl.z * w));
-    atomicAdd(a + 3, (unsigned long long)fix(w));
+    atomicAdd(a + 0, (unsigned long long)fix(v.x));
+    atomicAdd(a + 1, (unsigned long long)fix(v.y));
+    atomicAdd(a + 2, (unsigned long long)fix(v.z));
+    atomicAdd(a + 3, (unsigned long long)fix(v.w));
     unsigned long long k = atomicAdd(T.done_count + scene, 1ull) + 1ull;
     if (k == T.scene_total[scene]) {
         T.finish_ns[scene] = globaltimer();
@@ -347,6 +345,7 @@ __global__ void k_finalize(Tables T, float* const* outs) {
 // (pixel, stratum) pairs) and adds its fixed-point pixel sums to the scene's accumulators;
 // k_finalize writes the images, equal bit for bit to lum_render's.  Scene descriptors are
 // read in place (constant or global memory) rather than copied per task.
+constexpr uint32_t kLanes = 4;           // streams of the streams mode
 constexpr uint32_t kGroupStrata = 256;   // whole tiles up to 256 spp: the batch's queue is long anyway
 
 // Scene and render descriptors of batches of up to kConstScenes scenes live in constant memory,
@@ -472,6 +471,11 @@ struct lum_batch {
     uint32_t* d_order = nullptr;                   // queue position -> scene
     uint2* d_groups = nullptr;                     // per scene: (stratum groups, strata per group)
     int grid_mega = 0;
+    // streams mode
+    std::vector<cudaStream_t> lanes;
+    std::vector<cudaEvent_t> scene_ev;            // per scene: its last kernel done
+    std::vector<uint32_t> lane_order;             // launch order (heaviest first)
+    lum::WorkCounters* d_wc = nullptr;            // per scene
 };
 
 namespace {
@@ -496,10 +500,68 @@ lum_status enqueue_iteration(lum_batch* b) {
 
 std::mutex g_const_mu;   // guards the constant scene tables of megakernel-mode renders
 
+// Streams mode: each scene is lum_render's launch (the megakernel, stratum groups as
+// lum_render chooses them, the scene's slice of the batch accumulators as their fixed-point
+// sums), issued heaviest first round robin over the lanes with no host synchronisation in
+// between, so the hardware starts a scene's CTAs as the previous scenes' CTAs retire.
+lum_status run_lanes(lum_batch* b, float* const* d_outs, double* scene_done_ms, lum_batch_stats* stats,
+                     std::chrono::steady_clock::time_point t0) {
+    using namespace lum::wf;
+    WF(cudaMemsetAsync(b->d_wc, 0, sizeof(lum::WorkCounters) * b->n, b->stream), "memset counters");
+    WF(cudaEventRecord(b->ev0, b->stream), "event");
+    for (cudaStream_t l : b->lanes) WF(cudaStreamWaitEvent(l, b->ev0, 0), "fork");
+    for (uint32_t q = 0; q < b->n; ++q) {
+        const uint32_t s = b->lane_order[q];
+        cudaStream_t l = b->lanes[q % b->lanes.size()];
+        const lum::RenderDev& R = b->R[s];
+        if (R.n_tasks > 0 && R.s_end > R.s_begin) {
+            const lum::RenderGroups grp = lum::render_groups(R);
+            unsigned long long* gacc = grp.n_groups > 1 ? b->T.acc + 4 * b->acc_off[s] : nullptr;
+            WF(lum::launch_render_grouped(b->S[s], R, d_outs[s], b->d_wc + s, l, gacc, grp), "render launch");
+        } else if (R.w > 0 && R.h > 0) {
+            WF(cudaMemsetAsync(d_outs[s], 0, sizeof(float) * 3 * (size_t)R.w * R.h, l), "memset image");
+        }
+        WF(cudaEventRecord(b->scene_ev[s], l), "event");
+    }
+    for (uint32_t s = 0; s < b->n; ++s) WF(cudaStreamWaitEvent(b->stream, b->scene_ev[s], 0), "join");
+    WF(cudaEventRecord(b->ev1, b->stream), "event");
+    std::vector<lum::WorkCounters> wc(b->n);
+    WF(cudaMemcpyAsync(wc.data(), b->d_wc, sizeof(lum::WorkCounters) * b->n, cudaMemcpyDeviceToHost, b->stream),
+       "counters");
+    WF(cudaStreamSynchronize(b->stream), "batch");
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    unsigned long long segs = 0, shadows = 0;
+    uint32_t flags = 0;
+    for (uint32_t s = 0; s < b->n; ++s) {
+        segs += wc[s].segments;
+        shadows += wc[s].shadow_rays;
+        flags |= wc[s].error_flags;
+        if (scene_done_ms) {
+            float d = 0.0f;
+            cudaEventElapsedTime(&d, b->ev0, b->scene_ev[s]);
+            scene_done_ms[s] = d;
+        }
+    }
+    if (stats) {
+        stats->paths = b->total_work;
+        stats->segments = segs;
+        stats->shadow_rays = shadows;
+        stats->device_ms = ms;
+        stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        stats->graph_launches = 0;
+        stats->iterations = 1;
+        stats->error_flags = flags;
+    }
+    if (flags) return lum::set_error(LUM_ERR_KERNEL, "streams-mode batch reported error flags");
+    return LUM_OK;
+}
+
 lum_status run_batch(lum_batch* b, float* const* d_outs, double* scene_done_ms, lum_batch_stats* stats) {
     using namespace lum::wf;
     auto t0 = std::chrono::steady_clock::now();
     WF(cudaSetDevice(b->device), "cudaSetDevice");
+    if (b->cfg.mode == LUM_BATCH_STREAMS) return run_lanes(b, d_outs, scene_done_ms, stats, t0);
     WF(cudaMemcpyAsync(b->d_out_table, d_outs, sizeof(float*) * b->n, cudaMemcpyHostToDevice, b->stream), "outs");
     WF(cudaMemsetAsync(b->T.acc, 0, sizeof(unsigned long long) * 4 * b->total_pixels, b->stream), "memset acc");
     WF(cudaMemsetAsync(b->T.done_count, 0, sizeof(unsigned long long) * b->n, b->stream), "memset done");
@@ -638,8 +700,8 @@ lum_status create_batch(lum_scene* const* scenes, const lum_render_params* param
     }
     b->total_work = prefix[n];
     b->S = S;
-    const bool mega = cfg.mode == LUM_BATCH_MEGAKERNEL;
-    if (cfg.mode != LUM_BATCH_WAVEFRONT && !mega)
+    const bool mega = cfg.mode == LUM_BATCH_MEGAKERNEL, lanes = cfg.mode == LUM_BATCH_STREAMS;
+    if (cfg.mode != LUM_BATCH_WAVEFRONT && !mega && !lanes)
         return fail_out(lum::set_error(LUM_ERR_INVALID_ARGUMENT, "unknown batch mode"));
     // megakernel mode: tasks of one tile x one group of <= kGroupStrata strata, scenes queued
     // by decreasing task cost (strata per task x log2 of the primitive count), so the longest
@@ -661,13 +723,13 @@ lum_status create_batch(lum_scene* const* scenes, const lum_render_params* param
         tile_prefix[k + 1] = tile_prefix[k] + (unsigned long long)b->R[s].n_tasks * groups[s].x;
     }
     if (tile_prefix[n] > 0xFFFFFFFFull) return fail_out(lum::set_error(LUM_ERR_TOO_LARGE, "too many tiles in batch"));
-    const uint32_t Q = mega ? 1024u : cfg.pool_paths;
+    const uint32_t Q = mega || lanes ? 1024u : cfg.pool_paths;
     if (Q < 1024 || Q > (1u << 24)) return fail_out(lum::set_error(LUM_ERR_INVALID_ARGUMENT, "pool_paths out of range"));
     if (!mega && cfg.block_threads != 128 && cfg.block_threads != 256)
         return fail_out(lum::set_error(LUM_ERR_INVALID_ARGUMENT, "block_threads must be 128 or 256"));
     if (!mega && (cfg.iters_per_graph < 1 || cfg.iters_per_graph > 64))
         return fail_out(lum::set_error(LUM_ERR_INVALID_ARGUMENT, "iters_per_graph out of range"));
-    b->block = mega ? 128 : (int)cfg.block_threads;
+    b->block = mega || lanes ? 128 : (int)cfg.block_threads;
     b->stack_bytes = (size_t)lum::kStackDepth * b->block * sizeof(int);
 
     // one allocation: pool SoA, queues, tables, accumulators, staging images
@@ -688,6 +750,7 @@ lum_status create_batch(lum_scene* const* scenes, const lum_render_params* param
     size_t o_ctl = take(sizeof(Ctl)), o_outs = take(sizeof(float*) * n);
     size_t o_stage = take(12ull * b->total_pixels);
     size_t o_tpre = take(8ull * (n + 1)), o_next = take(4), o_order = take(4ull * n), o_groups = take(8ull * n);
+    size_t o_wc = take(sizeof(lum::WorkCounters) * n);
     cudaError_t e = cudaSetDevice(b->device);
     if (e != cudaSuccess) return fail_out(wf_cuda(e, "cudaSetDevice"));
     if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess ||
@@ -723,6 +786,7 @@ lum_status create_batch(lum_scene* const* scenes, const lum_render_params* param
     b->d_next_task = (uint32_t*)(m + o_next);
     b->d_order = (uint32_t*)(m + o_order);
     b->d_groups = (uint2*)(m + o_groups);
+    b->d_wc = (lum::WorkCounters*)(m + o_wc);
     if ((e = cudaMemcpy(m + o_scenes, S.data(), sizeof(lum::SceneDev) * n, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(m + o_renders, b->R.data(), sizeof(lum::RenderDev) * n, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(m + o_prefix, prefix.data(), 8ull * (n + 1), cudaMemcpyHostToDevice)) != cudaSuccess ||
@@ -750,6 +814,27 @@ lum_status create_batch(lum_scene* const* scenes, const lum_render_params* param
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_m, k_render_multi<true>, 128,
                                                   (size_t)lum::kStackDepth * 128 * sizeof(int));
     b->grid_mega = sms * std::max(occ_m, 1);
+
+    if (lanes) {
+        // streams mode: scenes launched by decreasing estimated time (paths x task cost per
+        // stratum), round robin over kLanes streams
+        b->lanes.assign(kLanes, nullptr);
+        for (auto& l : b->lanes)
+            if ((e = cudaStreamCreateWithFlags(&l, cudaStreamNonBlocking)) != cudaSuccess)
+                return fail_out(wf_cuda(e, "cudaStreamCreate"));
+        b->scene_ev.assign(n, nullptr);
+        for (auto& ev : b->scene_ev)
+            if ((e = cudaEventCreate(&ev)) != cudaSuccess) return fail_out(wf_cuda(e, "cudaEventCreate"));
+        std::vector<double> est(n);
+        for (uint32_t s = 0; s < n; ++s)
+            est[s] = (double)b->scene_total[s] * task_cost[s] / std::max(1u, groups[s].y);
+        b->lane_order.resize(n);
+        for (uint32_t s = 0; s < n; ++s) b->lane_order[s] = s;
+        std::stable_sort(b->lane_order.begin(), b->lane_order.end(),
+                         [&](uint32_t x, uint32_t y) { return est[x] > est[y]; });
+        *out = b;
+        return LUM_OK;
+    }
 
     // capture the batch's kernels into one graph: iters_per_graph wavefront iterations, or
     // the single persistent megakernel launch
@@ -797,7 +882,7 @@ std::string batch_key(lum_scene* const* scenes, const lum_render_params* params,
         paths += w * h * st * st;
         depth += params[s].max_depth;
     }
-    char buf[256];
+    char buf[512];
     snprintf(buf, sizeof buf, "%s|n=%u|paths=%llu|pixels=%llu|prims=%llu|depth=%llu", prop.name, n, paths, pixels,
              prims, depth);
     for (char* c = buf; *c; ++c)
@@ -869,14 +954,20 @@ lum_status lum_batch_autotune(lum_scene* const* scenes, const lum_render_params*
         if (best_ms) *best_ms = -1.0;
         return LUM_OK;
     }
-    // calibration batch: the same scenes, about an eighth of every scene's strata
-    std::vector<lum_render_params> cal(params, params + n);
-    for (auto& p : cal) {
-        uint32_t sq = (uint32_t)std::ceil(std::sqrt((double)p.samples_per_pixel));
-        uint32_t total = sq * sq;
-        uint32_t cnt = p.sample_count ? p.sample_count : total;
-        p.sample_count = std::max(1u, cnt / 8);
-    }
+    // Two rounds of successive halving: every candidate on a calibration batch of the same
+    // scenes with an eighth of each scene's strata, then the three fastest on a quarter of the
+    // strata (the short first round favours configurations that hide per-scene tails, which
+    // matter less at full size).
+    auto calibration = [&](uint32_t div) {
+        std::vector<lum_render_params> cal(params, params + n);
+        for (auto& p : cal) {
+            uint32_t sq = (uint32_t)std::ceil(std::sqrt((double)p.samples_per_pixel));
+            uint32_t total = sq * sq;
+            uint32_t cnt = p.sample_count ? p.sample_count : total;
+            p.sample_count = std::max(1u, cnt / div);
+        }
+        return cal;
+    };
     const uint32_t pools[] = {1u << 19, 1u << 20, 1u << 21};
     const uint32_t blocks[] = {128, 256};
     const uint32_t thresholds[] = {0u, 1u << 16, 0xFFFFFFFFu};
@@ -885,6 +976,8 @@ lum_status lum_batch_autotune(lum_scene* const* scenes, const lum_render_params*
         lum_batch_config c{};
         lum_batch_default_config(&c);
         c.mode = LUM_BATCH_MEGAKERNEL;
+        cands.push_back(c);
+        c.mode = LUM_BATCH_STREAMS;
         cands.push_back(c);
     }
     for (uint32_t q : pools)
@@ -898,29 +991,42 @@ lum_status lum_batch_autotune(lum_scene* const* scenes, const lum_render_params*
                 c.mode = LUM_BATCH_WAVEFRONT;
                 cands.push_back(c);
             }
+    // device ms of one render (after a warm-up render), or a negative value when it failed
+    auto time_cand = [&](const std::vector<lum_render_params>& cal, const lum_batch_config& c) {
+        lum_batch* b = nullptr;
+        if (create_batch(scenes, cal.data(), n, c, &b) != LUM_OK) return -1.0;
+        lum_batch_stats st{};
+        std::vector<float*> outs(n);
+        size_t off = 0;
+        for (uint32_t s = 0; s < n; ++s) {
+            outs[s] = b->d_staging + 3 * off;
+            off += (size_t)b->R[s].w * b->R[s].h;
+        }
+        lum_status rs = run_batch(b, outs.data(), nullptr, &st);   // warm-up
+        if (rs == LUM_OK) rs = run_batch(b, outs.data(), nullptr, &st);
+        lum_batch_destroy(b);
+        return rs == LUM_OK ? st.device_ms : -1.0;
+    };
+    std::vector<std::pair<double, size_t>> round1;
+    {
+        const auto cal = calibration(8);
+        for (size_t i = 0; i < cands.size(); ++i) {
+            const double t = time_cand(cal, cands[i]);
+            if (t >= 0.0) round1.push_back({t, i});
+        }
+    }
+    std::sort(round1.begin(), round1.end());
     lum_batch_config best{};
     double best_t = 1e30;
-    for (const lum_batch_config& cand : cands) {
-            {
-                const lum_batch_config& c = cand;
-                lum_batch* b = nullptr;
-                if (create_batch(scenes, cal.data(), n, c, &b) != LUM_OK) continue;
-                lum_batch_stats st{};
-                std::vector<float*> outs(n);
-                size_t off = 0;
-                for (uint32_t s = 0; s < n; ++s) {
-                    outs[s] = b->d_staging + 3 * off;
-                    off += (size_t)b->R[s].w * b->R[s].h;
-                }
-                lum_status rs = run_batch(b, outs.data(), nullptr, &st);   // warm-up
-                if (rs == LUM_OK) rs = run_batch(b, outs.data(), nullptr, &st);
-                lum_batch_destroy(b);
-                if (rs != LUM_OK) continue;
-                if (st.device_ms < best_t) {
-                    best_t = st.device_ms;
-                    best = c;
-                }
+    {
+        const auto cal = calibration(4);
+        for (size_t k = 0; k < round1.size() && k < 3; ++k) {
+            const double t = time_cand(cal, cands[round1[k].second]);
+            if (t >= 0.0 && t < best_t) {
+                best_t = t;
+                best = cands[round1[k].second];
             }
+        }
     }
     if (best_t >= 1e30) return lum::set_error(LUM_ERR_CUDA, "autotune: no configuration ran");
     *out = best;
@@ -979,6 +1085,11 @@ lum_status lum_batch_destroy(lum_batch* b) {
     if (!b) return LUM_OK;
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
+    for (cudaStream_t l : b->lanes) {
+        cudaStreamSynchronize(l);
+        cudaStreamDestroy(l);
+    }
+    for (cudaEvent_t e : b->scene_ev) cudaEventDestroy(e);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     if (b->d_mem) cudaFree(b->d_mem);

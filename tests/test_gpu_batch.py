@@ -68,12 +68,13 @@ def test_batch_is_deterministic_and_refills_a_small_pool():
         compare(img, ref)
 
 
-def test_batched_megakernel_mode_equals_lum_render():
+@pytest.mark.parametrize("mode", [abi.BATCH_MEGAKERNEL, abi.BATCH_STREAMS])
+def test_megakernel_modes_equal_lum_render(mode):
     items = small_batch()
     scenes = [L.GpuScene(w) for w, _ in items]
     cfgs = [c for _, c in items]
     refs = [s.render(c)[0] for s, c in zip(scenes, cfgs)]
-    b = L.Batch(scenes, cfgs, config={"mode": abi.BATCH_MEGAKERNEL})
+    b = L.Batch(scenes, cfgs, config={"mode": mode})
     imgs, done, st = b.render()
     assert st.error_flags == 0 and st.segments > 0
     for img, ref in zip(imgs, refs):
@@ -81,17 +82,21 @@ def test_batched_megakernel_mode_equals_lum_render():
     assert all(0 < t <= st.device_ms + 1e-3 for t in done)
 
 
-def test_batch_device_outputs_and_filters():
+@pytest.mark.parametrize("mode,pixel_filter", [(abi.BATCH_WAVEFRONT, abi.FILTER_GAUSSIAN),
+                                               (abi.BATCH_WAVEFRONT, abi.FILTER_MITCHELL),
+                                               (abi.BATCH_MEGAKERNEL, abi.FILTER_TRIANGLE),
+                                               (abi.BATCH_STREAMS, abi.FILTER_GAUSSIAN)])
+def test_batch_device_outputs_and_filters(mode, pixel_filter):
     import torch
     items = small_batch()[:3]
     for _, c in items:
-        c.pixel_filter = abi.FILTER_GAUSSIAN
+        c.pixel_filter = pixel_filter
         c.exposure = 0.5
     scenes = [L.GpuScene(w) for w, _ in items]
     cfgs = [c for _, c in items]
     refs = [s.render(c)[0] for s, c in zip(scenes, cfgs)]
     outs = [torch.empty(c.out_shape(), dtype=torch.float32, device="cuda") for c in cfgs]
-    b = L.Batch(scenes, cfgs, config="default")
+    b = L.Batch(scenes, cfgs, config={"mode": mode})
     b.render_device([o.data_ptr() for o in outs])
     for o, ref in zip(outs, refs):
         compare(o.cpu().numpy(), ref)
@@ -103,8 +108,8 @@ def test_autotuner_picks_and_caches(tmp_path, monkeypatch):
     scenes = [L.GpuScene(w) for w, _ in items]
     cfgs = [c for _, c in items]
     cfg, ms = L.autotune(scenes, cfgs)
-    assert ms > 0 and cfg["mode"] in (abi.BATCH_WAVEFRONT, abi.BATCH_MEGAKERNEL)
-    assert cfg["mode"] == abi.BATCH_MEGAKERNEL or cfg["pool_paths"] in (1 << 19, 1 << 20, 1 << 21)
+    assert ms > 0 and cfg["mode"] in (abi.BATCH_WAVEFRONT, abi.BATCH_MEGAKERNEL, abi.BATCH_STREAMS)
+    assert cfg["mode"] != abi.BATCH_WAVEFRONT or cfg["pool_paths"] in (1 << 19, 1 << 20, 1 << 21)
     cfg2, ms2 = L.autotune(scenes, cfgs)
     assert cfg2 == cfg and ms2 == -1.0
     b = L.Batch(scenes, cfgs)            # autotuned (cache hit)
