@@ -58,6 +58,7 @@ def parse_args():
     ap.add_argument("--adjoint-res", type=int, default=512, help="adjoint block: image side (workload: 512)")
     ap.add_argument("--adjoint-spp", type=int, default=64, help="adjoint block: samples per pixel (workload: 64)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-workload block")
+    ap.add_argument("--no-sampling", action="store_true", help="skip the adaptive / time-limit block")
     ap.add_argument("--scenes", type=int, default=64, help="batched workload: number of scenes")
     ap.add_argument("--max-res", type=int, default=1024, help="batched workload: largest resolution")
     ap.add_argument("--batch-config", default="auto", help="batched workload: auto | default | k=v,k=v")
@@ -374,6 +375,8 @@ def run_ours(args):
                          f"reference estimator restated in C++ f64 (oracle/, stream RNG), OpenMP over rows"}
 
     tone = tonemap_block(L, out, H, Wd, stream, hbm_peak, flush) if rank == 0 else None
+    sampling = (sampling_block(L, sc, cfg, out, stream)
+                if (rank == 0 and world_size == 1 and not args.no_sampling) else None)
     adjoint = (adjoint_block(L, args.adjoint_res, args.adjoint_spp)
                if (rank == 0 and world_size == 1 and not args.no_adjoint) else None)
     batched = None
@@ -398,7 +401,7 @@ def run_ours(args):
             "segments_per_path": segs / (paths_per_step * args.steps),
             "shadow_rays_per_path": shadows / (paths_per_step * args.steps),
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps,
-            "clocks": clock_info, "tonemap": tone, "adjoint": adjoint, "batched": batched,
+            "clocks": clock_info, "tonemap": tone, "sampling": sampling, "adjoint": adjoint, "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -439,6 +442,34 @@ def tonemap_block(L, hdr, H, Wd, stream, hbm_peak, flush):
     out["pixels"] = H * Wd
     out["l2"] = "flushed (256 MiB write) before each timed call"
     return out
+
+
+# ------------------------------------------------------------------------------ adaptive / time limit
+def sampling_block(L, sc, cfg, out, stream, threshold=0.03):
+    """The sample loop's in-loop branches on the headline frame (k_render_sampled): adaptive
+    sampling at the reference's default threshold, and a time limit of half the plain frame
+    time.  Kernel times (median of 5 after 2 warm-ups, lum_stats.kernel_ms); samples kept =
+    the reference's ray count."""
+    from dataclasses import replace
+
+    def run(c, n=5):
+        for _ in range(2):
+            sc.render_device(c, out.data_ptr(), stream.cuda_stream)
+        sts = [sc.render_device(c, out.data_ptr(), stream.cuda_stream) for _ in range(n)]
+        return statistics.median(s.kernel_ms for s in sts), sts[-1]
+
+    px = cfg.width * cfg.height
+    plain_ms, plain = run(cfg)
+    res = {"plain": {"ms": plain_ms, "samples": plain.paths, "segments": plain.segments}}
+    a_ms, a = run(replace(cfg, adaptive=True, adaptive_threshold=threshold))
+    res["adaptive"] = {"threshold": threshold, "ms": a_ms, "samples": a.paths, "avg_spp": a.paths / px,
+                       "segments": a.segments, "time_vs_plain": a_ms / plain_ms,
+                       "kept_mpaths_per_s": a.paths / a_ms / 1e3}
+    limit_s = plain_ms * 0.5e-3
+    t_ms, t = run(replace(cfg, time_limit=limit_s))
+    res["time_limit"] = {"limit_ms": limit_s * 1e3, "ms": t_ms, "samples": t.paths,
+                         "full_tiles_frac": (t.paths - px) / (plain.paths - px) if plain.paths > px else None}
+    return res
 
 
 # ------------------------------------------------------------------------------ adjoint

@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define LUM_ABI_VERSION 1
+#define LUM_ABI_VERSION 2
 
 typedef int32_t lum_status;
 enum {
@@ -219,7 +219,14 @@ typedef struct lum_render_params {
     uint32_t crop[4];           /* x, y, w, h  (src/render.rs:1575-1583) */
     uint32_t sample_begin;      /* first stratum index rendered (0 for a full render) */
     uint32_t sample_count;      /* strata rendered; 0 = all sqrt_spp^2 strata */
-    uint32_t reserved;
+    int32_t adaptive;           /* 1 = adaptive sampling (src/render.rs:1592, 1628-1676): strata in
+                                   order, a pixel stops once n >= max(spp/4, 16) and the standard
+                                   error of its clamped luminance is below adaptive_threshold; the
+                                   pixel is the plain mean (no pixel filter).  Needs all strata. */
+    double adaptive_threshold;  /* the reference's default is 0.03 (src/render.rs:456) */
+    double time_limit;          /* seconds; > 0: a tile that starts after the limit renders one
+                                   sample per pixel at the pixel centre (src/render.rs:1601-1623,
+                                   per row there); 0 = none */
 } lum_render_params;
 
 typedef struct lum_stats {

@@ -9,7 +9,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-LUM_ABI_VERSION = 1
+LUM_ABI_VERSION = 2
 
 # status codes
 LUM_OK = 0
@@ -188,7 +188,9 @@ class LumRenderParams(C.Structure):
         ("crop", C.c_uint32 * 4),
         ("sample_begin", C.c_uint32),
         ("sample_count", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("adaptive", C.c_int32),
+        ("adaptive_threshold", C.c_double),
+        ("time_limit", C.c_double),
     ]
 
 

@@ -744,6 +744,8 @@ lum_status adj_cuda(cudaError_t e, const char* what) {
 extern "C" {
 
 lum_status lum_forward(lum_scene* scene, const lum_render_params* params, float* out_rgb, lum_stats* stats) {
+    if (params && (params->adaptive || params->time_limit > 0.0))
+        return lum::set_error(LUM_ERR_UNSUPPORTED, "the differentiable render has no adaptive sampling or time limit");
     return lum_render(scene, params, out_rgb, stats);
 }
 

@@ -114,6 +114,8 @@ struct alignas(16) WorkCounters {
     unsigned long long segments;
     unsigned long long shadow_rays;
     TestTally tally;
+    unsigned long long samples;   // camera samples kept (adaptive / time-limited renders)
+    unsigned long long t0_ns;     // start of a time-limited render (%globaltimer)
 };
 
 struct RenderDev {

@@ -518,8 +518,27 @@ lum_status make_render_dev(const lum_scene* s, const lum_render_params& p, lum::
     return LUM_OK;
 }
 
+// Adaptive sampling or a time limit: the sample loop's in-loop branches (render.rs:1592-1678).
+bool sampled(const lum_render_params& p) { return p.adaptive != 0 || p.time_limit > 0.0; }
+
+lum::SamplingDev sampling_of(const lum_render_params& p, const lum::RenderDev& R) {
+    lum::SamplingDev A{};
+    A.adaptive = p.adaptive ? 1u : 0u;
+    A.min_samples = std::max<uint32_t>(R.sqrt_spp * R.sqrt_spp / 4, 16);   // render.rs:1592
+    A.threshold = p.adaptive_threshold;
+    if (p.time_limit > 0.0)
+        A.limit_ns = (unsigned long long)std::max(1.0, std::min(p.time_limit * 1e9, 1.8e19));
+    return A;
+}
+
 lum_status check_params(const lum_render_params* p) {
     if (!p) return fail(LUM_ERR_INVALID_ARGUMENT, "params is null");
+    if (sampled(*p)) {
+        const uint32_t sq = (uint32_t)std::ceil(std::sqrt((double)p->samples_per_pixel));
+        if (p->sample_begin != 0 || (p->sample_count != 0 && p->sample_count < sq * sq))
+            return fail(LUM_ERR_UNSUPPORTED, "adaptive sampling and the time limit need all strata "
+                                             "(sample_begin 0, sample_count 0)");
+    }
     if (p->background < LUM_BG_SKY || p->background > LUM_BG_SUN)
         return fail(LUM_ERR_INVALID_ARGUMENT, "unknown background %d", p->background);
     if (p->pixel_filter < LUM_FILTER_BOX || p->pixel_filter > LUM_FILTER_MITCHELL)
@@ -535,7 +554,11 @@ lum_status run_render(lum_scene* s, const lum_render_params* params, float* d_ou
     auto t0 = std::chrono::steady_clock::now();
     CU(cudaMemsetAsync(s->d_work, 0, sizeof(lum::WorkCounters), stream), "cudaMemsetAsync");
     CU(cudaEventRecord(s->ev0, stream), "cudaEventRecord");
-    if (R.n_tasks > 0 && R.s_end > R.s_begin) {
+    const bool smp = sampled(*params);
+    if (smp && R.n_tasks > 0) {
+        // adaptive sampling / time limit: one task per tile, all strata, no stratum groups
+        CU(lum::launch_render_sampled(s->dev, R, sampling_of(*params, R), d_out, s->d_work, stream), "render launch");
+    } else if (R.n_tasks > 0 && R.s_end > R.s_begin) {
         // frames with fewer tiles than resident warps split their strata into groups
         const lum::RenderGroups grp = lum::render_groups(R);
         unsigned long long* part = nullptr;
@@ -555,7 +578,7 @@ lum_status run_render(lum_scene* s, const lum_render_params* params, float* d_ou
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, s->ev0, s->ev1);
     if (stats) {
-        stats->paths = (uint64_t)R.w * R.h * (R.s_end - R.s_begin);
+        stats->paths = smp ? wc.samples : (uint64_t)R.w * R.h * (R.s_end - R.s_begin);
         stats->segments = wc.segments;
         stats->shadow_rays = wc.shadow_rays;
         stats->kernel_ms = ms;
@@ -885,6 +908,9 @@ lum_status prepare_render(lum_scene* s, const lum_render_params* params, SceneDe
     if (!s) return fail(LUM_ERR_INVALID_ARGUMENT, "scene is null");
     lum_status st = check_params(params);
     if (st != LUM_OK) return st;
+    if (sampled(*params))
+        return fail(LUM_ERR_UNSUPPORTED, "adaptive sampling and the time limit are lum_render / lum_render_device "
+                                         "/ lum_render_ldr features");
     st = make_render_dev(s, *params, R);
     if (st != LUM_OK) return st;
     CU(cudaSetDevice(s->device), "cudaSetDevice");
@@ -897,6 +923,9 @@ lum_status scene_view(lum_scene* s, const lum_render_params* params, SceneDev& d
     if (!s) return fail(LUM_ERR_INVALID_ARGUMENT, "scene is null");
     lum_status st = check_params(params);
     if (st != LUM_OK) return st;
+    if (sampled(*params))
+        return fail(LUM_ERR_UNSUPPORTED, "adaptive sampling and the time limit are lum_render / lum_render_device "
+                                         "/ lum_render_ldr features");
     st = make_render_dev(s, *params, R);
     if (st != LUM_OK) return st;
     dev = s->dev;

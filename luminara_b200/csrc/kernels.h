@@ -26,6 +26,18 @@ cudaError_t launch_render_grouped(const SceneDev& S, const RenderDev& R, float* 
 // Counter build of the megakernel: same image, plus node/primitive test tallies in wc->tally.
 cudaError_t launch_render_counted(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
                                   cudaStream_t stream);
+// The in-loop branches of the sample loop (render.rs:1601-1678): adaptive sampling and the
+// time limit.
+struct SamplingDev {
+    uint32_t adaptive;        // 1 = adaptive sampling
+    uint32_t min_samples;     // max(spp / 4, 16)
+    double threshold;         // standard-error threshold
+    unsigned long long limit_ns;   // 0 = no time limit
+};
+// Renders a frame with adaptive sampling and/or a time limit (one task per 8x4 tile, all
+// strata).  wc must be zeroed; wc->samples receives the samples kept.
+cudaError_t launch_render_sampled(const SceneDev& S, const RenderDev& R, const SamplingDev& A, float* out,
+                                  WorkCounters* wc, cudaStream_t stream);
 cudaError_t launch_intersect(const SceneDev& S, const lum_ray* rays, uint32_t n, lum_hit* hits, WorkCounters* wc,
                              cudaStream_t stream);
 cudaError_t launch_occluded(const SceneDev& S, const lum_ray* rays, uint32_t n, int32_t* occ, WorkCounters* wc,

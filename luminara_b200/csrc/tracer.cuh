@@ -729,14 +729,18 @@ struct Path {
     bool skip_emission;
 };
 
-// Camera ray of stratum st (render.rs:1683-1690, camera.rs:82-102).
-__device__ __forceinline__ void start_path(const SceneDev& S, const RenderDev& R, uint32_t gi, uint32_t gj,
-                                           uint32_t pixel, uint32_t st, Path& P) {
-    uint32_t sx = st % R.sqrt_spp, sy = st / R.sqrt_spp;
-    float4 c = draw4(R.key0, R.key1, pixel, st, 0, CALL_CAMERA);
-    float inv_n = 1.0f / (float)R.sqrt_spp;
-    P.jx = ((float)sx + c.x) * inv_n;
-    P.jy = ((float)sy + c.y) * inv_n;
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Camera ray through sub-pixel position (jx, jy) of pixel (gi, gj) for stratum st; c holds
+// the stratum's camera draws (z, w: lens) (render.rs:1683-1690, camera.rs:82-102).
+__device__ __forceinline__ void start_path_at(const SceneDev& S, const RenderDev& R, uint32_t gi, uint32_t gj,
+                                              uint32_t pixel, uint32_t st, float4 c, float jx, float jy, Path& P) {
+    P.jx = jx;
+    P.jy = jy;
     float y = (float)(R.full_h - 1 - gj);
     float uc = ((float)gi + P.jx) / (float)(R.full_w - 1);
     float vc = (y + P.jy) / (float)(R.full_h - 1);
@@ -755,6 +759,22 @@ __device__ __forceinline__ void start_path(const SceneDev& S, const RenderDev& R
     P.stratum = st;
     P.bounce = 0;
     P.skip_emission = false;
+}
+
+// Camera ray of stratum st: stratified jitter (render.rs:1683-1690).
+__device__ __forceinline__ void start_path(const SceneDev& S, const RenderDev& R, uint32_t gi, uint32_t gj,
+                                           uint32_t pixel, uint32_t st, Path& P) {
+    uint32_t sx = st % R.sqrt_spp, sy = st / R.sqrt_spp;
+    float4 c = draw4(R.key0, R.key1, pixel, st, 0, CALL_CAMERA);
+    float inv_n = 1.0f / (float)R.sqrt_spp;
+    start_path_at(S, R, gi, gj, pixel, st, c, ((float)sx + c.x) * inv_n, ((float)sy + c.y) * inv_n, P);
+}
+
+// The one sample of a pixel after the time limit: stratum 0's draws, the pixel centre
+// (render.rs:1612-1616).
+__device__ __forceinline__ void start_path_centre(const SceneDev& S, const RenderDev& R, uint32_t gi, uint32_t gj,
+                                                  uint32_t pixel, Path& P) {
+    start_path_at(S, R, gi, gj, pixel, 0, draw4(R.key0, R.key1, pixel, 0, 0, CALL_CAMERA), 0.5f, 0.5f, P);
 }
 
 // Path states of the megakernel lanes.

@@ -87,12 +87,6 @@ struct Tables {
     uint32_t sort_threshold;
 };
 
-__device__ __forceinline__ unsigned long long globaltimer() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
 // Appends `value` to queue q; lanes of the warp with the same queue share one atomic.
 __device__ __forceinline__ void append(uint32_t* q, uint32_t* counter, uint32_t value, unsigned group) {
     const int lane = threadIdx.x & 31;

@@ -279,6 +279,9 @@ class RenderConfig:
     crop: Optional[Sequence[int]] = None
     sample_begin: int = 0
     sample_count: int = 0
+    adaptive: bool = False
+    adaptive_threshold: float = 0.03
+    time_limit: float = 0.0
 
     def to_c(self) -> abi.LumRenderParams:
         p = abi.LumRenderParams()
@@ -299,6 +302,9 @@ class RenderConfig:
             p.crop[:] = [int(x) for x in self.crop]
         p.sample_begin = int(self.sample_begin)
         p.sample_count = int(self.sample_count)
+        p.adaptive = 1 if self.adaptive else 0
+        p.adaptive_threshold = float(self.adaptive_threshold)
+        p.time_limit = float(self.time_limit)
         return p
 
     def out_shape(self):

@@ -39,10 +39,10 @@ from . import abi
 from . import scene as S
 
 # RenderSettings keys the sample loop reads; every other [render] key is post-processing.
-_PATH_KEYS = {"width", "height", "samples", "max_depth", "seed", "exposure", "pixel_filter", "background"}
+_PATH_KEYS = {"width", "height", "samples", "max_depth", "seed", "exposure", "pixel_filter", "background",
+              "adaptive", "adaptive_threshold"}
 # [render] keys whose feature is in the sample loop but not built here.
-_UNBUILT_RENDER_KEYS = {"adaptive", "adaptive_threshold", "time_limit", "firefly_filter", "lens_distortion",
-                        "chromatic_aberration"}
+_UNBUILT_RENDER_KEYS = {"firefly_filter", "lens_distortion", "chromatic_aberration"}
 _SUPPORTED_TABLES = {"render", "camera", "sphere", "moving_sphere", "plane", "light", "fog", "disk", "triangle",
                      "quad", "mesh", "box", "rect_xy", "rect_xz", "rect_yz"}
 
@@ -193,6 +193,8 @@ class _Loader:
         cfg.max_depth = int(r.get("max_depth", cfg.max_depth))
         cfg.seed = int(r.get("seed", cfg.seed))
         cfg.exposure = float(r.get("exposure", cfg.exposure))
+        cfg.adaptive = bool(r.get("adaptive", cfg.adaptive))                    # scene.rs:914-919
+        cfg.adaptive_threshold = float(r.get("adaptive_threshold", cfg.adaptive_threshold))
         pf = r.get("pixel_filter")
         if pf is not None:
             cfg.pixel_filter = {"triangle": abi.FILTER_TRIANGLE, "tent": abi.FILTER_TRIANGLE,

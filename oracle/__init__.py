@@ -60,6 +60,7 @@ def lib():
         L.orc_occluded.argtypes = [vp, vp, C.c_uint32, vp]
         L.orc_tie_count.argtypes = [vp, vp, C.c_uint32, C.c_double, C.c_double, vp]
         L.orc_render.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.c_int, C.c_int, dp, C.POINTER(OrcStats)]
+        L.orc_render_expired.argtypes = L.orc_render.argtypes
         L.orc_render_rows.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.c_int, C.c_int, C.c_uint32,
                                       C.c_uint32, dp, C.POINTER(OrcStats)]
         L.orc_adjoint.argtypes = [vp, C.POINTER(abi.LumRenderParams), dp, vp, C.c_int, C.c_int, dp, dp, dp, dp]
@@ -127,12 +128,16 @@ class OracleScene:
         lib().orc_occluded(self.h, rays.ctypes.data, rays.shape[0], occ.ctypes.data)
         return occ
 
-    def render(self, cfg, mode=MODE_STREAM, threads=0, rows=None):
+    def render(self, cfg, mode=MODE_STREAM, threads=0, rows=None, expired=False):
+        """expired=True renders as if every row started after the time limit."""
         p = cfg.to_c()
         shape = cfg.out_shape()
         out = np.zeros(shape, dtype=np.float64)
         st = OrcStats()
-        if rows is None:
+        if expired:
+            rc = lib().orc_render_expired(self.h, C.byref(p), mode, threads,
+                                          out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(st))
+        elif rows is None:
             rc = lib().orc_render(self.h, C.byref(p), mode, threads,
                                   out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(st))
         else:

@@ -22,6 +22,7 @@
 #include "oracle.h"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -1591,16 +1592,83 @@ Frame frame_of(const lum_render_params& p) {
     return f;
 }
 
+V3 clamp_sample(V3 smp) {                                               // render.rs:1692-1697
+    double lum = 0.2126 * smp.x + 0.7152 * smp.y + 0.0722 * smp.z;
+    return lum > 100.0 ? smp * (100.0 / lum) : smp;
+}
+
+V3 trace_sample(const orc_scene& sc, const lum_render_params& p, const Ray& ray, Sampler& s, Counters& cnt) {
+    return s.mode == ORC_MODE_STREAM ? ray_color_stream(sc, p, ray, s, p.max_depth, false, cnt)
+                                     : ray_color_keyed(sc, p, ray, s, p.max_depth, cnt);
+}
+
+// One sample at the pixel centre after the time limit (render.rs:1612-1622): the lens and
+// time draws as usual (stratum 0 in keyed mode), luminance-clamped, no filter.
+V3 expired_sample(const orc_scene& sc, const lum_render_params& p, const Frame& f, Sampler& s, size_t gi, double y,
+                  Counters& cnt) {
+    s.stratum = 0;
+    s.begin_bounce(0);
+    double uc = ((double)gi + 0.5) / (double)(f.full_w - 1);
+    double vc = (y + 0.5) / (double)(f.full_h - 1);
+    Ray ray = sc.cam.get_ray(uc, vc, s);
+    return clamp_sample(trace_sample(sc, p, ray, s, cnt));
+}
+
+// Adaptive sampling (render.rs:1624-1678): strata in order sy-major; Welford's running mean
+// and squared deviations of the clamped luminance; stop once n >= min_samples, n > 1 and the
+// standard error sqrt(var / n) is below the threshold.  The pixel is the running mean of the
+// clamped samples (no pixel filter).
+V3 adaptive_pixel(const orc_scene& sc, const lum_render_params& p, const Frame& f, Sampler& s, size_t gi, double y,
+                  uint32_t min_samples, Counters& cnt, uint64_t& paths) {
+    V3 mean{0, 0, 0};
+    double m2_lum = 0.0, mean_lum = 0.0;
+    uint32_t n = 0;
+    const uint32_t total = f.sqrt_spp * f.sqrt_spp;
+    for (uint32_t st = 0; st < total; ++st) {
+        uint32_t sx = st % f.sqrt_spp, sy = st / f.sqrt_spp;
+        s.stratum = st;
+        s.begin_bounce(0);
+        double uc = ((double)gi + ((double)sx + s.draw(CALL_CAMERA, 0)) / (double)f.sqrt_spp) / (double)(f.full_w - 1);
+        double vc = (y + ((double)sy + s.draw(CALL_CAMERA, 1)) / (double)f.sqrt_spp) / (double)(f.full_h - 1);
+        Ray ray = sc.cam.get_ray(uc, vc, s);
+        V3 cl = clamp_sample(trace_sample(sc, p, ray, s, cnt));
+        ++n;
+        double lum = 0.2126 * cl.x + 0.7152 * cl.y + 0.0722 * cl.z;
+        double d1 = lum - mean_lum;
+        mean_lum += d1 / (double)n;
+        double d2 = lum - mean_lum;
+        m2_lum += d1 * d2;
+        mean = mean + (cl - mean) / (double)n;
+        if (n >= min_samples && n > 1) {
+            double var = m2_lum / (double)(n - 1);
+            if (std::sqrt(var / (double)n) < p.adaptive_threshold) break;
+        }
+    }
+    paths += n;
+    return mean;
+}
+
 }  // namespace
 
 extern "C" {
 
-int orc_render_rows(const orc_scene* sc, const lum_render_params* pp, int mode, int threads, uint32_t row_begin,
-                    uint32_t row_end, double* out, orc_stats* stats) {
+}  // extern "C"
+
+namespace {
+
+// The sample loop of render.rs:1598-1706.  expire: 0 = the wall-clock time limit of the
+// params (checked when a row starts, render.rs:1601-1605), 1 = every row starts after it.
+int render_rows(const orc_scene* sc, const lum_render_params* pp, int mode, int threads, uint32_t row_begin,
+                uint32_t row_end, double* out, orc_stats* stats, int expire) {
     if (!sc || !pp || !out) return 1;
     const lum_render_params& p = *pp;
     Frame f = frame_of(p);
-    if (mode == ORC_MODE_STREAM && (f.s_begin != 0 || f.s_end != f.sqrt_spp * f.sqrt_spp)) return 2;
+    const uint32_t actual_spp = f.sqrt_spp * f.sqrt_spp;
+    if (mode == ORC_MODE_STREAM && (f.s_begin != 0 || f.s_end != actual_spp)) return 2;
+    if (p.adaptive && (f.s_begin != 0 || f.s_end != actual_spp)) return 3;
+    // render.rs:1592: minimum samples before the variance test
+    const uint32_t min_samples = p.adaptive ? std::max<uint32_t>(actual_spp / 4, 16) : 0;
+    std::atomic<bool> expired{expire != 0};
     row_end = std::min<uint32_t>(row_end, (uint32_t)f.h);
     uint64_t segs = 0, shadows = 0, paths = 0;
     auto t0 = std::chrono::steady_clock::now();
@@ -1620,11 +1688,25 @@ int orc_render_rows(const orc_scene* sc, const lum_render_params* pp, int mode, 
         s.key[1] = (uint32_t)(p.seed >> 32);
         double y = (double)(f.full_h - 1 - gj);
         Counters cnt;
+        if (p.time_limit > 0.0 &&
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > p.time_limit)
+            expired.store(true, std::memory_order_relaxed);
+        const bool row_expired = expired.load(std::memory_order_relaxed);
         for (size_t i = 0; i < f.w; ++i) {
             size_t gi = i + f.crop_x;
             V3 color{0, 0, 0};
             double tw = 0.0;
             s.pixel = (uint32_t)(gj * f.full_w + gi);
+            double* o = out + ((size_t)j * f.w + i) * 3;
+            if (row_expired || p.adaptive) {
+                V3 px = row_expired ? expired_sample(*sc, p, f, s, gi, y, cnt)
+                                    : adaptive_pixel(*sc, p, f, s, gi, y, min_samples, cnt, paths);
+                paths += row_expired ? 1 : 0;
+                o[0] = px.x * p.exposure;
+                o[1] = px.y * p.exposure;
+                o[2] = px.z * p.exposure;
+                continue;
+            }
             for (uint32_t st = f.s_begin; st < f.s_end; ++st) {
                 uint32_t sx = st % f.sqrt_spp, sy = st / f.sqrt_spp;
                 s.stratum = st;
@@ -1644,7 +1726,6 @@ int orc_render_rows(const orc_scene* sc, const lum_render_params* pp, int mode, 
             }
             paths += f.s_end - f.s_begin;
             V3 px = tw > 0.0 ? color / tw : color;
-            double* o = out + ((size_t)j * f.w + i) * 3;
             o[0] = px.x * p.exposure;
             o[1] = px.y * p.exposure;
             o[2] = px.z * p.exposure;
@@ -1663,9 +1744,24 @@ int orc_render_rows(const orc_scene* sc, const lum_render_params* pp, int mode, 
     return 0;
 }
 
+}  // namespace
+
+extern "C" {
+
+int orc_render_rows(const orc_scene* sc, const lum_render_params* pp, int mode, int threads, uint32_t row_begin,
+                    uint32_t row_end, double* out, orc_stats* stats) {
+    return render_rows(sc, pp, mode, threads, row_begin, row_end, out, stats, 0);
+}
+
 int orc_render(const orc_scene* sc, const lum_render_params* p, int mode, int threads, double* out, orc_stats* st) {
     Frame f = frame_of(*p);
-    return orc_render_rows(sc, p, mode, threads, 0, (uint32_t)f.h, out, st);
+    return render_rows(sc, p, mode, threads, 0, (uint32_t)f.h, out, st, 0);
+}
+
+int orc_render_expired(const orc_scene* sc, const lum_render_params* p, int mode, int threads, double* out,
+                       orc_stats* st) {
+    Frame f = frame_of(*p);
+    return render_rows(sc, p, mode, threads, 0, (uint32_t)f.h, out, st, 1);
 }
 
 int orc_scatter(const lum_material* lm, const double ray[7], const double hp[3], const double on[3], double t,

@@ -63,9 +63,15 @@ int orc_intersect(const orc_scene* s, const orc_ray* rays, uint32_t n, orc_hit* 
 int orc_tie_count(const orc_scene* s, const orc_ray* rays, uint32_t n, double rel, double abs_eps, int32_t* counts);
 /* Shadow query: occluded[i] = world.hit(ray).is_some(). */
 int orc_occluded(const orc_scene* s, const orc_ray* rays, uint32_t n, int32_t* occluded);
-/* render() non-adaptive branch; out_rgb = W*H*3 doubles (exposure applied, not cast to f32). */
+/* render(): the stratified loop, or the adaptive loop when p->adaptive, and the time limit
+ * (p->time_limit, wall clock, checked when a row starts); out_rgb = W*H*3 doubles (exposure
+ * applied, not cast to f32); stats->paths counts the samples traced (the reference's rays). */
 int orc_render(const orc_scene* s, const lum_render_params* p, int mode, int threads,
                double* out_rgb, orc_stats* stats);
+/* As orc_render with every row starting after the time limit: one sample per pixel at the
+ * pixel centre (render.rs:1612-1622). */
+int orc_render_expired(const orc_scene* s, const lum_render_params* p, int mode, int threads,
+                       double* out_rgb, orc_stats* stats);
 /* Renders only rows [row_begin, row_end) of the (cropped) image into out_rgb rows of the
  * same index; used for bounded CPU-baseline samples. */
 int orc_render_rows(const orc_scene* s, const lum_render_params* p, int mode, int threads,

@@ -239,10 +239,17 @@ def test_meshes_from_obj_and_ply(tmp_path):
     assert np.isfinite(img).all()
 
 
+def test_adaptive_keys_reach_the_render_config():
+    cfg, _, _ = load_scene("[render]\nadaptive = true\nadaptive_threshold = 0.05\nsamples = 64\n")
+    assert cfg.adaptive and cfg.adaptive_threshold == 0.05
+    cfg, _, _ = load_scene("[render]\nsamples = 64\n")
+    assert not cfg.adaptive and cfg.adaptive_threshold == 0.03          # render.rs:455-456
+
+
 def test_unsupported_features_are_named():
     text = """
 [render]
-adaptive = true
+firefly_filter = 4.0
 background = { type = "starfield" }
 
 [camera]
@@ -263,7 +270,7 @@ material = { type = "marble", color = [0.5, 0.5, 0.5] }
     with pytest.raises(UnsupportedSceneError) as e:
         load_scene(text)
     items = e.value.items
-    for want in ("[torus]", "render.adaptive", "starfield", "camera.panorama", "bump_strength", "'marble'"):
+    for want in ("[torus]", "render.firefly_filter", "starfield", "camera.panorama", "bump_strength", "'marble'"):
         assert any(want in it for it in items), (want, items)
 
 
