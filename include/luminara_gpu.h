@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define LUM_ABI_VERSION 2
+#define LUM_ABI_VERSION 3
 
 typedef int32_t lum_status;
 enum {
@@ -120,7 +120,22 @@ enum {
     LUM_MAT_DIELECTRIC = 3, /* src/material.rs:111-214 */
     LUM_MAT_EMISSIVE = 4,   /* src/material.rs:218-244 */
     LUM_MAT_MICROFACET = 5, /* src/material.rs:248-391 */
-    LUM_MAT_ISOTROPIC = 6   /* src/constant_medium.rs:77-89 */
+    LUM_MAT_ISOTROPIC = 6,  /* src/constant_medium.rs:77-89 */
+    /* The other reference materials (src/material.rs:396-870).  Parameters beyond color /
+     * color2 / ior / roughness are in lum_material.extra[]; the constructors' clamps are
+     * applied by lum_scene_create. */
+    LUM_MAT_BLEND = 7,       /* :396-421  sub[0] = mat_a, sub[1] = mat_b, extra[0] = ratio
+                                (probability of mat_a).  Blends nest at most 4 deep. */
+    LUM_MAT_TRANSPARENT = 8, /* :427-440  no parameters */
+    LUM_MAT_IRIDESCENT = 9,  /* :447-528  color = base_color, extra[0] = thickness (nm),
+                                ior = film_ior, roughness */
+    LUM_MAT_TOON = 10,       /* :530-578  color, extra[0] = bands, extra[1] = specular */
+    LUM_MAT_ANISOTROPIC = 11,/* :581-642  color, extra[0] = roughness_u, extra[1] = roughness_v,
+                                extra[2] = tangent axis (0 x, 1 y, 2 z) */
+    LUM_MAT_CLEARCOAT = 12,  /* :645-708  color = base_color, extra[0] = coat_gloss, ior = coat_ior */
+    LUM_MAT_VELVET = 13,     /* :711-747  color, extra[0] = sheen */
+    LUM_MAT_TRANSLUCENT = 14,/* :750-798  color, extra[0] = translucency, extra[1] = scatter_width */
+    LUM_MAT_SUBSURFACE = 15  /* :801-865  color, extra[0] = mean_free_path, color2 = scatter_color */
 };
 enum {
     LUM_TEX_SOLID = 0,  /* src/texture.rs:9-23 */
@@ -139,6 +154,8 @@ typedef struct lum_material {
     double intensity;   /* Emissive */
     double dispersion;  /* Dielectric */
     double tint[3];     /* Dielectric Beer tint; (1,1,1) = clear */
+    int32_t sub[2];     /* Blend: the two blended materials */
+    double extra[4];    /* per-kind parameters (LUM_MAT_* above) */
 } lum_material;
 
 enum {
@@ -194,7 +211,10 @@ enum {
     LUM_BG_SKY = 0,      /* src/render.rs:75-79 */
     LUM_BG_SOLID = 1,    /* src/render.rs:80 */
     LUM_BG_GRADIENT = 2, /* src/render.rs:81-85 */
-    LUM_BG_SUN = 3       /* src/render.rs:152-169 */
+    LUM_BG_SUN = 3,      /* src/render.rs:152-169 */
+    LUM_BG_STARFIELD = 4,/* src/render.rs:86-112: bg_star_density, bg_star_brightness */
+    LUM_BG_ENVMAP = 5    /* src/render.rs:113-151: the scene's environment map
+                            (lum_scene_set_envmap) times bg_intensity */
 };
 enum {
     LUM_FILTER_BOX = 0, /* src/render.rs:201-237 */
@@ -227,6 +247,8 @@ typedef struct lum_render_params {
     double time_limit;          /* seconds; > 0: a tile that starts after the limit renders one
                                    sample per pixel at the pixel centre (src/render.rs:1601-1623,
                                    per row there); 0 = none */
+    double bg_star_density;     /* STARFIELD */
+    double bg_star_brightness;  /* STARFIELD */
 } lum_render_params;
 
 typedef struct lum_stats {
@@ -318,6 +340,21 @@ lum_status lum_render(lum_scene* scene, const lum_render_params* params, float* 
  * (cudaStream_t passed as void*, NULL = the scene's stream); no host copies. */
 lum_status lum_render_device(lum_scene* scene, const lum_render_params* params,
                              float* d_out_rgb, void* stream, lum_stats* stats);
+
+/* Environment map of LUM_BG_ENVMAP (Background::EnvMap, src/render.rs:113-151): an
+ * equirectangular linear RGB image, width*height*3 floats, top row first, copied to the
+ * scene's device memory (replacing any previous map; rgb NULL removes it). */
+lum_status lum_scene_set_envmap(lum_scene* scene, const float* rgb, uint32_t width, uint32_t height);
+
+/* AOV passes (src/render.rs:3508-3568): one ray per pixel through the pixel centre, its
+ * closest hit: depth = t (0 on a miss), W*H floats; normals = the hit normal facing the ray
+ * mapped to bytes ((n * 0.5 + 0.5) * 255, clamped, truncated), W*H*3; albedo = the scatter
+ * attenuation clamped to [0,1] * 255, or for a surface that does not scatter its emission
+ * divided by max(max component, 1), W*H*3.  Any output may be NULL.  Caller-owned HOST
+ * buffers (crop size when has_crop).  The lens and scatter draws come from the keyed RNG of
+ * (pixel, stratum 0), not the reference's per-pixel stream. */
+lum_status lum_render_aov(lum_scene* scene, const lum_render_params* params, float* depth,
+                          uint8_t* normals, uint8_t* albedo);
 
 /* Allocation-free render.  Same image as lum_render into the same caller-owned HOST buffer,
  * but it allocates no device memory, ever: the device image and the kernel's work counters

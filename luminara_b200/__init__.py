@@ -19,9 +19,10 @@ import numpy as np
 
 from . import abi
 from .scene import (  # noqa: F401  (re-exported reference names)
-    CameraConfig, Checker, ConstantMedium, Dielectric, Disk, Emissive, Isotropic, Lambertian, LightInfo, Mesh,
-    Metal, Microfacet, MovingSphere, Plane, Quad, RenderConfig, RotateX, RotateY, RotateZ, Scale, SolidColor,
-    Sphere, ToneMapConfig, Translate, Triangle, World, XyRect, XzRect, YzRect, make_box,
+    Anisotropic, Blend, CameraConfig, Checker, Clearcoat, ConstantMedium, Dielectric, Disk, Emissive, Iridescent,
+    Isotropic, Lambertian, LightInfo, Mesh, Metal, Microfacet, MovingSphere, Plane, Quad, RenderConfig, RotateX,
+    RotateY, RotateZ, Scale, SolidColor, Sphere, Subsurface, ToneMapConfig, Toon, Translate, Translucent,
+    Transparent, Triangle, Velvet, World, XyRect, XzRect, YzRect, make_box,
 )
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -71,6 +72,8 @@ def lib():
                                  C.POINTER(abi.LumStats)]
     L.lum_forward.argtypes = [vp, C.POINTER(abi.LumRenderParams), vp, C.POINTER(abi.LumStats)]
     L.lum_backward.argtypes = [vp, C.POINTER(abi.LumRenderParams), vp, vp, vp, vp, vp, C.POINTER(abi.LumStats)]
+    L.lum_scene_set_envmap.argtypes = [vp, vp, C.c_uint32, C.c_uint32]
+    L.lum_render_aov.argtypes = [vp, C.POINTER(abi.LumRenderParams), vp, vp, vp]
     L.lum_intersect.argtypes = [vp, vp, C.c_uint32, vp]
     L.lum_occluded.argtypes = [vp, vp, C.c_uint32, vp]
     PP = C.POINTER(C.c_void_p)
@@ -85,7 +88,7 @@ def lib():
     L.lum_batch_destroy.argtypes = [vp]
     for name in ("lum_scene_create", "lum_scene_destroy", "lum_scene_info", "lum_render", "lum_render_device",
                  "lum_count_tests", "lum_intersect", "lum_occluded", "lum_forward", "lum_backward",
-                 "lum_tonemap_device", "lum_render_ldr",
+                 "lum_tonemap_device", "lum_render_ldr", "lum_scene_set_envmap", "lum_render_aov",
                  "lum_batch_default_config",
                  "lum_batch_autotune", "lum_batch_create", "lum_batch_config_of", "lum_batch_render",
                  "lum_batch_render_device", "lum_batch_destroy"):
@@ -109,6 +112,8 @@ class GpuScene:
         h = C.c_void_p()
         check(lib().lum_scene_create(self.desc.ref(), C.byref(h)))
         self.h = h
+        if getattr(world, "env_map", None) is not None:
+            self.set_envmap(world.env_map)
 
     def close(self):
         if getattr(self, "h", None):
@@ -140,6 +145,25 @@ class GpuScene:
         st = abi.LumStats()
         check(lib().lum_render_device(self.h, C.byref(p), C.c_void_p(d_out), C.c_void_p(stream), C.byref(st)))
         return st
+
+    def set_envmap(self, rgb: Optional[np.ndarray]):
+        """lum_scene_set_envmap: an (H, W, 3) float32 equirectangular map (None removes it)."""
+        if rgb is None:
+            check(lib().lum_scene_set_envmap(self.h, None, 0, 0))
+            return
+        rgb = np.ascontiguousarray(rgb, dtype=np.float32)
+        assert rgb.ndim == 3 and rgb.shape[2] == 3
+        check(lib().lum_scene_set_envmap(self.h, rgb.ctypes.data, rgb.shape[1], rgb.shape[0]))
+
+    def render_aov(self, cfg: RenderConfig):
+        """lum_render_aov: (depth (H, W) float32, normals (H, W, 3) uint8, albedo (H, W, 3) uint8)."""
+        h, w, _ = cfg.out_shape()
+        p = cfg.to_c()
+        depth = np.empty((h, w), dtype=np.float32)
+        normals = np.empty((h, w, 3), dtype=np.uint8)
+        albedo = np.empty((h, w, 3), dtype=np.uint8)
+        check(lib().lum_render_aov(self.h, C.byref(p), depth.ctypes.data, normals.ctypes.data, albedo.ctypes.data))
+        return depth, normals, albedo
 
     def render_ldr(self, cfg: RenderConfig, tm: Optional["ToneMapConfig"] = None):
         """lum_render_ldr: (H, W, 4) uint8 RGBA through the LDR colour chain, and stats.  The

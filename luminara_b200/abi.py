@@ -9,7 +9,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-LUM_ABI_VERSION = 2
+LUM_ABI_VERSION = 3
 
 # status codes
 LUM_OK = 0
@@ -48,6 +48,15 @@ MAT_DIELECTRIC = 3
 MAT_EMISSIVE = 4
 MAT_MICROFACET = 5
 MAT_ISOTROPIC = 6
+MAT_BLEND = 7
+MAT_TRANSPARENT = 8
+MAT_IRIDESCENT = 9
+MAT_TOON = 10
+MAT_ANISOTROPIC = 11
+MAT_CLEARCOAT = 12
+MAT_VELVET = 13
+MAT_TRANSLUCENT = 14
+MAT_SUBSURFACE = 15
 
 TEX_SOLID = 0
 TEX_CHECKER = 1
@@ -60,6 +69,8 @@ BG_SKY = 0
 BG_SOLID = 1
 BG_GRADIENT = 2
 BG_SUN = 3
+BG_STARFIELD = 4
+BG_ENVMAP = 5
 
 FILTER_BOX = 0
 FILTER_TRIANGLE = 1
@@ -123,6 +134,8 @@ class LumMaterial(C.Structure):
         ("intensity", C.c_double),
         ("dispersion", C.c_double),
         ("tint", D3),
+        ("sub", C.c_int32 * 2),
+        ("extra", C.c_double * 4),
     ]
 
 
@@ -191,6 +204,8 @@ class LumRenderParams(C.Structure):
         ("adaptive", C.c_int32),
         ("adaptive_threshold", C.c_double),
         ("time_limit", C.c_double),
+        ("bg_star_density", C.c_double),
+        ("bg_star_brightness", C.c_double),
     ]
 
 

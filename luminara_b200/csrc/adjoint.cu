@@ -648,7 +648,7 @@ __global__ void __launch_bounds__(128, LUM_ADJ_MIN_BLOCKS) k_replay(SceneDev S, 
                     verts[(size_t)(K - 1) * n_slots + slot].flags = vflags;
                     state = P.bounce >= R.max_depth ? A_DONE : A_CLOSEST;
                 } else if (!found) {
-                    bg = background(R, P.ray);                     // render.rs:1535
+                    bg = background(S, R, P.ray);                     // render.rs:1535
                     P.L = P.L + mul(P.beta, bg);
                     state = A_DONE;
                 } else {
@@ -763,6 +763,9 @@ lum_status lum_backward(lum_scene* scene, const lum_render_params* params, const
     if (st != LUM_OK) return st;
     if (R.max_depth > (uint32_t)adj::kMaxVerts)
         return set_error(LUM_ERR_UNSUPPORTED, "lum_backward supports max_depth <= 16");
+    if (scene_max_material_kind(scene) > LUM_MAT_ISOTROPIC)
+        return set_error(LUM_ERR_UNSUPPORTED, "lum_backward differentiates Lambertian, Metal, Dielectric, Emissive, "
+                                              "Microfacet and Isotropic materials only");
     const int n_mat = dev.n_mats;
     if (light_material)
         for (int k = 0; k < dev.n_lights; ++k)

@@ -26,6 +26,7 @@ enum PrimType : int32_t {
 };
 
 constexpr int kStackDepth = 64;     // traversal stack entries per thread
+constexpr int kMaxBlendDepth = 4;   // nesting levels of Blend materials (checked by lum_scene_create)
 constexpr int kMaxBvhDepth = 62;    // the builder keeps every leaf at most this deep
 constexpr int kMedianDepth = 40;    // below this depth the builder splits at the object median
 
@@ -44,6 +45,10 @@ struct alignas(16) MatDev {
     float dispersion;
     int32_t tint_white;
     int32_t specular;
+    float extra[4];      // per-kind parameters of the other materials (lum_material.extra)
+    int32_t sub[2];      // Blend: the blended materials
+    int32_t emits;       // Blend: some leaf below it is emissive
+    int32_t pad;
 };
 
 struct alignas(16) LightDev {
@@ -96,6 +101,8 @@ struct SceneDev {
     int32_t n_planes;
     int32_t n_mats;
     int32_t pad;
+    const float* env;        // environment map, env_w * env_h RGB floats (or null)
+    uint32_t env_w, env_h;
     CameraDev cam;
 };
 
@@ -129,6 +136,7 @@ struct RenderDev {
     float bg_intensity;
     float exposure;
     uint32_t tiles_x, n_tasks;
+    float star_density, star_brightness;   // STARFIELD background
 };
 
 }  // namespace lum

@@ -14,6 +14,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -416,7 +417,72 @@ lum::MatDev make_mat(const lum_material& m) {
         double r = std::min(std::max(m.roughness, 0.01), 1.0), mt = std::min(std::max(m.metallic, 0.0), 1.0);
         o.specular = mt > 0.9 && r < 0.1;
     }
+    // the other materials: their constructors' clamps (material.rs:396-865)
+    auto clamp = [](double x, double lo, double hi) { return std::min(std::max(x, lo), hi); };
+    const double* e = m.extra;
+    switch (m.kind) {
+        case LUM_MAT_BLEND:                                                     // :402-406
+            o.extra[0] = (float)clamp(e[0], 0.0, 1.0);
+            o.sub[0] = m.sub[0];
+            o.sub[1] = m.sub[1];
+            break;
+        case LUM_MAT_TRANSPARENT: o.specular = 1; break;                        // :437-439
+        case LUM_MAT_IRIDESCENT:                                                // :459-466
+            o.extra[0] = (float)std::max(e[0], 100.0);
+            o.ior = (float)std::max(m.ior, 1.0);
+            o.roughness = (float)clamp(m.roughness, 0.0, 1.0);
+            o.specular = 1;
+            break;
+        case LUM_MAT_TOON:                                                      // :538-545 (bands: u32)
+            o.extra[0] = (float)std::max(std::floor(clamp(e[0], 0.0, 4294967295.0)), 2.0);
+            o.extra[1] = (float)std::max(e[1], 0.0);
+            break;
+        case LUM_MAT_ANISOTROPIC:                                               // :592-599 (axis: usize)
+            o.extra[0] = (float)clamp(e[0], 0.001, 1.0);
+            o.extra[1] = (float)clamp(e[1], 0.001, 1.0);
+            o.extra[2] = (float)std::min(std::floor(std::max(e[2], 0.0)), 2.0);
+            o.specular = 1;
+            break;
+        case LUM_MAT_CLEARCOAT:                                                 // :655-661
+            o.extra[0] = (float)clamp(e[0], 0.0, 1.0);
+            o.ior = (float)std::max(m.ior, 1.0);
+            break;
+        case LUM_MAT_VELVET: o.extra[0] = (float)clamp(e[0], 0.0, 2.0); break;  // :718-720
+        case LUM_MAT_TRANSLUCENT:                                               // :760-766
+            o.extra[0] = (float)clamp(e[0], 0.0, 1.0);
+            o.extra[1] = (float)clamp(e[1], 0.0, 1.0);
+            break;
+        case LUM_MAT_SUBSURFACE: o.extra[0] = (float)std::max(e[0], 0.001); break;   // :812-818
+        default: break;
+    }
     return o;
+}
+
+// Blend trees: children in range, nesting at most kMaxBlendDepth levels (which also rules out
+// cycles); `emits` marks Blends with an emissive leaf.
+lum_status check_blends(const lum_scene_desc& d, std::vector<lum::MatDev>& mats) {
+    const int n = (int)d.n_materials;
+    std::function<int(int, int)> depth = [&](int i, int level) -> int {
+        const lum_material& m = d.materials[i];
+        if (m.kind != LUM_MAT_BLEND) return m.kind == LUM_MAT_EMISSIVE ? 1 : 0;
+        if (level > lum::kMaxBlendDepth) return -1;
+        int r = 0;
+        for (int k = 0; k < 2; ++k) {
+            if (m.sub[k] < 0 || m.sub[k] >= n) return -2;
+            int c = depth(m.sub[k], level + 1);
+            if (c < 0) return c;
+            r |= c;
+        }
+        return r;
+    };
+    for (int i = 0; i < n; ++i) {
+        if (d.materials[i].kind != LUM_MAT_BLEND) continue;
+        int r = depth(i, 1);
+        if (r == -2) return fail(LUM_ERR_INVALID_ARGUMENT, "material %d: blend child index out of range", i);
+        if (r < 0) return fail(LUM_ERR_UNSUPPORTED, "material %d: blends nest more than %d deep", i, lum::kMaxBlendDepth);
+        mats[i].emits = r;
+    }
+    return LUM_OK;
 }
 
 lum::CameraDev make_camera(const lum_camera& c) {                      // camera.rs:48-76
@@ -463,8 +529,12 @@ struct lum_scene {
     size_t d_tone_cap = 0;
     void* d_part = nullptr;     // fixed-point pixel accumulators of grouped (small) frames
     size_t d_part_cap = 0;
+    void* d_env = nullptr;      // environment map (LUM_BG_ENVMAP)
+    void* d_aov = nullptr;      // AOV outputs of lum_render_aov
+    size_t d_aov_cap = 0;
     lum::SceneDev dev{};
     uint32_t n_prims = 0, n_nodes = 0, n_lights = 0, bvh_depth = 0;
+    int max_mat_kind = 0;
     std::mutex mu;
 };
 
@@ -510,6 +580,10 @@ lum_status make_render_dev(const lum_scene* s, const lum_render_params& p, lum::
     }
     R.bg_intensity = (float)p.bg_intensity;
     R.exposure = (float)p.exposure;
+    R.star_density = (float)p.bg_star_density;
+    R.star_brightness = (float)p.bg_star_brightness;
+    if (p.background == LUM_BG_ENVMAP && !s->dev.env)
+        return fail(LUM_ERR_INVALID_ARGUMENT, "LUM_BG_ENVMAP without an environment map (lum_scene_set_envmap)");
     R.tiles_x = (R.w + 7) / 8;
     uint64_t tasks = (uint64_t)R.tiles_x * ((R.h + 3) / 4);
     if (tasks > 0x7FFFFFFFull) return fail(LUM_ERR_TOO_LARGE, "image too large");
@@ -539,7 +613,7 @@ lum_status check_params(const lum_render_params* p) {
             return fail(LUM_ERR_UNSUPPORTED, "adaptive sampling and the time limit need all strata "
                                              "(sample_begin 0, sample_count 0)");
     }
-    if (p->background < LUM_BG_SKY || p->background > LUM_BG_SUN)
+    if (p->background < LUM_BG_SKY || p->background > LUM_BG_ENVMAP)
         return fail(LUM_ERR_INVALID_ARGUMENT, "unknown background %d", p->background);
     if (p->pixel_filter < LUM_FILTER_BOX || p->pixel_filter > LUM_FILTER_MITCHELL)
         return fail(LUM_ERR_INVALID_ARGUMENT, "unknown pixel filter %d", p->pixel_filter);
@@ -606,7 +680,7 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
     if (desc->camera.panorama) return fail(LUM_ERR_UNSUPPORTED, "panorama camera is not on the GPU path");
     for (uint32_t i = 0; i < desc->n_materials; ++i) {
         int k = desc->materials[i].kind;
-        if (k < LUM_MAT_LAMBERTIAN || k > LUM_MAT_ISOTROPIC)
+        if (k < LUM_MAT_LAMBERTIAN || k > LUM_MAT_SUBSURFACE)
             return fail(LUM_ERR_INVALID_ARGUMENT, "material %u: unknown kind %d", i, k);
         int t = desc->materials[i].texture;
         if (t != LUM_TEX_SOLID && t != LUM_TEX_CHECKER)
@@ -640,6 +714,8 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
     }
     std::vector<lum::MatDev> mats(desc->n_materials);
     for (uint32_t i = 0; i < desc->n_materials; ++i) mats[i] = make_mat(desc->materials[i]);
+    st = check_blends(*desc, mats);
+    if (st != LUM_OK) return st;
     std::vector<lum::LightDev> lights(desc->n_lights);
     for (uint32_t i = 0; i < desc->n_lights; ++i) {
         const lum_light& l = desc->lights[i];
@@ -717,6 +793,7 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
     s->n_nodes = (uint32_t)bvh.nodes.size();
     s->n_lights = (uint32_t)lights.size();
     s->bvh_depth = bvh.max_depth;
+    for (uint32_t i = 0; i < desc->n_materials; ++i) s->max_mat_kind = std::max(s->max_mat_kind, desc->materials[i].kind);
     *out = s;
     return LUM_OK;
 }
@@ -732,6 +809,8 @@ lum_status lum_scene_destroy(lum_scene* s) {
     if (s->d_ldr) cudaFree(s->d_ldr);
     if (s->d_tone) cudaFree(s->d_tone);
     if (s->d_part) cudaFree(s->d_part);
+    if (s->d_env) cudaFree(s->d_env);
+    if (s->d_aov) cudaFree(s->d_aov);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -758,6 +837,57 @@ lum_status lum_render_device(lum_scene* s, const lum_render_params* params, floa
     CU(cudaSetDevice(s->device), "cudaSetDevice");
     cudaStream_t cs = stream ? (cudaStream_t)stream : s->stream;
     return run_render(s, params, d_out, cs, stats);
+}
+
+lum_status lum_scene_set_envmap(lum_scene* s, const float* rgb, uint32_t width, uint32_t height) {
+    if (!s) return fail(LUM_ERR_INVALID_ARGUMENT, "scene is null");
+    if (rgb && (width == 0 || height == 0)) return fail(LUM_ERR_INVALID_ARGUMENT, "empty environment map");
+    if (rgb && (uint64_t)width * height > (1ull << 31)) return fail(LUM_ERR_TOO_LARGE, "environment map too large");
+    std::lock_guard<std::mutex> lk(s->mu);
+    CU(cudaSetDevice(s->device), "cudaSetDevice");
+    CU(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
+    if (s->d_env) cudaFree(s->d_env);
+    s->d_env = nullptr;
+    s->dev.env = nullptr;
+    s->dev.env_w = s->dev.env_h = 0;
+    if (!rgb) return LUM_OK;
+    const size_t bytes = sizeof(float) * 3 * (size_t)width * height;
+    CU(cudaMalloc(&s->d_env, bytes), "cudaMalloc");
+    CU(cudaMemcpy(s->d_env, rgb, bytes, cudaMemcpyHostToDevice), "cudaMemcpy H2D");
+    s->dev.env = (const float*)s->d_env;
+    s->dev.env_w = width;
+    s->dev.env_h = height;
+    return LUM_OK;
+}
+
+lum_status lum_render_aov(lum_scene* s, const lum_render_params* params, float* depth, uint8_t* normals,
+                          uint8_t* albedo) {
+    if (!s) return fail(LUM_ERR_INVALID_ARGUMENT, "null argument");
+    lum_status st = check_params(params);
+    if (st != LUM_OK) return st;
+    std::lock_guard<std::mutex> lk(s->mu);
+    CU(cudaSetDevice(s->device), "cudaSetDevice");
+    lum::RenderDev R;
+    st = make_render_dev(s, *params, R);
+    if (st != LUM_OK) return st;
+    const size_t px = (size_t)R.w * R.h;
+    if (px == 0 || (!depth && !normals && !albedo)) return LUM_OK;
+    st = ensure(&s->d_aov, &s->d_aov_cap, 10 * px);
+    if (st != LUM_OK) return st;
+    float* d_depth = (float*)s->d_aov;
+    uint8_t* d_norm = (uint8_t*)s->d_aov + 4 * px;
+    uint8_t* d_alb = d_norm + 3 * px;
+    CU(cudaMemsetAsync(s->d_work, 0, sizeof(lum::WorkCounters), s->stream), "cudaMemsetAsync");
+    CU(lum::launch_aov(s->dev, R, depth ? d_depth : nullptr, normals ? d_norm : nullptr, albedo ? d_alb : nullptr,
+                       s->d_work, s->stream), "aov launch");
+    if (depth) CU(cudaMemcpyAsync(depth, d_depth, 4 * px, cudaMemcpyDeviceToHost, s->stream), "D2H");
+    if (normals) CU(cudaMemcpyAsync(normals, d_norm, 3 * px, cudaMemcpyDeviceToHost, s->stream), "D2H");
+    if (albedo) CU(cudaMemcpyAsync(albedo, d_alb, 3 * px, cudaMemcpyDeviceToHost, s->stream), "D2H");
+    lum::WorkCounters wc{};
+    CU(cudaMemcpyAsync(&wc, s->d_work, sizeof wc, cudaMemcpyDeviceToHost, s->stream), "D2H");
+    CU(cudaStreamSynchronize(s->stream), "aov");
+    if (wc.error_flags) return fail(LUM_ERR_KERNEL, "AOV kernel reported error flags 0x%x", wc.error_flags);
+    return LUM_OK;
 }
 
 lum_status lum_render(lum_scene* s, const lum_render_params* params, float* out_rgb, lum_stats* stats) {
@@ -918,6 +1048,8 @@ lum_status prepare_render(lum_scene* s, const lum_render_params* params, SceneDe
     stream = s->stream;
     return LUM_OK;
 }
+
+int scene_max_material_kind(const lum_scene* s) { return s ? s->max_mat_kind : 0; }
 
 lum_status scene_view(lum_scene* s, const lum_render_params* params, SceneDev& dev, RenderDev& R, int& device) {
     if (!s) return fail(LUM_ERR_INVALID_ARGUMENT, "scene is null");

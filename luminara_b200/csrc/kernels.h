@@ -38,6 +38,10 @@ struct SamplingDev {
 // strata).  wc must be zeroed; wc->samples receives the samples kept.
 cudaError_t launch_render_sampled(const SceneDev& S, const RenderDev& R, const SamplingDev& A, float* out,
                                   WorkCounters* wc, cudaStream_t stream);
+// AOV passes into device buffers (any may be null): depth W*H floats, normals and albedo
+// W*H*3 bytes.
+cudaError_t launch_aov(const SceneDev& S, const RenderDev& R, float* depth, uint8_t* normals, uint8_t* albedo,
+                       WorkCounters* wc, cudaStream_t stream);
 cudaError_t launch_intersect(const SceneDev& S, const lum_ray* rays, uint32_t n, lum_hit* hits, WorkCounters* wc,
                              cudaStream_t stream);
 cudaError_t launch_occluded(const SceneDev& S, const lum_ray* rays, uint32_t n, int32_t* occ, WorkCounters* wc,

@@ -19,5 +19,7 @@ lum_status prepare_render(lum_scene* s, const lum_render_params* params, SceneDe
 // Device view, owning device ordinal and render description of a scene for `params`
 // (validated), without touching the scene's stream.
 lum_status scene_view(lum_scene* s, const lum_render_params* params, SceneDev& dev, RenderDev& R, int& device);
+// Largest LUM_MAT_* kind among the scene's materials (0 when it has none).
+int scene_max_material_kind(const lum_scene* s);
 
 }  // namespace lum

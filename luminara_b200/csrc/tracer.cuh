@@ -66,7 +66,7 @@ __device__ __forceinline__ float4 draw4(uint32_t k0, uint32_t k1, uint32_t pixel
     uint4 o = philox(make_uint4(pixel, stratum, bounce, call), k0, k1);
     return make_float4(u24(o.x), u24(o.y), u24(o.z), u24(o.w));
 }
-enum : uint32_t { CALL_CAMERA = 0, CALL_CAMERA2 = 1, CALL_SCATTER = 2, CALL_NEE = 3, CALL_EXTRA = 4 };
+enum : uint32_t { CALL_CAMERA = 0, CALL_CAMERA2 = 1, CALL_SCATTER = 2, CALL_NEE = 3, CALL_EXTRA = 4, CALL_BLEND = 5 };
 
 // Direct (rejection-free) samplers; same distributions as src/vec3.rs:96-122.
 __device__ __forceinline__ V unit_vector(float a, float b) {
@@ -479,7 +479,178 @@ __device__ __forceinline__ V ggx_normal(V n, float alpha, float r1, float r2) {
 struct Scatter {
     V dir;
     V att;
+    V org;   // origin of the scattered ray: the hit point (set by the caller), or Subsurface's exit point
 };
+
+enum : int { MAT_BLEND = 7 };
+
+// Blend::scatter's choice (material.rs:408-415): one draw per level, mat_a with probability
+// ratio, down to a material that is not a Blend.
+__device__ __noinline__ inline const MatDev& blend_walk(const SceneDev& S, const MatDev& m0, const RenderDev& R,
+                                                        uint32_t pixel, uint32_t stratum, uint32_t bounce) {
+    const MatDev* m = &m0;
+    const float4 u = draw4(R.key0, R.key1, pixel, stratum, bounce, CALL_BLEND);
+    const float uu[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+    for (int l = 0; l < kMaxBlendDepth; ++l) {
+        if (m->kind != MAT_BLEND) break;
+        m = &S.mats[uu[l] < m->extra[0] ? m->sub[0] : m->sub[1]];
+    }
+    return *m;
+}
+__device__ __forceinline__ const MatDev& blend_leaf(const SceneDev& S, const MatDev& m, const RenderDev& R,
+                                                    uint32_t pixel, uint32_t stratum, uint32_t bounce) {
+    return m.kind == MAT_BLEND ? blend_walk(S, m, R, pixel, stratum, bounce) : m;
+}
+
+// Blend::emitted (material.rs:417-420): ratio * emitted(a) + (1 - ratio) * emitted(b).
+template <int D>
+__device__ __noinline__ V blend_emitted(const SceneDev& S, int idx, V p) {
+    const MatDev& m = S.mats[idx];
+    if (m.kind != MAT_BLEND) return emitted(m, p);
+    if constexpr (D > 0)
+        return blend_emitted<D - 1>(S, m.sub[0], p) * m.extra[0] + blend_emitted<D - 1>(S, m.sub[1], p) * (1.0f - m.extra[0]);
+    return mk(0.f, 0.f, 0.f);
+}
+__device__ __forceinline__ V emitted_at(const SceneDev& S, int idx, const MatDev& m, V p) {
+    if (m.kind == MAT_BLEND) return m.emits ? blend_emitted<kMaxBlendDepth>(S, idx, p) : mk(0.f, 0.f, 0.f);
+    return emitted(m, p);
+}
+
+// Iridescent::thin_film_color (material.rs:469-491): sin^2(phase / 2) at 650 / 532 / 450 nm
+// with phase = 2 pi opd / lambda, i.e. sin^2(pi opd / lambda).
+__device__ __forceinline__ V thin_film(float cos_t, float thickness, float film_ior) {
+    float sin_t = sqrtf(fmaxf(1.0f - cos_t * cos_t, 0.0f));
+    float sf = sin_t / film_ior;
+    float cf = sqrtf(fmaxf(1.0f - sf * sf, 0.0f));
+    float opd = 2.0f * thickness * film_ior * cf;
+    float r = sinpif(opd / 650.0f), g = sinpif(opd / 532.0f), b = sinpif(opd / 450.0f);
+    return mk(r * r, g * g, b * b);
+}
+
+// The other materials' scatter (material.rs:408-865), out of line: the megakernel's register
+// allocation stays that of the common materials.  Keyed draws: CALL_SCATTER slots as noted,
+// Subsurface's exit direction from CALL_EXTRA.
+__device__ __noinline__ inline bool scatter_more(const MatDev& m, const Ray& ray, const Surface& sf, float4 s,
+                                                 const RenderDev& R, uint32_t pixel, uint32_t stratum,
+                                                 uint32_t bounce, Scatter& out) {
+    switch (m.kind) {
+        case 8: {                                                      // Transparent, material.rs:429-435
+            out.dir = ray.d;
+            out.att = mk(1.f, 1.f, 1.f);
+            return true;
+        }
+        case 9: {                                                      // Iridescent, material.rs:499-527
+            V ud = unit(ray.d);
+            float ct = fminf(fabsf(dot(-ud, sf.n)), 1.0f);
+            out.att = mul(mk(m.color), thin_film(ct, m.extra[0], m.ior));
+            V d = reflect(ud, sf.n);
+            if (m.roughness > 0.0f) {
+                d = d + in_unit_sphere(s.x, s.y, s.z) * m.roughness;
+                if (dot(d, sf.n) <= 0.0f) return false;
+            }
+            out.dir = d;
+            return true;
+        }
+        case 10: {                                                     // Toon, material.rs:549-577
+            V d = sf.n + unit_vector(s.x, s.y);
+            if (near_zero(d)) d = sf.n;
+            V du = unit(d);
+            float ndl = fmaxf(dot(du, sf.n), 0.0f);
+            float band = fminf(fmaxf(floorf(ndl * m.extra[0]) / (m.extra[0] - 1.0f), 0.0f), 1.0f);
+            V hv = unit(unit(-ray.d) + du);
+            float spec = powf(fmaxf(dot(hv, sf.n), 0.0f), m.extra[1] * 100.0f);
+            out.dir = d;
+            out.att = mk(m.color) * (band + (spec > 0.5f ? 0.3f : 0.0f));
+            return true;
+        }
+        case 11: {                                                     // Anisotropic, material.rs:607-641
+            V refl = reflect(unit(ray.d), sf.n);
+            const int ax = (int)m.extra[2];
+            V wt = ax == 0 ? mk(1.f, 0.f, 0.f) : (ax == 1 ? mk(0.f, 1.f, 0.f) : mk(0.f, 0.f, 1.f));
+            V t = unit(wt - sf.n * dot(wt, sf.n));
+            V b = cross(sf.n, t);
+            float sp, cp;
+            sincospif(2.0f * s.x, &sp, &cp);
+            float r2 = sqrtf(s.y);
+            V sc = unit(refl + t * (cp * r2 * m.extra[0]) + b * (sp * r2 * m.extra[1]));
+            if (!(dot(sc, sf.n) > 0.0f)) return false;
+            out.dir = sc;
+            out.att = mk(m.color);
+            return true;
+        }
+        case 12: {                                                     // Clearcoat, material.rs:664-707
+            V ud = unit(ray.d);
+            float ct = fminf(fabsf(dot(-ud, sf.n)), 1.0f);
+            float r0 = (1.0f - m.ior) / (1.0f + m.ior);
+            r0 = r0 * r0;
+            float om = 1.0f - ct, om2 = om * om;
+            float fr = r0 + (1.0f - r0) * (om2 * om2 * om);
+            if (s.x < fr * m.extra[0]) {
+                V refl = reflect(ud, sf.n);
+                float rough = (1.0f - m.extra[0]) * 0.3f;
+                V d = refl;
+                if (rough > 0.001f) {
+                    V fz = refl + in_unit_sphere(s.y, s.z, s.w) * rough;
+                    if (dot(fz, sf.n) > 0.0f) d = fz;
+                }
+                out.dir = d;
+                out.att = mk(1.f, 1.f, 1.f);
+                return true;
+            }
+            V d = sf.n + unit_vector(s.y, s.z);
+            if (near_zero(d)) d = sf.n;
+            out.dir = d;
+            out.att = mk(m.color);
+            return true;
+        }
+        case 13: {                                                     // Velvet, material.rs:724-746
+            V d = sf.n + unit_vector(s.x, s.y);
+            if (near_zero(d)) d = sf.n;
+            float ct = fabsf(dot(-unit(ray.d), sf.n));
+            float st = sqrtf(fmaxf(1.0f - ct * ct, 0.0f));
+            out.dir = d;
+            out.att = mk(m.color) * (1.0f + st * sqrtf(st) * m.extra[0]);
+            return true;
+        }
+        case 14: {                                                     // Translucent, material.rs:769-797
+            V d;
+            if (s.x < m.extra[0]) {
+                V below = -sf.n + unit_vector(s.y, s.z);
+                d = unit(ray.d) * (1.0f - m.extra[1]) + below * m.extra[1];
+                if (near_zero(d)) d = -sf.n;
+            } else {
+                d = sf.n + unit_vector(s.y, s.z);
+                if (near_zero(d)) d = sf.n;
+            }
+            out.dir = d;
+            out.att = mk(m.color);
+            return true;
+        }
+        case 15: {                                                     // Subsurface, material.rs:823-864
+            float fr = schlick(fabsf(dot(unit(ray.d), sf.n)), 1.0f / 1.4f);
+            if (s.x < fr) {
+                V d = sf.n + unit_vector(s.y, s.z);
+                if (near_zero(d)) d = sf.n;
+                out.dir = d;
+                out.att = mk(m.color);
+                return true;
+            }
+            const float mfp = m.extra[0];
+            float step = -mfp * logf(fmaxf(s.y, 1e-10f));
+            out.org = sf.p + unit_vector(s.z, s.w) * step;
+            float4 ex = draw4(R.key0, R.key1, pixel, stratum, bounce, CALL_EXTRA);
+            V d = sf.n + unit_vector(ex.x, ex.y);
+            out.dir = near_zero(d) ? sf.n : unit(d);
+            const float k = -step / mfp;
+            out.att = mul(mk(m.color), mk(__expf(k * (1.0f - m.color2[0])), __expf(k * (1.0f - m.color2[1])),
+                                          __expf(k * (1.0f - m.color2[2]))));
+            return true;
+        }
+        default:
+            return false;
+    }
+}
 
 // Material::scatter; draws s = (s0..s3) of CALL_SCATTER, extra for dispersion.
 // KIND >= 0 fixes the material kind at compile time (the material-sorted shading kernels of
@@ -574,6 +745,8 @@ __device__ __forceinline__ bool scatter(const MatDev& m, const Ray& ray, const S
             out.att = mk(m.color);
             return true;
         }
+        case 8: case 9: case 10: case 11: case 12: case 13: case 14: case 15:
+            return scatter_more(m, ray, sf, s, R, pixel, stratum, bounce, out);
         default:                                                       // Emissive: no scatter
             return false;
     }
@@ -664,7 +837,43 @@ __device__ __forceinline__ bool sample_light(const SceneDev& S, V hp, V normal, 
     return true;
 }
 
-__device__ __forceinline__ V background(const RenderDev& R, const Ray& r) {  // render.rs:73-171
+// Background::Starfield (render.rs:86-112): dark blue space plus stars hashed from the
+// direction quantised at 500 * density cells per unit.
+__device__ __noinline__ inline V starfield(const RenderDev& R, V ud, float t) {
+    V space = mk(0.0f, 0.0f, 0.02f) * (1.0f - t) + mk(0.02f, 0.0f, 0.05f) * t;
+    const float scale = 500.0f * R.star_density;
+    const long long ix = (long long)floorf(ud.x * scale), iy = (long long)floorf(ud.y * scale),
+                    iz = (long long)floorf(ud.z * scale);
+    const unsigned long long hash = ((unsigned long long)ix * 73856093ull) ^ ((unsigned long long)iy * 19349663ull) ^
+                                    ((unsigned long long)iz * 83492791ull);
+    const float star = (float)(hash % 10000ull) / 10000.0f;
+    if (!(star > 0.997f)) return space;
+    const float rh = (float)((hash >> 8) % 100ull) / 100.0f;
+    const V c = rh < 0.3f ? mk(1.0f, 0.9f, 0.8f) : (rh < 0.6f ? mk(0.9f, 0.9f, 1.0f) : mk(1.f, 1.f, 1.f));
+    return space + c * (star * R.star_brightness);
+}
+
+// Background::EnvMap (render.rs:113-151): equirectangular lookup, bilinear, times intensity.
+__device__ __noinline__ inline V envmap(const SceneDev& S, const RenderDev& R, V ud) {
+    if (!S.env) return mk(0.f, 0.f, 0.f);
+    const float theta = acosf(-ud.y);
+    const float phi = atan2f(-ud.z, ud.x) + CUDART_PI_F;
+    const float fx = phi * (0.5f / CUDART_PI_F) * (float)S.env_w - 0.5f;
+    const float fy = theta * (1.0f / CUDART_PI_F) * (float)S.env_h - 0.5f;
+    const float flx = floorf(fx), fly = floorf(fy);
+    const int w = (int)S.env_w, h = (int)S.env_h;
+    int x0 = (int)flx % w;
+    if (x0 < 0) x0 += w;
+    const int y0 = (int)fminf(fmaxf(fly, 0.0f), (float)(h - 1));
+    const int x1 = (x0 + 1) % w, y1 = min(y0 + 1, h - 1);
+    const float tx = fx - flx, ty = fy - fly;
+    auto px = [&](int x, int y) { return mk(S.env + 3 * ((size_t)y * w + x)); };
+    const V c = px(x0, y0) * ((1.0f - tx) * (1.0f - ty)) + px(x1, y0) * (tx * (1.0f - ty)) +
+                px(x0, y1) * ((1.0f - tx) * ty) + px(x1, y1) * (tx * ty);
+    return c * R.bg_intensity;
+}
+
+__device__ __forceinline__ V background(const SceneDev& S, const RenderDev& R, const Ray& r) {  // render.rs:73-171
     if (R.background == 1) return mk(R.bg_color);
     V ud = unit(r.d);
     float t = 0.5f * (ud.y + 1.0f);
@@ -679,6 +888,8 @@ __device__ __forceinline__ V background(const RenderDev& R, const Ray& r) {  // 
         }
         return sky;
     }
+    if (R.background == 4) return starfield(R, ud, t);
+    if (R.background == 5) return envmap(S, R, ud);
     return mk(1.f, 1.f, 1.f) * (1.0f - t) + mk(0.5f, 0.7f, 1.0f) * t;
 }
 
@@ -795,7 +1006,7 @@ template <int KIND = -1>
 __device__ __forceinline__ int shade(const SceneDev& S, const RenderDev& R, uint32_t pixel, Path& P, bool found,
                                      const Hit& h, Pending& pend) {
     if (!found) {
-        P.L = P.L + mul(P.beta, background(R, P.ray));
+        P.L = P.L + mul(P.beta, background(S, R, P.ray));
         return ST_DONE;
     }
     const uint32_t depth = R.max_depth - P.bounce;
@@ -807,10 +1018,12 @@ __device__ __forceinline__ int shade(const SceneDev& S, const RenderDev& R, uint
     // (whose slab tests pass every box) out of the traversal.
     if (!isfinite(sf.p.x) || !isfinite(sf.p.y) || !isfinite(sf.p.z)) return ST_DONE;
     const MatDev& m = S.mats[sf.mat];
-    V e = P.skip_emission ? mk(0.f, 0.f, 0.f) : emitted(m, sf.p);
+    V e = P.skip_emission ? mk(0.f, 0.f, 0.f) : (KIND < 0 ? emitted_at(S, sf.mat, m, sf.p) : emitted(m, sf.p));
     float4 su = draw4(R.key0, R.key1, pixel, P.stratum, P.bounce, CALL_SCATTER);
     Scatter sc;
-    if (!scatter<KIND>(m, P.ray, sf, h.t, su, R, pixel, P.stratum, P.bounce, sc)) {
+    sc.org = sf.p;
+    const MatDev& ms = KIND < 0 ? blend_leaf(S, m, R, pixel, P.stratum, P.bounce) : m;
+    if (!scatter<KIND>(ms, P.ray, sf, h.t, su, R, pixel, P.stratum, P.bounce, sc)) {
         P.L = P.L + mul(P.beta, e);
         return ST_DONE;
     }
@@ -844,7 +1057,7 @@ __device__ __forceinline__ int shade(const SceneDev& S, const RenderDev& R, uint
     }
     P.beta = nb;
     P.skip_emission = use_nee;
-    P.ray.o = sf.p;
+    P.ray.o = sc.org;
     P.ray.d = sc.dir;
     ++P.bounce;
     if (shadow) return ST_SHADOW;

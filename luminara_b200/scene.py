@@ -52,8 +52,12 @@ class Material:
     intensity: float = 1.0
     dispersion: float = 0.0
     tint: Vec = (1.0, 1.0, 1.0)
+    color2: Optional[Vec] = None      # Subsurface scatter_color
+    extra: Sequence[float] = (0.0, 0.0, 0.0, 0.0)
+    children: Optional[Sequence["Material"]] = None   # Blend: (mat_a, mat_b)
 
-    def to_c(self) -> abi.LumMaterial:
+    def to_c(self, index_of=None) -> abi.LumMaterial:
+        """index_of(material) -> material index; needed by Blend for its children."""
         m = abi.LumMaterial()
         m.kind = self.kind
         m.texture = abi.TEX_SOLID
@@ -74,6 +78,11 @@ class Material:
         m.intensity = float(self.intensity)
         m.dispersion = float(self.dispersion)
         m.tint[:] = list(map(float, self.tint))
+        if self.color2 is not None:
+            m.color2[:] = list(map(float, self.color2))
+        m.extra[:] = [float(x) for x in tuple(self.extra) + (0.0,) * (4 - len(self.extra))]
+        if self.children is not None:
+            m.sub[:] = [index_of(c) for c in self.children]
         return m
 
 
@@ -101,6 +110,43 @@ def Microfacet(albedo: Vec, roughness: float = 0.5, metallic: float = 0.0, textu
 
 def Isotropic(albedo: Vec) -> Material:
     return Material(abi.MAT_ISOTROPIC, color=albedo)
+
+
+# The other reference materials (material.rs:396-865); clamps are applied by the library.
+def Blend(mat_a: Material, mat_b: Material, ratio: float) -> Material:
+    return Material(abi.MAT_BLEND, extra=(ratio,), children=(mat_a, mat_b))
+
+
+def Transparent() -> Material:
+    return Material(abi.MAT_TRANSPARENT)
+
+
+def Iridescent(base_color: Vec, thickness: float, film_ior: float, roughness: float) -> Material:
+    return Material(abi.MAT_IRIDESCENT, color=base_color, extra=(thickness,), ior=film_ior, roughness=roughness)
+
+
+def Toon(color: Vec, bands: int, specular: float) -> Material:
+    return Material(abi.MAT_TOON, color=color, extra=(bands, specular))
+
+
+def Anisotropic(color: Vec, roughness_u: float, roughness_v: float, tangent_axis: int) -> Material:
+    return Material(abi.MAT_ANISOTROPIC, color=color, extra=(roughness_u, roughness_v, tangent_axis))
+
+
+def Clearcoat(base_color: Vec, coat_gloss: float, coat_ior: float) -> Material:
+    return Material(abi.MAT_CLEARCOAT, color=base_color, extra=(coat_gloss,), ior=coat_ior)
+
+
+def Velvet(color: Vec, sheen: float) -> Material:
+    return Material(abi.MAT_VELVET, color=color, extra=(sheen,))
+
+
+def Translucent(color: Vec, translucency: float, scatter_width: float) -> Material:
+    return Material(abi.MAT_TRANSLUCENT, color=color, extra=(translucency, scatter_width))
+
+
+def Subsurface(color: Vec, mean_free_path: float, scatter_color: Vec) -> Material:
+    return Material(abi.MAT_SUBSURFACE, color=color, extra=(mean_free_path,), color2=scatter_color)
 
 
 # --------------------------------------------------------------------------------------
@@ -282,6 +328,8 @@ class RenderConfig:
     adaptive: bool = False
     adaptive_threshold: float = 0.03
     time_limit: float = 0.0
+    bg_star_density: float = 0.0      # BG_STARFIELD
+    bg_star_brightness: float = 0.0
 
     def to_c(self) -> abi.LumRenderParams:
         p = abi.LumRenderParams()
@@ -305,6 +353,8 @@ class RenderConfig:
         p.adaptive = 1 if self.adaptive else 0
         p.adaptive_threshold = float(self.adaptive_threshold)
         p.time_limit = float(self.time_limit)
+        p.bg_star_density = float(self.bg_star_density)
+        p.bg_star_brightness = float(self.bg_star_brightness)
         return p
 
     def out_shape(self):
@@ -361,7 +411,8 @@ OBJECT_DTYPE = np.dtype([("kind", "<i4"), ("material", "<i4"), ("transform", "<i
                          ("p", "<f8", 12)])
 MATERIAL_DTYPE = np.dtype([("kind", "<i4"), ("texture", "<i4"), ("color", "<f8", 3), ("color2", "<f8", 3),
                            ("tex_scale", "<f8"), ("fuzz", "<f8"), ("ior", "<f8"), ("roughness", "<f8"),
-                           ("metallic", "<f8"), ("intensity", "<f8"), ("dispersion", "<f8"), ("tint", "<f8", 3)])
+                           ("metallic", "<f8"), ("intensity", "<f8"), ("dispersion", "<f8"), ("tint", "<f8", 3),
+                           ("sub", "<i4", 2), ("extra", "<f8", 4)])
 
 
 def material_array(n: int) -> np.ndarray:
@@ -388,6 +439,7 @@ class World:
         self._mat_index = {}
         self._bulk = []          # (insert position in objects, object array, material array)
         self.light_materials: List[Optional[Material]] = []
+        self.env_map: Optional[np.ndarray] = None      # (H, W, 3) float32 map of BG_ENVMAP
         self.camera = CameraConfig()
 
     def add_bulk(self, objects: np.ndarray, materials: np.ndarray) -> int:
@@ -402,6 +454,8 @@ class World:
             return -1
         key = id(m)
         if key not in self._mat_index:
+            for c in (m.children or ()):          # Blend children get indices too
+                self.material_index(c)
             self._mat_index[key] = len(self.materials)
             self.materials.append(m)
         return self._mat_index[key]
@@ -515,7 +569,7 @@ class SceneDesc:
             lm.material = world.material_index(m.material)
             meshes.append(lm)
         self._meshes = (abi.LumMesh * max(len(meshes), 1))(*meshes)
-        mats = [m.to_c() for m in world.materials]
+        mats = [m.to_c(world.material_index) for m in world.materials]
         if self._bulk_mats is not None:
             reg = np.zeros(len(mats), dtype=MATERIAL_DTYPE)
             if mats:

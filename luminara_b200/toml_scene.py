@@ -88,6 +88,7 @@ class _Loader:
     def __init__(self, base_dir: str):
         self.base_dir = base_dir
         self.unsupported: List[str] = []
+        self.env_map: Optional[np.ndarray] = None
 
     def bad(self, what: str):
         if what not in self.unsupported:
@@ -127,6 +128,35 @@ class _Loader:
             return S.Dielectric(1.5)
         if t in ("Blackbody", "blackbody"):
             return S.Emissive(blackbody_to_rgb(float(desc["temperature"])), float(desc.get("intensity", 1.0)))
+        # the other materials, with build_material's defaults (src/scene.rs:1823-1832, 1991-2047)
+        if t in ("Toon", "toon", "cel"):
+            return S.Toon(_v3(c), int(desc.get("bands", 3)), float(desc.get("specular", 0.5)))
+        if t in ("Anisotropic", "anisotropic", "brushed"):
+            return S.Anisotropic(_v3(c), float(desc.get("roughness_u", 0.1)), float(desc.get("roughness_v", 0.5)),
+                                 int(desc.get("tangent_axis", 1)))
+        if t in ("Clearcoat", "clearcoat"):
+            return S.Clearcoat(_v3(c), float(desc.get("coat_gloss", 0.8)), float(desc.get("coat_ior", 1.5)))
+        if t in ("Velvet", "velvet"):
+            return S.Velvet(_v3(c), float(desc.get("sheen", 1.0)))
+        if t in ("Iridescent", "iridescent"):
+            return S.Iridescent(_v3(c if c is not None else (0.9, 0.9, 0.9)), float(desc.get("thickness", 400.0)),
+                                float(desc.get("film_ior", 1.4)), float(desc.get("roughness", 0.05)))
+        if t in ("Translucent", "translucent"):
+            return S.Translucent(_v3(c), float(desc.get("translucency", 0.5)), float(desc.get("scatter_width", 0.8)))
+        if t in ("Subsurface", "subsurface", "sss"):
+            return S.Subsurface(_v3(c), float(desc.get("mean_free_path", 0.5)),
+                                _v3(desc.get("scatter_color", (0.8, 0.5, 0.5))))
+        if t in ("BlendMat", "blend"):
+            a = self.material(desc["material_a"], where + ".material_a")
+            b = self.material(desc["material_b"], where + ".material_b")
+            if a is None or b is None:
+                return None
+            return S.Blend(a, b, float(desc.get("ratio", 0.5)))
+        if t in ("Opacity", "opacity", "alpha"):
+            inner = self.material(desc["material"], where + ".material")
+            if inner is None:
+                return None
+            return S.Blend(inner, S.Transparent(), min(max(float(desc["opacity"]), 0.0), 1.0))
         self.bad(f"{where}: material type '{t}'")
         return None
 
@@ -204,6 +234,7 @@ class _Loader:
             self.background(r["background"], cfg)
 
         world = S.World()
+        world.env_map = self.env_map
         cam = S.CameraConfig(aspect_ratio=cfg.width / cfg.height)
         c = doc.get("camera", {})
         if "look_from" in c:
@@ -341,8 +372,79 @@ class _Loader:
             cfg.bg_color = _v3(bg.get("sun_color", (1.0, 0.95, 0.85)))
             cfg.bg_intensity = float(bg.get("intensity", 20.0))
             cfg.bg_color2 = _v3(bg.get("sky_color", (0.5, 0.7, 1.0)))
+        elif t in ("Starfield", "starfield"):                                   # src/scene.rs:1133-1138
+            cfg.background = abi.BG_STARFIELD
+            cfg.bg_star_density = float(bg.get("star_density", 1.0))
+            cfg.bg_star_brightness = float(bg.get("star_brightness", 5.0))
+        elif t in ("EnvMap", "env_map"):                                        # src/scene.rs:1139-1141
+            path = bg["file"]
+            if not os.path.isabs(path):
+                path = os.path.join(self.base_dir, path)
+            cfg.background = abi.BG_ENVMAP
+            cfg.bg_intensity = float(bg.get("intensity", 1.0))
+            self.env_map = load_env_map(path)
         else:
             self.bad(f"render.background type '{t}'")
+
+
+def _read_radiance_hdr(path: str) -> np.ndarray:
+    """Radiance RGBE (.hdr / .pic): header, resolution line, flat or run-length-encoded scanlines;
+    each pixel (r, g, b, e) is (r, g, b) * 2^(e - 136), e = 0 black."""
+    with open(path, "rb") as f:
+        data = f.read()
+    pos = 0
+    while True:                                                 # header lines up to a blank line
+        end = data.index(b"\n", pos)
+        line = data[pos:end].strip()
+        pos = end + 1
+        if not line:
+            break
+    end = data.index(b"\n", pos)
+    res = data[pos:end].split()
+    pos = end + 1
+    if len(res) != 4 or res[0] not in (b"-Y", b"+Y") or res[2] != b"+X":
+        raise ValueError(f"{path}: unsupported Radiance orientation {res}")
+    h, w = int(res[1]), int(res[3])
+    buf = np.frombuffer(data, dtype=np.uint8)
+    out = np.zeros((h, w, 4), dtype=np.uint8)
+    for y in range(h):
+        if 8 <= w < 32768 and buf[pos] == 2 and buf[pos + 1] == 2 and (int(buf[pos + 2]) << 8 | int(buf[pos + 3])) == w:
+            pos += 4
+            for c in range(4):                                  # new-style RLE, one channel at a time
+                x = 0
+                while x < w:
+                    n = int(buf[pos])
+                    pos += 1
+                    if n > 128:
+                        out[y, x:x + n - 128, c] = buf[pos]
+                        pos += 1
+                        x += n - 128
+                    else:
+                        out[y, x:x + n, c] = buf[pos:pos + n]
+                        pos += n
+                        x += n
+        else:
+            out[y] = buf[pos:pos + 4 * w].reshape(w, 4)
+            pos += 4 * w
+    if res[0] == b"+Y":
+        out = out[::-1]
+    e = out[..., 3].astype(np.int32)
+    scale = np.where(e > 0, np.ldexp(1.0, e - 136), 0.0)
+    return (out[..., :3].astype(np.float64) * scale[..., None]).astype(np.float32)
+
+
+def load_env_map(path: str) -> np.ndarray:
+    """Background::load_env_map (src/render.rs:3589-3602): the image as linear float RGB, top
+    row first -- Radiance .hdr as stored, 8/16-bit images divided by 255 / 65535 (no sRGB
+    decoding, as image's to_rgb32f)."""
+    if path.lower().endswith((".hdr", ".pic")):
+        return _read_radiance_hdr(path)
+    from PIL import Image
+    with Image.open(path) as im:
+        if im.mode in ("I;16", "I;16B", "I;16L", "I"):
+            return np.repeat((np.asarray(im, dtype=np.float64) / 65535.0)[..., None], 3, axis=2).astype(np.float32)
+        a = np.asarray(im.convert("RGB"), dtype=np.float32) / 255.0
+    return np.ascontiguousarray(a)
 
 
 def _load_obj(text: str, scale: float, offset: np.ndarray):

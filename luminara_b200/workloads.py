@@ -276,9 +276,48 @@ def batched(n_scenes=64, seed=3, res_choices=(128, 256, 512, 1024), spp_choices=
     return out
 
 
+def material_zoo(width=160, height=120, spp=16, max_depth=8, seed=31337, background=abi.BG_SOLID):
+    """A lit room with one sphere per remaining material (material.rs:396-865), Blends included
+    (one with an emissive leaf, one nested two deep)."""
+    w = S.World()
+    white = S.Lambertian((0.73, 0.73, 0.73))
+    red = S.Lambertian((0.65, 0.05, 0.05))
+    light = S.Emissive((1.0, 1.0, 1.0), 12.0)
+    w.add(S.XzRect(-6, 6, -6, 6, 0, white))                      # floor
+    w.add(S.XyRect(-6, 6, 0, 8, -4, S.Lambertian((0.4, 0.5, 0.7))))   # back wall
+    w.add(S.YzRect(0, 8, -6, 6, -6, red))
+    w.add(S.XzRect(-1.5, 1.5, -1.5, 1.5, 7.9, light))
+    w.add_light(S.LightInfo.Rect((-1.5, 7.9, -1.5), (3, 0, 0), (0, 0, 3), (0, -1, 0), (12.0, 12.0, 12.0)))
+    glow = S.Emissive((1.0, 0.6, 0.2), 4.0)
+    mats = [
+        S.Blend(red, S.Metal((0.8, 0.8, 0.9), 0.1), 0.4),
+        S.Blend(glow, S.Lambertian((0.2, 0.6, 0.3)), 0.3),
+        S.Blend(S.Blend(S.Velvet((0.5, 0.1, 0.4), 1.0), S.Toon((0.9, 0.7, 0.1), 4, 0.5), 0.5), white, 0.7),
+        S.Transparent(),
+        S.Iridescent((0.9, 0.9, 0.9), 380.0, 1.33, 0.0),
+        S.Iridescent((0.8, 0.9, 1.0), 520.0, 1.5, 0.2),
+        S.Toon((0.2, 0.5, 0.9), 3, 0.0),
+        S.Anisotropic((0.9, 0.8, 0.6), 0.4, 0.05, 0),
+        S.Clearcoat((0.7, 0.1, 0.1), 0.8, 1.5),
+        S.Velvet((0.3, 0.1, 0.5), 1.2),
+        S.Translucent((0.3, 0.8, 0.3), 0.6, 0.5),
+        S.Subsurface((0.9, 0.7, 0.6), 0.3, (0.9, 0.3, 0.3)),
+    ]
+    for k, m in enumerate(mats):
+        x = -4.5 + 3.0 * (k % 4)
+        z = -2.0 + 2.2 * (k // 4)
+        w.add(S.Sphere((x, 0.9, z), 0.9, m))
+    w.camera = S.CameraConfig(look_from=(0, 4.5, 9.5), look_at=(0, 1.2, 0), vfov_degrees=50.0,
+                              aspect_ratio=width / height, aperture=0.0, focus_dist=1.0)
+    cfg = S.RenderConfig(width=width, height=height, samples_per_pixel=spp, max_depth=max_depth, seed=seed,
+                         background=background, bg_color=(0.05, 0.05, 0.08))
+    return w, cfg
+
+
 CONFIGS = {
     "box_room": box_room,
     "random_spheres": random_spheres,
     "dense_mesh": dense_mesh,
     "diff_quads": diff_quads,
+    "material_zoo": material_zoo,
 }

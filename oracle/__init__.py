@@ -61,12 +61,21 @@ def lib():
         L.orc_tie_count.argtypes = [vp, vp, C.c_uint32, C.c_double, C.c_double, vp]
         L.orc_render.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.c_int, C.c_int, dp, C.POINTER(OrcStats)]
         L.orc_render_expired.argtypes = L.orc_render.argtypes
+        L.orc_scene_set_envmap.argtypes = [vp, vp, C.c_uint32, C.c_uint32]
+        L.orc_render_aov.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.c_int, vp, vp, vp]
         L.orc_render_rows.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.c_int, C.c_int, C.c_uint32,
                                       C.c_uint32, dp, C.POINTER(OrcStats)]
         L.orc_adjoint.argtypes = [vp, C.POINTER(abi.LumRenderParams), dp, vp, C.c_int, C.c_int, dp, dp, dp, dp]
         L.orc_adjoint_dir.argtypes = [vp, C.POINTER(abi.LumRenderParams), dp, vp, C.c_int, C.c_int, dp, dp]
         L.orc_scatter.argtypes = [C.POINTER(abi.LumMaterial), dp, dp, dp, C.c_double, C.c_double, C.c_double,
                                   C.c_uint64, C.c_int, dp]
+        L.orc_scatter_in.argtypes = [C.POINTER(abi.LumMaterial), C.c_uint32, C.c_uint32, dp, dp, dp, C.c_double,
+                                     C.c_double, C.c_double, C.c_uint64, C.c_int, dp]
+        L.orc_emitted.argtypes = [C.POINTER(abi.LumMaterial), C.c_uint32, C.c_uint32, C.c_double, C.c_double, dp]
+        L.orc_emitted.restype = C.c_double
+        L.orc_is_specular.argtypes = [C.POINTER(abi.LumMaterial)]
+        L.orc_thin_film.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int]
+        L.orc_thin_film.restype = C.c_double
         L.orc_schlick.argtypes = [C.c_double, C.c_double]
         L.orc_schlick.restype = C.c_double
         L.orc_ggx_d.argtypes = [C.c_double, C.c_double]
@@ -104,6 +113,8 @@ class OracleScene:
         if rc != 0:
             raise RuntimeError(f"orc_scene_create failed: {rc}")
         self.h = h
+        if getattr(world, "env_map", None) is not None:
+            self.set_envmap(world.env_map)
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -146,6 +157,26 @@ class OracleScene:
         if rc != 0:
             raise RuntimeError(f"orc_render failed: {rc}")
         return out, st
+
+    def set_envmap(self, rgb):
+        if rgb is None:
+            lib().orc_scene_set_envmap(self.h, None, 0, 0)
+            return
+        self._env = np.ascontiguousarray(rgb, dtype=np.float32)
+        lib().orc_scene_set_envmap(self.h, self._env.ctypes.data, self._env.shape[1], self._env.shape[0])
+
+    def render_aov(self, cfg, mode=MODE_KEYED):
+        """(depth (H, W) f64 holding f32 values, normals (H, W, 3) u8, albedo (H, W, 3) u8)."""
+        h, w, _ = cfg.out_shape()
+        p = cfg.to_c()
+        depth = np.zeros((h, w), dtype=np.float64)
+        normals = np.zeros((h, w, 3), dtype=np.uint8)
+        albedo = np.zeros((h, w, 3), dtype=np.uint8)
+        rc = lib().orc_render_aov(self.h, C.byref(p), mode, depth.ctypes.data, normals.ctypes.data,
+                                  albedo.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(f"orc_render_aov failed: {rc}")
+        return depth, normals, albedo
 
     def adjoint(self, cfg, dl_dimage, light_material=None, detach=True, threads=0):
         """f64 adjoint of the keyed estimator: (d_albedo (n,3), d_roughness (n,), d_emission (n,3),
@@ -215,16 +246,55 @@ def make_rays(org, dir, tmin=0.001, tmax=np.inf, time=0.0) -> np.ndarray:
     return r
 
 
-def scatter(material, ray_o, ray_d, point, outward_normal, t=1.0, u=0.5, v=0.5, seed=42, n_iter=1, time=0.0):
-    m = material.to_c()
+def _material_array(material):
+    """lum_material records of `material` (index 0) and every Blend child below it."""
+    order = []
+
+    def visit(m):
+        if any(m is x for x in order):
+            return
+        order.append(m)
+        for c in (m.children or ()):
+            visit(c)
+
+    visit(material)
+
+    def index_of(m):
+        return next(i for i, x in enumerate(order) if x is m)
+
+    return (abi.LumMaterial * len(order))(*[m.to_c(index_of) for m in order]), len(order)
+
+
+def scatter(material, ray_o, ray_d, point, outward_normal, t=1.0, u=0.5, v=0.5, seed=42, n_iter=1, time=0.0,
+            origin=False):
+    """Material::scatter n_iter times from one stream (stream mode): rows of ok, dir[3], att[3],
+    front_face (and origin[3] with origin=True)."""
+    arr, n = _material_array(material)
     ray = np.array([*ray_o, *ray_d, time], dtype=np.float64)
-    out = np.zeros((n_iter, 8))
+    out = np.zeros((n_iter, 11))
     p = np.asarray(point, dtype=np.float64)
-    n = np.asarray(outward_normal, dtype=np.float64)
-    lib().orc_scatter(C.byref(m), ray.ctypes.data_as(C.POINTER(C.c_double)),
-                      p.ctypes.data_as(C.POINTER(C.c_double)), n.ctypes.data_as(C.POINTER(C.c_double)),
-                      t, u, v, seed, n_iter, out.ctypes.data_as(C.POINTER(C.c_double)))
-    return out
+    nrm = np.asarray(outward_normal, dtype=np.float64)
+    dp = C.POINTER(C.c_double)
+    rc = lib().orc_scatter_in(arr, n, 0, ray.ctypes.data_as(dp), p.ctypes.data_as(dp), nrm.ctypes.data_as(dp),
+                              t, u, v, seed, n_iter, out.ctypes.data_as(dp))
+    if rc != 0:
+        raise RuntimeError(f"orc_scatter_in failed: {rc}")
+    return out if origin else out[:, :8]
+
+
+def emitted_sum(material, u=0.5, v=0.5, p=(0.0, 0.0, 0.0)):
+    arr, n = _material_array(material)
+    q = np.asarray(p, dtype=np.float64)
+    return lib().orc_emitted(arr, n, 0, u, v, q.ctypes.data_as(C.POINTER(C.c_double)))
+
+
+def is_specular(material):
+    m = material.to_c(lambda _m: 0)
+    return bool(lib().orc_is_specular(C.byref(m)))
+
+
+def thin_film(cos_theta, thickness, film_ior):
+    return np.array([lib().orc_thin_film(cos_theta, thickness, film_ior, c) for c in range(3)])
 
 
 def schlick(cosine, ref_idx):

@@ -27,6 +27,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <functional>
 #include <limits>
 #include <memory>
 #include <vector>
@@ -153,11 +154,11 @@ struct Sampler {
     Xoshiro* stream;
     uint32_t key[2];
     uint32_t pixel, stratum, bounce;
-    double cache[5][4];
-    bool have[5];
+    double cache[6][4];
+    bool have[6];
     void begin_bounce(uint32_t b) {
         bounce = b;
-        for (int i = 0; i < 5; ++i) have[i] = false;
+        for (int i = 0; i < 6; ++i) have[i] = false;
     }
     double keyed(int call, int slot) {
         if (!have[call]) {
@@ -173,7 +174,7 @@ struct Sampler {
     double draw(int call, int slot) { return mode == ORC_MODE_STREAM ? stream->next_f64() : keyed(call, slot); }
 };
 // Keyed call indices (must match the device mapping).
-enum { CALL_CAMERA = 0, CALL_CAMERA2 = 1, CALL_SCATTER = 2, CALL_NEE = 3, CALL_EXTRA = 4 };
+enum { CALL_CAMERA = 0, CALL_CAMERA2 = 1, CALL_SCATTER = 2, CALL_NEE = 3, CALL_EXTRA = 4, CALL_BLEND = 5 };
 
 // Direct samplers of the keyed mode.
 inline V3 keyed_unit_vector(double a, double b) {
@@ -295,18 +296,163 @@ struct Material {
     V3 albedo{0, 0, 0};
     double fuzz = 0, ior = 1.5, roughness = 0, metallic = 0, intensity = 1, dispersion = 0;
     V3 tint{1, 1, 1};
+    double extra[4] = {0, 0, 0, 0};   // the other materials' parameters (after their clamps)
+    V3 color2{0, 0, 0};               // Subsurface scatter_color
+    const Material* sub[2] = {nullptr, nullptr};   // Blend children
 
     bool is_specular() const {
         switch (kind) {
             case LUM_MAT_METAL: return true;                           // material.rs:90-92
             case LUM_MAT_DIELECTRIC: return true;                      // material.rs:145-147
             case LUM_MAT_MICROFACET: return metallic > 0.9 && roughness < 0.1;  // material.rs:323-326
-            default: return false;
+            case LUM_MAT_TRANSPARENT: return true;                     // material.rs:437-439
+            case LUM_MAT_IRIDESCENT: return true;                      // material.rs:495-497
+            case LUM_MAT_ANISOTROPIC: return true;                     // material.rs:603-605
+            default: return false;                                     // Blend: the trait default
         }
     }
     V3 emitted(double u, double v, V3 p) const {                       // material.rs:19-21, 241-243
         if (kind == LUM_MAT_EMISSIVE) return tex.value(u, v, p) * intensity;
+        if (kind == LUM_MAT_BLEND)                                     // material.rs:417-420
+            return sub[0]->emitted(u, v, p) * extra[0] + sub[1]->emitted(u, v, p) * (1.0 - extra[0]);
         return {0, 0, 0};
+    }
+    // Iridescent::thin_film_color (material.rs:469-491)
+    static V3 thin_film(double cos_theta, double thickness, double film_ior) {
+        double sin_theta = std::sqrt(1.0 - cos_theta * cos_theta);
+        double sin_f = sin_theta / film_ior;
+        double cos_f = std::sqrt(std::fmax(1.0 - sin_f * sin_f, 0.0));
+        double opd = 2.0 * thickness * film_ior * cos_f;
+        const double wl[3] = {650.0, 532.0, 450.0};
+        double c[3];
+        for (int i = 0; i < 3; ++i) {
+            double ph = 2.0 * PI * opd / wl[i];
+            double sn = std::sin(ph / 2.0);
+            c[i] = sn * sn;
+        }
+        return {c[0], c[1], c[2]};
+    }
+    // The other materials' scatter (material.rs:408-865); keyed slots as on the device.
+    bool scatter_other(const Ray& r, const HitRecord& h, Sampler& s, Scatter& out, int level) const {
+        switch (kind) {
+            case LUM_MAT_BLEND: {                                      // material.rs:408-415
+                double x = s.draw(CALL_BLEND, level);
+                return (x < extra[0] ? sub[0] : sub[1])->scatter(r, h, s, out, level + 1);
+            }
+            case LUM_MAT_TRANSPARENT:                                  // material.rs:429-435
+                out.ray = {h.p, r.d, r.time};
+                out.att = {1, 1, 1};
+                return true;
+            case LUM_MAT_IRIDESCENT: {                                 // material.rs:499-527
+                V3 ud = unit(r.d);
+                double ct = std::fmin(std::fabs(dot(-ud, h.n)), 1.0);
+                out.att = hadamard(albedo, thin_film(ct, extra[0], ior));
+                V3 dir = reflect(ud, h.n);
+                if (roughness > 0.0) {
+                    dir += random_in_unit_sphere_at(s, CALL_SCATTER, 0) * roughness;
+                    if (dot(dir, h.n) <= 0.0) return false;
+                }
+                out.ray = {h.p, dir, r.time};
+                return true;
+            }
+            case LUM_MAT_TOON: {                                       // material.rs:549-577
+                V3 dir = h.n + random_unit_vector(s, CALL_SCATTER, 0);
+                if (near_zero(dir)) dir = h.n;
+                double ndl = std::fmax(dot(unit(dir), h.n), 0.0);
+                double band = std::floor(ndl * extra[0]) / (extra[0] - 1.0);
+                double q = rclamp(band, 0.0, 1.0);
+                V3 view = unit(-r.d);
+                V3 hv = unit(view + unit(dir));
+                double spec = std::pow(std::fmax(dot(hv, h.n), 0.0), extra[1] * 100.0);
+                out.ray = {h.p, dir, r.time};
+                out.att = albedo * (q + (spec > 0.5 ? 0.3 : 0.0));
+                return true;
+            }
+            case LUM_MAT_ANISOTROPIC: {                                // material.rs:607-641
+                V3 refl = reflect(unit(r.d), h.n);
+                int ax = (int)extra[2];
+                V3 wt = ax == 0 ? v3(1, 0, 0) : (ax == 1 ? v3(0, 1, 0) : v3(0, 0, 1));
+                V3 t = unit(wt - h.n * dot(wt, h.n));
+                V3 b = cross(h.n, t);
+                double r1 = s.draw(CALL_SCATTER, 0) * 2.0 * PI;
+                double r2 = std::sqrt(s.draw(CALL_SCATTER, 1));
+                V3 sc = unit(refl + t * (std::cos(r1) * r2 * extra[0]) + b * (std::sin(r1) * r2 * extra[1]));
+                if (!(dot(sc, h.n) > 0.0)) return false;
+                out.ray = {h.p, sc, r.time};
+                out.att = albedo;
+                return true;
+            }
+            case LUM_MAT_CLEARCOAT: {                                  // material.rs:664-707
+                V3 ud = unit(r.d);
+                double ct = std::fmin(std::fabs(dot(-ud, h.n)), 1.0);
+                double r0 = (1.0 - ior) / (1.0 + ior);
+                r0 = r0 * r0;
+                double om = 1.0 - ct;
+                double fr = r0 + (1.0 - r0) * (om * om * om * om * om);
+                if (s.draw(CALL_SCATTER, 0) < fr * extra[0]) {
+                    V3 refl = reflect(ud, h.n);
+                    double rough = (1.0 - extra[0]) * 0.3;
+                    V3 dir = refl;
+                    if (rough > 0.001) {
+                        V3 fz = refl + random_in_unit_sphere_at(s, CALL_SCATTER, 1) * rough;
+                        if (dot(fz, h.n) > 0.0) dir = fz;
+                    }
+                    out.ray = {h.p, dir, r.time};
+                    out.att = {1, 1, 1};
+                    return true;
+                }
+                V3 dir = h.n + random_unit_vector(s, CALL_SCATTER, 1);
+                if (near_zero(dir)) dir = h.n;
+                out.ray = {h.p, dir, r.time};
+                out.att = albedo;
+                return true;
+            }
+            case LUM_MAT_VELVET: {                                     // material.rs:724-746
+                V3 dir = h.n + random_unit_vector(s, CALL_SCATTER, 0);
+                if (near_zero(dir)) dir = h.n;
+                double ct = std::fabs(dot(-unit(r.d), h.n));
+                double st = std::sqrt(std::fmax(1.0 - ct * ct, 0.0));
+                out.ray = {h.p, dir, r.time};
+                out.att = albedo * (1.0 + std::pow(st, 1.5) * extra[0]);
+                return true;
+            }
+            case LUM_MAT_TRANSLUCENT: {                                // material.rs:769-797
+                V3 dir;
+                if (s.draw(CALL_SCATTER, 0) < extra[0]) {
+                    V3 through = unit(r.d);
+                    V3 below = -h.n + random_unit_vector(s, CALL_SCATTER, 1);
+                    dir = through * (1.0 - extra[1]) + below * extra[1];
+                    if (near_zero(dir)) dir = -h.n;
+                } else {
+                    dir = h.n + random_unit_vector(s, CALL_SCATTER, 1);
+                    if (near_zero(dir)) dir = h.n;
+                }
+                out.ray = {h.p, dir, r.time};
+                out.att = albedo;
+                return true;
+            }
+            case LUM_MAT_SUBSURFACE: {                                 // material.rs:823-864
+                double fr = reflectance(std::fabs(dot(unit(r.d), h.n)), 1.0 / 1.4);
+                if (s.draw(CALL_SCATTER, 0) < fr) {
+                    V3 dir = h.n + random_unit_vector(s, CALL_SCATTER, 1);
+                    if (near_zero(dir)) dir = h.n;
+                    out.ray = {h.p, dir, r.time};
+                    out.att = albedo;
+                    return true;
+                }
+                double mfp = extra[0];
+                double step = -mfp * std::log(std::fmax(s.draw(CALL_SCATTER, 1), 1e-10));
+                V3 exit = h.p + random_unit_vector(s, CALL_SCATTER, 2) * step;
+                V3 ed = h.n + random_unit_vector(s, CALL_EXTRA, 0);
+                ed = near_zero(ed) ? h.n : unit(ed);
+                double k = -step / mfp;
+                out.ray = {exit, ed, r.time};
+                out.att = hadamard(albedo, v3(std::exp(k * (1.0 - color2.x)), std::exp(k * (1.0 - color2.y)),
+                                              std::exp(k * (1.0 - color2.z))));
+                return true;
+            }
+        }
+        return false;
     }
     static double reflectance(double cosine, double ref_idx) {         // material.rs:138-141
         double r0 = (1.0 - ref_idx) / (1.0 + ref_idx);
@@ -336,7 +482,8 @@ struct Material {
         return unit(tangent * h.x + bitangent * h.y + n * h.z);
     }
 
-    bool scatter(const Ray& r, const HitRecord& h, Sampler& s, Scatter& out) const {
+    bool scatter(const Ray& r, const HitRecord& h, Sampler& s, Scatter& out, int level = 0) const {
+        if (kind >= LUM_MAT_BLEND) return scatter_other(r, h, s, out, level);
         switch (kind) {
             case LUM_MAT_LAMBERTIAN: {                                 // material.rs:59-71
                 V3 dir = h.n + random_unit_vector(s, CALL_SCATTER, 0);
@@ -454,7 +601,57 @@ Material make_material(const lum_material& m) {
     out.intensity = m.intensity;
     out.dispersion = m.dispersion;
     out.tint = from(m.tint);
+    out.color2 = from(m.color2);
+    const double* e = m.extra;
+    auto cl = [](double x, double lo, double hi) { return std::fmin(std::fmax(x, lo), hi); };
+    switch (m.kind) {                                                   // the constructors' clamps
+        case LUM_MAT_BLEND: out.extra[0] = cl(e[0], 0.0, 1.0); break;  // material.rs:402-406
+        case LUM_MAT_IRIDESCENT:                                        // material.rs:459-466
+            out.extra[0] = std::fmax(e[0], 100.0);
+            out.ior = std::fmax(m.ior, 1.0);
+            out.roughness = cl(m.roughness, 0.0, 1.0);
+            break;
+        case LUM_MAT_TOON:                                              // material.rs:538-545
+            out.extra[0] = std::fmax(std::floor(cl(e[0], 0.0, 4294967295.0)), 2.0);
+            out.extra[1] = std::fmax(e[1], 0.0);
+            break;
+        case LUM_MAT_ANISOTROPIC:                                       // material.rs:592-599
+            out.extra[0] = cl(e[0], 0.001, 1.0);
+            out.extra[1] = cl(e[1], 0.001, 1.0);
+            out.extra[2] = std::fmin(std::floor(std::fmax(e[2], 0.0)), 2.0);
+            break;
+        case LUM_MAT_CLEARCOAT:                                         // material.rs:655-661
+            out.extra[0] = cl(e[0], 0.0, 1.0);
+            out.ior = std::fmax(m.ior, 1.0);
+            break;
+        case LUM_MAT_VELVET: out.extra[0] = cl(e[0], 0.0, 2.0); break;  // material.rs:718-720
+        case LUM_MAT_TRANSLUCENT:                                       // material.rs:760-766
+            out.extra[0] = cl(e[0], 0.0, 1.0);
+            out.extra[1] = cl(e[1], 0.0, 1.0);
+            break;
+        case LUM_MAT_SUBSURFACE: out.extra[0] = std::fmax(e[0], 0.001); break;  // material.rs:812-818
+        default: break;
+    }
     return out;
+}
+
+// Links Blend children (indices into the same array); false when an index is out of range or
+// Blends nest more than 4 deep (the device's limit).
+bool link_blends(std::vector<Material>& ms, const lum_material* mats, uint32_t n) {
+    for (uint32_t i = 0; i < n; ++i) {
+        if (mats[i].kind != LUM_MAT_BLEND) continue;
+        for (int k = 0; k < 2; ++k) {
+            if (mats[i].sub[k] < 0 || (uint32_t)mats[i].sub[k] >= n) return false;
+            ms[i].sub[k] = &ms[mats[i].sub[k]];
+        }
+    }
+    std::function<bool(const Material*, int)> ok = [&](const Material* m, int lv) {
+        if (m->kind != LUM_MAT_BLEND) return true;
+        return lv < 4 && ok(m->sub[0], lv + 1) && ok(m->sub[1], lv + 1);
+    };
+    for (uint32_t i = 0; i < n; ++i)
+        if (!ok(&ms[i], 0)) return false;
+    return true;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1057,8 +1254,48 @@ double filter_weight(int f, double dx, double dy) {                     // rende
     }
 }
 
-V3 background(const lum_render_params& p, const Ray& r) {               // render.rs:73-171
+// Equirectangular environment map (Background::EnvMap).
+struct EnvMap {
+    std::vector<float> px;
+    uint32_t w = 0, h = 0;
+};
+
+V3 background(const lum_render_params& p, const Ray& r, const EnvMap* env) {   // render.rs:73-171
     switch (p.background) {
+        case LUM_BG_STARFIELD: {                                        // render.rs:86-112
+            V3 ud = unit(r.d);
+            double t = 0.5 * (ud.y + 1.0);
+            V3 space = v3(0.0, 0.0, 0.02) * (1.0 - t) + v3(0.02, 0.0, 0.05) * t;
+            double scale = 500.0 * p.bg_star_density;
+            int64_t ix = (int64_t)std::floor(ud.x * scale), iy = (int64_t)std::floor(ud.y * scale),
+                    iz = (int64_t)std::floor(ud.z * scale);
+            uint64_t hash = ((uint64_t)ix * 73856093ull) ^ ((uint64_t)iy * 19349663ull) ^ ((uint64_t)iz * 83492791ull);
+            double star = (double)(hash % 10000) / 10000.0;
+            if (!(star > 0.997)) return space;
+            double rh = (double)((hash >> 8) % 100) / 100.0;
+            V3 c = rh < 0.3 ? v3(1.0, 0.9, 0.8) : (rh < 0.6 ? v3(0.9, 0.9, 1.0) : v3(1, 1, 1));
+            return space + c * (star * p.bg_star_brightness);
+        }
+        case LUM_BG_ENVMAP: {                                           // render.rs:113-151
+            if (!env || env->w == 0) return {0, 0, 0};
+            V3 ud = unit(r.d);
+            double theta = std::acos(-ud.y);
+            double phi = std::atan2(-ud.z, ud.x) + PI;
+            double u = phi / (2.0 * PI), v = theta / PI;
+            double fx = u * env->w - 0.5, fy = v * env->h - 0.5;
+            int64_t w = env->w, h = env->h;
+            int64_t x0 = (((int64_t)std::floor(fx)) % w + w) % w;
+            int64_t y0 = (int64_t)rclamp(std::floor(fy), 0.0, (double)(h - 1));
+            int64_t x1 = (x0 + 1) % w, y1 = std::min<int64_t>(y0 + 1, h - 1);
+            double tx = fx - std::floor(fx), ty = fy - std::floor(fy);
+            auto at = [&](int64_t x, int64_t y) {
+                const float* q = &env->px[3 * (size_t)(y * w + x)];
+                return v3(q[0], q[1], q[2]);
+            };
+            V3 c = at(x0, y0) * ((1.0 - tx) * (1.0 - ty)) + at(x1, y0) * (tx * (1.0 - ty)) +
+                   at(x0, y1) * ((1.0 - tx) * ty) + at(x1, y1) * (tx * ty);
+            return c * p.bg_intensity;
+        }
         case LUM_BG_SOLID: return from(p.bg_color);
         case LUM_BG_GRADIENT: {
             V3 ud = unit(r.d);
@@ -1092,6 +1329,7 @@ V3 background(const lum_render_params& p, const Ray& r) {               // rende
 // ---------------------------------------------------------------------------------------
 struct orc_scene {
     std::vector<Material> mats;
+    EnvMap env;
     HPtr bvh;
     std::vector<HPtr> unbounded;
     std::vector<const Hittable*> top;   // every top-level object (tie queries)
@@ -1185,6 +1423,10 @@ int orc_scene_create(const lum_scene_desc* d, orc_scene** out) {
     auto* s = new orc_scene();
     s->mats.reserve(d->n_materials);
     for (uint32_t i = 0; i < d->n_materials; ++i) s->mats.push_back(make_material(d->materials[i]));
+    if (!link_blends(s->mats, d->materials, d->n_materials)) {
+        delete s;
+        return 3;
+    }
     s->cam_desc = d->camera;
     s->cam.init(d->camera);
     std::vector<HPtr> world;
@@ -1512,7 +1754,7 @@ V3 ray_color_stream(const orc_scene& sc, const lum_render_params& p, const Ray& 
         }
         return emitted;
     }
-    return background(p, r);
+    return background(p, r, &sc.env);
 }
 
 // Keyed mode: the device estimator (iterative; draws addressed per bounce).  Same terms as
@@ -1528,7 +1770,7 @@ V3 ray_color_keyed(const orc_scene& sc, const lum_render_params& p, Ray r, Sampl
         HitRecord h;
         cnt.segments++;
         if (!sc.hit(r, 0.001, INF, h)) {
-            L += hadamard(B, background(p, r));
+            L += hadamard(B, background(p, r, &sc.env));
             break;
         }
         // Non-finite vertex: the recursion's NaN guard zeroes this level and deeper.
@@ -1764,9 +2006,86 @@ int orc_render_expired(const orc_scene* sc, const lum_render_params* p, int mode
     return render_rows(sc, p, mode, threads, 0, (uint32_t)f.h, out, st, 1);
 }
 
-int orc_scatter(const lum_material* lm, const double ray[7], const double hp[3], const double on[3], double t,
-                double u, double v, uint64_t seed, int n_iter, double* out) {
-    Material m = make_material(*lm);
+int orc_scene_set_envmap(orc_scene* sc, const float* rgb, uint32_t w, uint32_t h) {
+    if (!sc) return 1;
+    if (!rgb || !w || !h) {
+        sc->env = EnvMap{};
+        return 0;
+    }
+    sc->env.px.assign(rgb, rgb + 3 * (size_t)w * h);
+    sc->env.w = w;
+    sc->env.h = h;
+    return 0;
+}
+
+// AOV passes (render.rs:3508-3568): one ray per pixel through the pixel centre.  Stream mode:
+// the reference's per-pixel SmallRng seeded with (j * W + i) * seed (wrapping); keyed mode:
+// the draws of (pixel, stratum 0, bounce 0) as on the device.
+int orc_render_aov(const orc_scene* sc, const lum_render_params* pp, int mode, double* depth, uint8_t* normals,
+                   uint8_t* albedo) {
+    if (!sc || !pp) return 1;
+    const lum_render_params& p = *pp;
+    Frame f = frame_of(p);
+    auto to_u8 = [](double x) -> uint8_t {            // Rust `as u8`: NaN -> 0, saturating
+        if (!(x > 0.0)) return 0;
+        if (x >= 255.0) return 255;
+        return (uint8_t)x;
+    };
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t j = 0; j < (int64_t)f.h; ++j) {
+        size_t gj = (size_t)j + f.crop_y;
+        double y = (double)(f.full_h - 1 - gj);
+        for (size_t i = 0; i < f.w; ++i) {
+            size_t gi = i + f.crop_x;
+            size_t o = (size_t)j * f.w + i;
+            Xoshiro rng(((uint64_t)gj * (uint64_t)f.full_w + (uint64_t)gi) * p.seed);
+            Sampler s;
+            s.mode = mode;
+            s.stream = &rng;
+            s.key[0] = (uint32_t)p.seed;
+            s.key[1] = (uint32_t)(p.seed >> 32);
+            s.pixel = (uint32_t)(gj * f.full_w + gi);
+            s.stratum = 0;
+            s.begin_bounce(0);
+            double uc = ((double)gi + 0.5) / (double)(f.full_w - 1);
+            double vc = (y + 0.5) / (double)(f.full_h - 1);
+            Ray ray = sc->cam.get_ray(uc, vc, s);
+            HitRecord h;
+            double dv = 0.0;
+            uint8_t nb[3] = {0, 0, 0}, ab[3] = {0, 0, 0};
+            if (sc->hit(ray, 0.001, INF, h)) {
+                dv = (double)(float)h.t;
+                const double n[3] = {h.n.x, h.n.y, h.n.z};
+                for (int c = 0; c < 3; ++c) nb[c] = to_u8(rclamp((n[c] * 0.5 + 0.5) * 255.0, 0.0, 255.0));
+                Scatter sct;
+                if (h.mat && h.mat->scatter(ray, h, s, sct)) {
+                    const double a[3] = {sct.att.x, sct.att.y, sct.att.z};
+                    for (int c = 0; c < 3; ++c) ab[c] = to_u8(rclamp(a[c], 0.0, 1.0) * 255.0);
+                } else if (h.mat) {
+                    V3 e = h.mat->emitted(h.u, h.v, h.p);
+                    double me = std::fmax(std::fmax(e.x, std::fmax(e.y, e.z)), 1.0);
+                    const double a[3] = {e.x, e.y, e.z};
+                    for (int c = 0; c < 3; ++c) ab[c] = to_u8(rclamp(a[c] / me * 255.0, 0.0, 255.0));
+                }
+            }
+            if (depth) depth[o] = dv;
+            for (int c = 0; c < 3; ++c) {
+                if (normals) normals[3 * o + c] = nb[c];
+                if (albedo) albedo[3 * o + c] = ab[c];
+            }
+        }
+    }
+    return 0;
+}
+
+int orc_scatter_in(const lum_material* mats, uint32_t n_mats, uint32_t index, const double ray[7], const double hp[3],
+                   const double on[3], double t, double u, double v, uint64_t seed, int n_iter, double* out) {
+    if (!mats || index >= n_mats) return 1;
+    std::vector<Material> ms;
+    ms.reserve(n_mats);
+    for (uint32_t i = 0; i < n_mats; ++i) ms.push_back(make_material(mats[i]));
+    if (!link_blends(ms, mats, n_mats)) return 2;
+    const Material& m = ms[index];
     Xoshiro rng(seed);
     Sampler s;
     s.mode = ORC_MODE_STREAM;
@@ -1782,14 +2101,41 @@ int orc_scatter(const lum_material* lm, const double ray[7], const double hp[3],
     for (int i = 0; i < n_iter; ++i) {
         Scatter sc;
         bool ok = m.scatter(r, h, s, sc);
-        double* o = out + (size_t)i * 8;
+        double* o = out + (size_t)i * 11;
         o[0] = ok ? 1.0 : 0.0;
         o[1] = sc.ray.d.x; o[2] = sc.ray.d.y; o[3] = sc.ray.d.z;
         o[4] = sc.att.x; o[5] = sc.att.y; o[6] = sc.att.z;
         o[7] = h.front_face ? 1.0 : 0.0;
-        if (!ok) { o[1] = o[2] = o[3] = o[4] = o[5] = o[6] = 0.0; }
+        o[8] = sc.ray.o.x; o[9] = sc.ray.o.y; o[10] = sc.ray.o.z;
+        if (!ok) o[1] = o[2] = o[3] = o[4] = o[5] = o[6] = o[8] = o[9] = o[10] = 0.0;
     }
     return 0;
+}
+
+int orc_scatter(const lum_material* lm, const double ray[7], const double hp[3], const double on[3], double t,
+                double u, double v, uint64_t seed, int n_iter, double* out) {
+    std::vector<double> full((size_t)std::max(n_iter, 0) * 11);
+    int rc = orc_scatter_in(lm, 1, 0, ray, hp, on, t, u, v, seed, n_iter, full.data());
+    if (rc) return rc;
+    for (int i = 0; i < n_iter; ++i)
+        for (int k = 0; k < 8; ++k) out[(size_t)i * 8 + k] = full[(size_t)i * 11 + k];
+    return 0;
+}
+
+double orc_emitted(const lum_material* mats, uint32_t n_mats, uint32_t index, double u, double v,
+                   const double p[3]) {
+    std::vector<Material> ms;
+    for (uint32_t i = 0; i < n_mats; ++i) ms.push_back(make_material(mats[i]));
+    if (index >= n_mats || !link_blends(ms, mats, n_mats)) return NAN;
+    V3 e = ms[index].emitted(u, v, from(p));
+    return e.x + e.y + e.z;
+}
+
+int orc_is_specular(const lum_material* m) { return make_material(*m).is_specular() ? 1 : 0; }
+
+double orc_thin_film(double cos_theta, double thickness, double film_ior, int channel) {
+    V3 c = Material::thin_film(cos_theta, thickness, film_ior);
+    return channel == 0 ? c.x : (channel == 1 ? c.y : c.z);
 }
 
 double orc_schlick(double c, double r) { return Material::reflectance(c, r); }
@@ -2130,7 +2476,7 @@ DV path_dual(const AdjCtx& C, Ray r, Sampler& s, uint32_t max_depth, Counters& c
         HitRecord h;
         cnt.segments++;
         if (!sc.hit(r, 0.001, INF, h)) {
-            L = L + had(B, dv(background(*C.p, r)));
+            L = L + had(B, dv(background(*C.p, r, &C.sc->env)));
             break;
         }
         if (!std::isfinite(h.p.x) || !std::isfinite(h.p.y) || !std::isfinite(h.p.z)) break;

@@ -77,7 +77,24 @@ int orc_render_expired(const orc_scene* s, const lum_render_params* p, int mode,
 int orc_render_rows(const orc_scene* s, const lum_render_params* p, int mode, int threads,
                     uint32_t row_begin, uint32_t row_end, double* out_rgb, orc_stats* stats);
 
+/* Environment map of LUM_BG_ENVMAP: width*height*3 floats, top row first (NULL removes it). */
+int orc_scene_set_envmap(orc_scene* s, const float* rgb, uint32_t width, uint32_t height);
+/* AOV passes (render.rs:3508-3568): depth (W*H doubles, the f32 value of t), normals and
+ * albedo (W*H*3 bytes); any may be NULL. */
+int orc_render_aov(const orc_scene* s, const lum_render_params* p, int mode, double* depth, uint8_t* normals,
+                   uint8_t* albedo);
+
 /* Known-answer helpers mirroring the reference's unit tests. */
+/* Material::scatter of mats[index] (Blend children index the same array); n_iter rows of 11:
+ * ok, dir[3], att[3], front_face, origin[3]. */
+int orc_scatter_in(const lum_material* mats, uint32_t n_mats, uint32_t index, const double ray[7],
+                   const double hit_point[3], const double outward_normal[3], double t, double u, double v,
+                   uint64_t seed, int n_iter, double* out);
+/* Sum of the three channels of mats[index].emitted(u, v, p). */
+double orc_emitted(const lum_material* mats, uint32_t n_mats, uint32_t index, double u, double v, const double p[3]);
+int orc_is_specular(const lum_material* m);
+/* Iridescent::thin_film_color channel (0 r, 1 g, 2 b). */
+double orc_thin_film(double cos_theta, double thickness, double film_ior, int channel);
 int orc_scatter(const lum_material* m, const double ray[7], const double hit_point[3],
                 const double outward_normal[3], double t, double u, double v, uint64_t seed,
                 int n_iter, double* out /* n_iter * 8: ok, dir[3], att[3], front */);

@@ -328,6 +328,89 @@ def _nee_scene(blocker: bool):
     return O.OracleScene(w)
 
 
+# ---------------------------------------------------------------- material.rs:396-865, tests :1063-1298
+def test_blend_chooses_between_materials():                      # material.rs:1063-1088
+    mat = S.Blend(S.Lambertian((1.0, 0.0, 0.0)), S.Metal((0.0, 0.0, 1.0), 0.0), 0.5)
+    out = O.scatter(mat, seed=42, n_iter=100, **HIT)
+    ok = out[:, 0] == 1
+    assert (out[ok, 4] > 0.5).any() and (out[ok, 6] > 0.5).any()
+    # ratio 1 always picks mat_a; the blend's emission is the ratio mix (:417-420)
+    assert (O.scatter(S.Blend(S.Lambertian((1, 0, 0)), S.Metal((0, 0, 1), 0.0), 1.0), n_iter=50, **HIT)[:, 4] == 1).all()
+    glow = S.Emissive((1.0, 1.0, 1.0), 4.0)
+    assert abs(O.emitted_sum(S.Blend(glow, S.Lambertian((1, 1, 1)), 0.25)) - 3.0) < 1e-12
+    assert abs(O.emitted_sum(S.Blend(S.Blend(glow, glow, 0.5), S.Lambertian((1, 1, 1)), 0.5)) - 6.0) < 1e-12
+    assert not O.is_specular(mat)                                 # the trait default
+
+
+def test_transparent_passes_straight_through():                  # material.rs:429-440
+    h = dict(HIT, ray_d=(0.3, -1.0, 0.2))
+    out = O.scatter(S.Transparent(), seed=1, n_iter=3, **h)
+    np.testing.assert_array_equal(out[:, 1:4], np.tile([0.3, -1.0, 0.2], (3, 1)))
+    np.testing.assert_array_equal(out[:, 4:7], 1.0)
+    assert O.is_specular(S.Transparent())
+
+
+def test_iridescent_color_varies_with_angle():                   # material.rs:1178-1196
+    c1 = O.thin_film(1.0, 400.0, 1.4)
+    c2 = O.thin_film(0.3, 400.0, 1.4)
+    assert np.abs(c1 - c2).sum() > 0.01
+    # known answer at normal incidence: sin^2(2 pi (2 t n) / lambda / 2)
+    np.testing.assert_allclose(c1, np.sin(np.pi * 2 * 400.0 * 1.4 / np.array([650.0, 532.0, 450.0])) ** 2, rtol=1e-12)
+    out = O.scatter(S.Iridescent((1.0, 1.0, 1.0), 400.0, 1.4, 0.0), seed=42, **HIT)
+    assert out[0, 0] == 1 and np.linalg.norm(out[0, 1:4]) > 1e-6 and out[0, 4] >= 0.0
+    np.testing.assert_allclose(out[0, 1:4], [0, 1, 0], atol=1e-12)           # mirror, no roughness
+    np.testing.assert_allclose(out[0, 4:7], c1, rtol=1e-12)
+    # the constructor's clamps: thickness >= 100, film_ior >= 1
+    np.testing.assert_allclose(O.scatter(S.Iridescent((1, 1, 1), 10.0, 0.5, 0.0), **HIT)[0, 4:7],
+                               O.thin_film(1.0, 100.0, 1.0), rtol=1e-12)
+
+
+def test_translucent_transmits_and_reflects():                   # material.rs:1198-1220
+    out = O.scatter(S.Translucent((0.8, 0.9, 0.7), 0.5, 0.8), seed=42, n_iter=200, **HIT)
+    assert (out[:, 0] == 1).all()
+    below = out[:, 1:4] @ np.array([0.0, 1.0, 0.0]) < 0.0
+    assert below.sum() > 30 and (~below).sum() > 30
+    np.testing.assert_allclose(out[:, 4], 0.8, atol=1e-6)
+
+
+def test_subsurface_scatters_near_surface():                     # material.rs:1237-1259, 1261-1265
+    mat = S.Subsurface((0.9, 0.7, 0.6), 0.5, (0.9, 0.4, 0.3))
+    out = O.scatter(mat, seed=42, n_iter=2000, origin=True, **HIT)
+    ok = out[:, 0] == 1
+    assert ok.sum() > 50
+    assert (out[ok, 4:7] >= 0.0).all() and (np.linalg.norm(out[ok, 1:4], axis=1) > 1e-6).all()
+    assert not O.is_specular(mat)
+    # subsurface branch: exit point at an Exp(mfp) distance; attenuation exp(-s/mfp (1 - c))
+    moved = np.linalg.norm(out[:, 8:11], axis=1) > 0
+    s = np.linalg.norm(out[moved, 8:11], axis=1)
+    assert abs(s.mean() / 0.5 - 1.0) < 0.1
+    np.testing.assert_allclose(out[moved, 5] / 0.7, np.exp(-s / 0.5 * (1 - 0.4)), rtol=1e-9)
+
+
+def test_toon_velvet_clearcoat_anisotropic_known_answers():
+    # Velvet: att = color (1 + sin^1.5 theta * sheen) (material.rs:734-741)
+    h = dict(HIT, ray_d=(0.6, -0.8, 0.0), ray_o=(-0.6, 0.8, 0.0))
+    out = O.scatter(S.Velvet((0.5, 0.4, 0.3), 1.5), n_iter=5, **h)
+    np.testing.assert_allclose(out[:, 4], 0.5 * (1 + 0.6 ** 1.5 * 1.5), rtol=1e-12)
+    # Toon: attenuation is color * (band + 0 or 0.3); bands >= 2 (material.rs:538-577)
+    out = O.scatter(S.Toon((1.0, 1.0, 1.0), 3, 0.2), n_iter=300, **HIT)
+    vals = np.unique(np.round(out[:, 4], 12))
+    assert set(vals) <= {0.0, 0.3, 0.5, 0.8, 1.0, 1.3}
+    # specular 0: pow(x, 0) = 1 > 0.5 adds the highlight band everywhere
+    assert (O.scatter(S.Toon((1, 1, 1), 2, 0.0), n_iter=50, **HIT)[:, 4] >= 0.3).all()
+    # Clearcoat: the coat reflects white, the base diffuses its colour (material.rs:664-707)
+    out = O.scatter(S.Clearcoat((0.7, 0.1, 0.1), 1.0, 1.5), n_iter=2000,
+                    **dict(HIT, ray_d=(0.995, -0.0998, 0), ray_o=(-1, 0.1, 0)))
+    white = np.all(out[:, 4:7] == 1.0, axis=1)
+    assert 0.3 < white.mean() < 0.9 and np.allclose(out[~white, 4:7], [0.7, 0.1, 0.1])
+    # Anisotropic: specular; rays stay above the surface or are absorbed (material.rs:607-641)
+    out = O.scatter(S.Anisotropic((0.9, 0.8, 0.6), 0.5, 0.05, 0), n_iter=200, **HIT)
+    ok = out[:, 0] == 1
+    assert ok.mean() > 0.9 and (out[ok, 2] > 0).all()
+    assert np.abs(out[ok, 1]).std() > 3 * np.abs(out[ok, 3]).std()      # stretched along the tangent (x)
+    assert O.is_specular(S.Anisotropic((1, 1, 1), 0.5, 0.5, 1))
+
+
 def test_nee_direct_light_nonzero():
     r = _nee_scene(False).sample_direct_light((0, 0, 0), (0, 1, 0), (0.8, 0.8, 0.8), 42, 1000)
     avg = r.mean(axis=0)

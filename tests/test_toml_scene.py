@@ -246,11 +246,109 @@ def test_adaptive_keys_reach_the_render_config():
     assert not cfg.adaptive and cfg.adaptive_threshold == 0.03          # render.rs:455-456
 
 
+OTHER_MATERIALS = """
+[render]
+width = 32
+height = 24
+samples = 4
+background = { type = "starfield", star_density = 0.5 }
+
+[[sphere]]
+center = [0.0, 0.0, 0.0]
+radius = 1.0
+material = { type = "toon", color = [0.2, 0.5, 0.9] }
+
+[[sphere]]
+center = [2.0, 0.0, 0.0]
+radius = 1.0
+material = { type = "brushed", color = [0.8, 0.8, 0.85], roughness_u = 0.05 }
+
+[[sphere]]
+center = [4.0, 0.0, 0.0]
+radius = 1.0
+material = { type = "blend", ratio = 0.25, material_a = { type = "velvet", color = [0.5, 0.1, 0.1] }, material_b = { type = "sss", color = [0.9, 0.7, 0.6] } }
+
+[[sphere]]
+center = [6.0, 0.0, 0.0]
+radius = 1.0
+material = { type = "opacity", opacity = 1.5, material = { type = "clearcoat", color = [0.8, 0.1, 0.05] } }
+
+[[sphere]]
+center = [8.0, 0.0, 0.0]
+radius = 1.0
+material = { type = "iridescent", thickness = 500 }
+
+[[sphere]]
+center = [10.0, 0.0, 0.0]
+radius = 1.0
+material = { type = "translucent", color = [0.7, 0.9, 0.7] }
+"""
+
+
+def test_other_materials_and_starfield():
+    cfg, world, _ = load_scene(OTHER_MATERIALS)
+    assert cfg.background == abi.BG_STARFIELD and cfg.bg_star_density == 0.5 and cfg.bg_star_brightness == 5.0
+    kinds = [o.material.kind for o in world.objects]
+    assert kinds == [abi.MAT_TOON, abi.MAT_ANISOTROPIC, abi.MAT_BLEND, abi.MAT_BLEND, abi.MAT_IRIDESCENT,
+                     abi.MAT_TRANSLUCENT]
+    toon, aniso, blend, opac, irid, transl = [o.material for o in world.objects]
+    assert tuple(toon.extra) == (3, 0.5)                                     # scene.rs:1991-1996 defaults
+    assert tuple(aniso.extra) == (0.05, 0.5, 1)
+    assert blend.extra[0] == 0.25 and [c.kind for c in blend.children] == [abi.MAT_VELVET, abi.MAT_SUBSURFACE]
+    assert tuple(blend.children[1].color2) == (0.8, 0.5, 0.5) and blend.children[1].extra[0] == 0.5
+    assert opac.extra[0] == 1.0 and [c.kind for c in opac.children] == [abi.MAT_CLEARCOAT, abi.MAT_TRANSPARENT]
+    assert tuple(irid.color) == (0.9, 0.9, 0.9) and irid.extra[0] == 500 and irid.ior == 1.4
+    assert tuple(transl.extra) == (0.5, 0.8)
+    img, st = O.OracleScene(world).render(cfg, mode=O.MODE_KEYED)
+    assert np.isfinite(img).all() and st.paths == 32 * 24 * 4
+
+
+def _write_hdr(path, img, rle):
+    """Radiance RGBE writer (test fixture): flat or new-style RLE scanlines (literal runs)."""
+    h, w, _ = img.shape
+    m = img.max(axis=2)
+    e = np.where(m > 1e-32, np.floor(np.log2(np.maximum(m, 1e-32))) + 1, 0).astype(np.int32)
+    mant = np.where(m[..., None] > 1e-32, img / np.ldexp(1.0, e - 8)[..., None], 0)
+    rgbe = np.concatenate([np.clip(mant, 0, 255).astype(np.uint8), np.where(m > 1e-32, e + 128, 0)[..., None]
+                           .astype(np.uint8)], axis=2)
+    with open(path, "wb") as f:
+        f.write(b"#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n" + f"-Y {h} +X {w}\n".encode())
+        for y in range(h):
+            if not rle:
+                f.write(rgbe[y].tobytes())
+                continue
+            f.write(bytes([2, 2, w >> 8, w & 255]))
+            for c in range(4):
+                row = rgbe[y, :, c]
+                for x0 in range(0, w, 128):
+                    chunk = row[x0:x0 + 128]
+                    f.write(bytes([len(chunk)]) + chunk.tobytes())
+    return rgbe
+
+
+@pytest.mark.parametrize("rle", [False, True])
+def test_env_map_hdr_and_png(tmp_path, rle):
+    from luminara_b200.toml_scene import load_env_map
+    rng = np.random.default_rng(1)
+    img = (rng.random((6, 16, 3)) * 4.0).astype(np.float32)
+    rgbe = _write_hdr(str(tmp_path / "sky.hdr"), img, rle)
+    got = load_env_map(str(tmp_path / "sky.hdr"))
+    want = rgbe[..., :3] * np.ldexp(1.0, rgbe[..., 3].astype(int) - 136)[..., None]
+    np.testing.assert_allclose(got, want, rtol=1e-6)
+    assert (np.abs(got - img) <= img.max(axis=2, keepdims=True) / 64).all()  # 8-bit shared-exponent mantissas
+    from PIL import Image
+    px = (rng.random((5, 9, 3)) * 255).astype(np.uint8)
+    Image.fromarray(px).save(str(tmp_path / "sky.png"))
+    np.testing.assert_allclose(load_env_map(str(tmp_path / "sky.png")), px / 255.0, rtol=1e-6)
+    cfg, world, _ = load_scene('[render]\nbackground = { type = "env_map", file = "sky.png", intensity = 2.0 }\n',
+                               base_dir=str(tmp_path))
+    assert cfg.background == abi.BG_ENVMAP and cfg.bg_intensity == 2.0 and world.env_map.shape == (5, 9, 3)
+
+
 def test_unsupported_features_are_named():
     text = """
 [render]
 firefly_filter = 4.0
-background = { type = "starfield" }
 
 [camera]
 panorama = true
@@ -270,7 +368,7 @@ material = { type = "marble", color = [0.5, 0.5, 0.5] }
     with pytest.raises(UnsupportedSceneError) as e:
         load_scene(text)
     items = e.value.items
-    for want in ("[torus]", "render.firefly_filter", "starfield", "camera.panorama", "bump_strength", "'marble'"):
+    for want in ("[torus]", "render.firefly_filter", "camera.panorama", "bump_strength", "'marble'"):
         assert any(want in it for it in items), (want, items)
 
 
