@@ -658,7 +658,8 @@ __global__ void __launch_bounds__(128, LUM_ADJ_MIN_BLOCKS) k_replay(SceneDev S, 
                     Surface sf = surface_of(S, in, h);
                     const bool finite = isfinite(sf.p.x) && isfinite(sf.p.y) && isfinite(sf.p.z);
                     const uint32_t b0 = P.bounce;
-                    const int stt = shade(S, R, pixel, P, true, h, pend);
+                    // the adjoint rejects the other materials: the base-material shading
+                    const int stt = shade<-1, false>(S, R, pixel, P, true, h, pend);
                     if (finite) {
                         Vert& vx = verts[(size_t)K * n_slots + slot];
                         vx.p = sf.p;

@@ -47,8 +47,15 @@ struct alignas(16) MatDev {
     int32_t specular;
     float extra[4];      // per-kind parameters of the other materials (lum_material.extra)
     int32_t sub[2];      // Blend: the blended materials
-    int32_t emits;       // Blend: some leaf below it is emissive
-    int32_t pad;
+    int32_t n_emit;      // Blend: emissive leaves below it (entries of SceneDev::blend_emit)
+    int32_t emit_first;  // Blend: its first entry in SceneDev::blend_emit
+};
+
+// A Blend's emission flattened: sum over its emissive leaves of weight * emitted(leaf), the
+// weight being the product of the ratios (or 1 - ratio) on the way down.
+struct BlendEmit {
+    int32_t leaf;
+    float weight;
 };
 
 struct alignas(16) LightDev {
@@ -101,6 +108,7 @@ struct SceneDev {
     int32_t n_planes;
     int32_t n_mats;
     int32_t pad;
+    const BlendEmit* blend_emit;   // emissive leaves of Blend materials
     const float* env;        // environment map, env_w * env_h RGB floats (or null)
     uint32_t env_w, env_h;
     CameraDev cam;
@@ -137,6 +145,8 @@ struct RenderDev {
     float exposure;
     uint32_t tiles_x, n_tasks;
     float star_density, star_brightness;   // STARFIELD background
+    uint32_t ext;            // the scene or background uses the other materials / backgrounds
+    uint32_t pad_ext;
 };
 
 }  // namespace lum

@@ -459,28 +459,35 @@ lum::MatDev make_mat(const lum_material& m) {
 }
 
 // Blend trees: children in range, nesting at most kMaxBlendDepth levels (which also rules out
-// cycles); `emits` marks Blends with an emissive leaf.
-lum_status check_blends(const lum_scene_desc& d, std::vector<lum::MatDev>& mats) {
+// cycles); each Blend's emissive leaves with their weights go to `table` (Blend::emitted,
+// material.rs:417-420, flattened).
+lum_status check_blends(const lum_scene_desc& d, std::vector<lum::MatDev>& mats, std::vector<lum::BlendEmit>& table) {
     const int n = (int)d.n_materials;
-    std::function<int(int, int)> depth = [&](int i, int level) -> int {
+    std::function<int(int, int, double, std::vector<lum::BlendEmit>&)> walk =
+        [&](int i, int level, double w, std::vector<lum::BlendEmit>& out) -> int {
         const lum_material& m = d.materials[i];
-        if (m.kind != LUM_MAT_BLEND) return m.kind == LUM_MAT_EMISSIVE ? 1 : 0;
+        if (m.kind != LUM_MAT_BLEND) {
+            if (m.kind == LUM_MAT_EMISSIVE) out.push_back({i, (float)w});
+            return 0;
+        }
         if (level > lum::kMaxBlendDepth) return -1;
-        int r = 0;
+        const double r = std::min(std::max(m.extra[0], 0.0), 1.0);
         for (int k = 0; k < 2; ++k) {
             if (m.sub[k] < 0 || m.sub[k] >= n) return -2;
-            int c = depth(m.sub[k], level + 1);
+            int c = walk(m.sub[k], level + 1, w * (k == 0 ? r : 1.0 - r), out);
             if (c < 0) return c;
-            r |= c;
         }
-        return r;
+        return 0;
     };
     for (int i = 0; i < n; ++i) {
         if (d.materials[i].kind != LUM_MAT_BLEND) continue;
-        int r = depth(i, 1);
+        std::vector<lum::BlendEmit> leaves;
+        int r = walk(i, 1, 1.0, leaves);
         if (r == -2) return fail(LUM_ERR_INVALID_ARGUMENT, "material %d: blend child index out of range", i);
         if (r < 0) return fail(LUM_ERR_UNSUPPORTED, "material %d: blends nest more than %d deep", i, lum::kMaxBlendDepth);
-        mats[i].emits = r;
+        mats[i].n_emit = (int32_t)leaves.size();
+        mats[i].emit_first = (int32_t)table.size();
+        table.insert(table.end(), leaves.begin(), leaves.end());
     }
     return LUM_OK;
 }
@@ -580,6 +587,7 @@ lum_status make_render_dev(const lum_scene* s, const lum_render_params& p, lum::
     }
     R.bg_intensity = (float)p.bg_intensity;
     R.exposure = (float)p.exposure;
+    R.ext = (s->max_mat_kind > LUM_MAT_ISOTROPIC || p.background >= LUM_BG_STARFIELD) ? 1u : 0u;
     R.star_density = (float)p.bg_star_density;
     R.star_brightness = (float)p.bg_star_brightness;
     if (p.background == LUM_BG_ENVMAP && !s->dev.env)
@@ -714,7 +722,8 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
     }
     std::vector<lum::MatDev> mats(desc->n_materials);
     for (uint32_t i = 0; i < desc->n_materials; ++i) mats[i] = make_mat(desc->materials[i]);
-    st = check_blends(*desc, mats);
+    std::vector<lum::BlendEmit> blend_emit;
+    st = check_blends(*desc, mats, blend_emit);
     if (st != LUM_OK) return st;
     std::vector<lum::LightDev> lights(desc->n_lights);
     for (uint32_t i = 0; i < desc->n_lights; ++i) {
@@ -754,7 +763,8 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
     size_t off_mats = align256(off_smooth + F.smooth.size() * 4);
     size_t off_lights = align256(off_mats + mats.size() * sizeof(lum::MatDev));
     size_t off_planes = align256(off_lights + lights.size() * sizeof(lum::LightDev));
-    size_t total = align256(off_planes + F.planes.size() * sizeof(lum::PlaneDev)) + 256;
+    size_t off_blend = align256(off_planes + F.planes.size() * sizeof(lum::PlaneDev));
+    size_t total = align256(off_blend + blend_emit.size() * sizeof(lum::BlendEmit)) + 256;
     if ((ce = cudaMalloc(&s->d_buf, total)) != cudaSuccess) return cleanup(cuda_fail(ce, "cudaMalloc scene"));
     s->d_bytes = total;
     if ((ce = cudaMalloc((void**)&s->d_work, sizeof(lum::WorkCounters))) != cudaSuccess)
@@ -771,7 +781,8 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
         (ce = up(off_smooth, F.smooth.data(), F.smooth.size() * 4)) != cudaSuccess ||
         (ce = up(off_mats, mats.data(), mats.size() * sizeof(lum::MatDev))) != cudaSuccess ||
         (ce = up(off_lights, lights.data(), lights.size() * sizeof(lum::LightDev))) != cudaSuccess ||
-        (ce = up(off_planes, F.planes.data(), F.planes.size() * sizeof(lum::PlaneDev))) != cudaSuccess)
+        (ce = up(off_planes, F.planes.data(), F.planes.size() * sizeof(lum::PlaneDev))) != cudaSuccess ||
+        (ce = up(off_blend, blend_emit.data(), blend_emit.size() * sizeof(lum::BlendEmit))) != cudaSuccess)
         return cleanup(cuda_fail(ce, "cudaMemcpy scene"));
 
     lum::SceneDev& D = s->dev;
@@ -783,6 +794,7 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
     D.mats = (const lum::MatDev*)(base + off_mats);
     D.lights = (const lum::LightDev*)(base + off_lights);
     D.planes = (const lum::PlaneDev*)(base + off_planes);
+    D.blend_emit = (const lum::BlendEmit*)(base + off_blend);
     D.n_nodes = (int32_t)bvh.nodes.size();
     D.n_prims = (int32_t)np;
     D.n_lights = (int32_t)lights.size();

@@ -51,13 +51,14 @@ __device__ __forceinline__ void flush_counters(WorkCounters* wc, uint32_t err, u
 // then writes its pixels; a grouped one adds its sums to the frame's fixed-point accumulators,
 // which k_fixed_finalize turns into pixels.  Integer sums make the image deterministic and the
 // same whether or not the frame was grouped.
-template <bool COUNT>
+template <bool COUNT, bool EXT>
 __global__ void __launch_bounds__(kRenderThreads, LUM_RENDER_MIN_BLOCKS) k_render(SceneDev S, RenderDev R, float* __restrict__ out,
                                                            WorkCounters* wc, unsigned long long* __restrict__ gacc,
                                                            uint32_t n_groups, uint32_t group_strata) {
     extern __shared__ int s_stack[];
     __shared__ unsigned long long s_acc[kRenderThreads / 32][32][4];
     __shared__ uint32_t s_next[kRenderThreads / 32];
+    __shared__ V s_exit[kRenderThreads / 32][32];      // deferred Subsurface origins (EXT only)
     int* stack = s_stack + threadIdx.x;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     uint32_t err = 0, nseg = 0, nsh = 0;
@@ -72,7 +73,8 @@ __global__ void __launch_bounds__(kRenderThreads, LUM_RENDER_MIN_BLOCKS) k_rende
         const uint32_t tw = min(8u, R.w - x0), th = min(4u, R.h - y0);
         const uint32_t s_lo = R.s_begin + group * group_strata;
         const uint32_t s_hi = min(R.s_end, s_lo + group_strata);
-        tile_task<COUNT>(S, R, x0, y0, tw, th, s_lo, s_hi, s_acc[wid], &s_next[wid], stack, err, nseg, nsh, &tally);
+        tile_task<COUNT, EXT>(S, R, x0, y0, tw, th, s_lo, s_hi, s_acc[wid], &s_next[wid], s_exit[wid], stack, err,
+                              nseg, nsh, &tally);
         if (lane < (int)(tw * th)) {
             const uint32_t i = x0 + lane % tw, j = y0 + lane / tw;
             const unsigned long long* a = s_acc[wid][lane];
@@ -209,11 +211,9 @@ static size_t stack_bytes(int threads) { return (size_t)kStackDepth * threads * 
 static int render_occupancy() {
     static int occ = -1;
     if (occ < 0) {
-        cudaFuncSetAttribute(k_render<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)stack_bytes(kRenderThreads));
-        cudaFuncSetAttribute(k_render<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)stack_bytes(kRenderThreads));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_render<false>, kRenderThreads,
+        for (auto fn : {k_render<false, false>, k_render<false, true>, k_render<true, false>, k_render<true, true>})
+            cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stack_bytes(kRenderThreads));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_render<false, false>, kRenderThreads,
                                                       stack_bytes(kRenderThreads));
         if (occ <= 0) occ = 4;
     }
@@ -253,8 +253,10 @@ static cudaError_t launch_render_t(const SceneDev& S, const RenderDev& R, float*
     const uint64_t tasks = (uint64_t)R.n_tasks * grp.n_groups;
     int blocks_needed = (int)((tasks + 3) / 4);   // 4 warps per block, one task per warp at least
     if (grid > blocks_needed) grid = blocks_needed > 0 ? blocks_needed : 1;
-    k_render<COUNT><<<grid, kRenderThreads, stack_bytes(kRenderThreads), stream>>>(S, R, out, wc, gacc,
-                                                                                   grp.n_groups, grp.group_strata);
+    // scenes without the other materials and backgrounds run the kernel built without them
+    auto kernel = R.ext ? k_render<COUNT, true> : k_render<COUNT, false>;
+    kernel<<<grid, kRenderThreads, stack_bytes(kRenderThreads), stream>>>(S, R, out, wc, gacc, grp.n_groups,
+                                                                          grp.group_strata);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || grp.n_groups <= 1) return e;
     const int cgrid = (int)std::min<size_t>((n_px + 255) / 256, (size_t)num_sms() * 8);

@@ -34,11 +34,12 @@ __device__ __forceinline__ void fixed_pixel(const unsigned long long* a, float e
 
 // Runs the task; on return acc[k][0..3] (k < tw * th, pixel (k % tw, k / tw) of the tile) hold
 // the sums.  acc (32 x 4) and *next are the warp's shared memory; the call zeroes them.
-template <bool COUNT>
+// EXT: the scene may use the other materials or backgrounds (shade's EXT).
+template <bool COUNT, bool EXT = true>
 __device__ __forceinline__ void tile_task(const SceneDev& S, const RenderDev& R, uint32_t x0, uint32_t y0,
                                           uint32_t tw, uint32_t th, uint32_t s_lo, uint32_t s_hi,
-                                          unsigned long long (*acc)[4], uint32_t* next, int* stack, uint32_t& err,
-                                          uint32_t& nseg, uint32_t& nsh, TestTally* tally) {
+                                          unsigned long long (*acc)[4], uint32_t* next, V* exit_stash, int* stack,
+                                          uint32_t& err, uint32_t& nseg, uint32_t& nsh, TestTally* tally) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     acc[lane][0] = acc[lane][1] = acc[lane][2] = acc[lane][3] = 0ull;
@@ -70,17 +71,18 @@ __device__ __forceinline__ void tile_task(const SceneDev& S, const RenderDev& R,
             r.d = shadow ? pend.dir : P.ray.d;
             r.time = shadow ? 0.0f : P.ray.time;                  // Ray::new (render.rs:1457)
             Hit h;
-            h.t = shadow ? pend.tmax : CUDART_INF_F;
+            h.t = shadow ? (EXT ? fabsf(pend.tmax) : pend.tmax) : CUDART_INF_F;
             h.prim = -1;
             h.b1 = h.b2 = 0.0f;
             const bool found = trace<COUNT>(S, r, 0.001f, shadow, h, stack, err, tally);
             if (shadow) {
                 ++nsh;
                 if (!found) P.L = P.L + pend.contrib;
+                shadow_done<EXT>(P, pend, exit_stash + lane);
                 state = P.bounce >= R.max_depth ? ST_DONE : ST_CLOSEST;
             } else {
                 ++nseg;
-                state = shade(S, R, pixel, P, found, h, pend);
+                state = shade<-1, EXT>(S, R, pixel, P, found, h, pend, exit_stash + lane);
             }
         }
         if (state == ST_DONE) {

@@ -49,8 +49,8 @@ __device__ __forceinline__ V clamp_sample(V L) {
 // the traversal and shading code serves every kind of tile.
 __device__ __forceinline__ void sample_pool(const SceneDev& S, const RenderDev& R, uint32_t x0, uint32_t y0, uint32_t tw,
                             const uint32_t* slot_px, uint32_t n_slots, uint32_t st_lo, uint32_t n_st, bool centre,
-                            unsigned long long (*acc)[4], float (*smp)[32][3], uint32_t* next, int* stack,
-                            uint32_t& err, uint32_t& nseg, uint32_t& nsh) {
+                            unsigned long long (*acc)[4], float (*smp)[32][3], uint32_t* next, V* exit_stash,
+                            int* stack, uint32_t& err, uint32_t& nseg, uint32_t& nsh) {
     const int lane = threadIdx.x & 31;
     if (acc) acc[lane][0] = acc[lane][1] = acc[lane][2] = acc[lane][3] = 0ull;
     if (lane == 0) *next = 0u;
@@ -83,17 +83,18 @@ __device__ __forceinline__ void sample_pool(const SceneDev& S, const RenderDev& 
             r.d = shadow ? pend.dir : P.ray.d;
             r.time = shadow ? 0.0f : P.ray.time;                  // Ray::new (render.rs:1457)
             Hit h;
-            h.t = shadow ? pend.tmax : CUDART_INF_F;
+            h.t = shadow ? fabsf(pend.tmax) : CUDART_INF_F;
             h.prim = -1;
             h.b1 = h.b2 = 0.0f;
             const bool found = trace<false>(S, r, 0.001f, shadow, h, stack, err);
             if (shadow) {
                 ++nsh;
                 if (!found) P.L = P.L + pend.contrib;
+                shadow_done<true>(P, pend, exit_stash + lane);
                 state = P.bounce >= R.max_depth ? ST_DONE : ST_CLOSEST;
             } else {
                 ++nseg;
-                state = shade(S, R, pixel, P, found, h, pend);
+                state = shade(S, R, pixel, P, found, h, pend, exit_stash + lane);
             }
         }
         if (state == ST_DONE) {
@@ -125,6 +126,7 @@ __global__ void __launch_bounds__(kSampThreads, ADAPTIVE ? 4 : 5) k_render_sampl
     __shared__ float s_smp[kSampWarps][ADAPTIVE ? kRoundStrata : 1][32][3];
     __shared__ uint32_t s_slot[kSampWarps][32];
     __shared__ uint32_t s_next[kSampWarps];
+    __shared__ V s_exit[kSampWarps][32];            // deferred Subsurface origins
     int* stack = s_stack + threadIdx.x;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     uint32_t err = 0, nseg = 0, nsh = 0;
@@ -157,7 +159,8 @@ __global__ void __launch_bounds__(kSampThreads, ADAPTIVE ? 4 : 5) k_render_sampl
             const uint32_t st_lo = expired ? 0u : ADAPTIVE ? lo : R.s_begin;
             const uint32_t n_st = expired ? 1u : ADAPTIVE ? min(kRoundStrata, total - lo) : R.s_end - R.s_begin;
             sample_pool(S, R, x0, y0, tw, s_slot[wid], __popc(act), st_lo, n_st, expired != 0,
-                        fixed_sums ? s_acc[wid] : nullptr, s_smp[wid], &s_next[wid], stack, err, nseg, nsh);
+                        fixed_sums ? s_acc[wid] : nullptr, s_smp[wid], &s_next[wid], s_exit[wid], stack, err, nseg,
+                        nsh);
             if (active) {
                 if (expired) {
                     for (int c = 0; c < 3; ++c) o[c] = s_smp[wid][0][lane][c] * R.exposure;

@@ -486,35 +486,33 @@ enum : int { MAT_BLEND = 7 };
 
 // Blend::scatter's choice (material.rs:408-415): one draw per level, mat_a with probability
 // ratio, down to a material that is not a Blend.
-__device__ __noinline__ inline const MatDev& blend_walk(const SceneDev& S, const MatDev& m0, const RenderDev& R,
-                                                        uint32_t pixel, uint32_t stratum, uint32_t bounce) {
-    const MatDev* m = &m0;
-    const float4 u = draw4(R.key0, R.key1, pixel, stratum, bounce, CALL_BLEND);
+__device__ __forceinline__ const MatDev* blend_walk(const MatDev* mats, const MatDev* m, uint32_t key0,
+                                                        uint32_t key1, uint32_t pixel, uint32_t stratum,
+                                                        uint32_t bounce) {
+    const float4 u = draw4(key0, key1, pixel, stratum, bounce, CALL_BLEND);
     const float uu[4] = {u.x, u.y, u.z, u.w};
 #pragma unroll
     for (int l = 0; l < kMaxBlendDepth; ++l) {
         if (m->kind != MAT_BLEND) break;
-        m = &S.mats[uu[l] < m->extra[0] ? m->sub[0] : m->sub[1]];
+        m = &mats[uu[l] < m->extra[0] ? m->sub[0] : m->sub[1]];
     }
-    return *m;
+    return m;
 }
 __device__ __forceinline__ const MatDev& blend_leaf(const SceneDev& S, const MatDev& m, const RenderDev& R,
                                                     uint32_t pixel, uint32_t stratum, uint32_t bounce) {
-    return m.kind == MAT_BLEND ? blend_walk(S, m, R, pixel, stratum, bounce) : m;
+    return m.kind == MAT_BLEND ? *blend_walk(S.mats, &m, R.key0, R.key1, pixel, stratum, bounce) : m;
 }
 
-// Blend::emitted (material.rs:417-420): ratio * emitted(a) + (1 - ratio) * emitted(b).
-template <int D>
-__device__ __noinline__ V blend_emitted(const SceneDev& S, int idx, V p) {
-    const MatDev& m = S.mats[idx];
-    if (m.kind != MAT_BLEND) return emitted(m, p);
-    if constexpr (D > 0)
-        return blend_emitted<D - 1>(S, m.sub[0], p) * m.extra[0] + blend_emitted<D - 1>(S, m.sub[1], p) * (1.0f - m.extra[0]);
-    return mk(0.f, 0.f, 0.f);
-}
+// Blend::emitted (material.rs:417-420): ratio * emitted(a) + (1 - ratio) * emitted(b),
+// evaluated from the blend's flattened list of emissive leaves (no recursion, no call).
 __device__ __forceinline__ V emitted_at(const SceneDev& S, int idx, const MatDev& m, V p) {
-    if (m.kind == MAT_BLEND) return m.emits ? blend_emitted<kMaxBlendDepth>(S, idx, p) : mk(0.f, 0.f, 0.f);
-    return emitted(m, p);
+    if (m.kind != MAT_BLEND) return emitted(m, p);
+    V e = mk(0.f, 0.f, 0.f);
+    for (int k = 0; k < m.n_emit; ++k) {
+        const BlendEmit be = S.blend_emit[m.emit_first + k];
+        e = e + emitted(S.mats[be.leaf], p) * be.weight;
+    }
+    return e;
 }
 
 // Iridescent::thin_film_color (material.rs:469-491): sin^2(phase / 2) at 650 / 532 / 450 nm
@@ -528,17 +526,31 @@ __device__ __forceinline__ V thin_film(float cos_t, float thickness, float film_
     return mk(r * r, g * g, b * b);
 }
 
-// The other materials' scatter (material.rs:408-865), out of line: the megakernel's register
-// allocation stays that of the common materials.  Keyed draws: CALL_SCATTER slots as noted,
-// Subsurface's exit direction from CALL_EXTRA.
-__device__ __noinline__ inline bool scatter_more(const MatDev& m, const Ray& ray, const Surface& sf, float4 s,
-                                                 const RenderDev& R, uint32_t pixel, uint32_t stratum,
-                                                 uint32_t bounce, Scatter& out) {
+// The other materials' scatter (material.rs:408-865).  Keyed draws: CALL_SCATTER slots as
+// noted, Subsurface's exit direction from CALL_EXTRA.  Inlined like everything the megakernel
+// calls: a device-function call makes every value live across it a spill candidate.
+struct ScatterMore {
+    V dir, att, org;
+    bool ok;
+};
+__device__ __forceinline__ ScatterMore scatter_more(const MatDev* mp, V rd, V hp, V hn, float4 s, uint32_t key0,
+                                                       uint32_t key1, uint32_t pixel, uint32_t stratum,
+                                                       uint32_t bounce) {
+    const MatDev& m = *mp;
+    ScatterMore out;
+    out.org = hp;
+    out.ok = true;
+    struct {
+        V p, n;
+    } sf{hp, hn};
+    struct {
+        V d;
+    } ray{rd};
     switch (m.kind) {
         case 8: {                                                      // Transparent, material.rs:429-435
             out.dir = ray.d;
             out.att = mk(1.f, 1.f, 1.f);
-            return true;
+            return out;
         }
         case 9: {                                                      // Iridescent, material.rs:499-527
             V ud = unit(ray.d);
@@ -547,10 +559,10 @@ __device__ __noinline__ inline bool scatter_more(const MatDev& m, const Ray& ray
             V d = reflect(ud, sf.n);
             if (m.roughness > 0.0f) {
                 d = d + in_unit_sphere(s.x, s.y, s.z) * m.roughness;
-                if (dot(d, sf.n) <= 0.0f) return false;
+                if (dot(d, sf.n) <= 0.0f) { out.ok = false; return out; }
             }
             out.dir = d;
-            return true;
+            return out;
         }
         case 10: {                                                     // Toon, material.rs:549-577
             V d = sf.n + unit_vector(s.x, s.y);
@@ -562,7 +574,7 @@ __device__ __noinline__ inline bool scatter_more(const MatDev& m, const Ray& ray
             float spec = powf(fmaxf(dot(hv, sf.n), 0.0f), m.extra[1] * 100.0f);
             out.dir = d;
             out.att = mk(m.color) * (band + (spec > 0.5f ? 0.3f : 0.0f));
-            return true;
+            return out;
         }
         case 11: {                                                     // Anisotropic, material.rs:607-641
             V refl = reflect(unit(ray.d), sf.n);
@@ -574,10 +586,10 @@ __device__ __noinline__ inline bool scatter_more(const MatDev& m, const Ray& ray
             sincospif(2.0f * s.x, &sp, &cp);
             float r2 = sqrtf(s.y);
             V sc = unit(refl + t * (cp * r2 * m.extra[0]) + b * (sp * r2 * m.extra[1]));
-            if (!(dot(sc, sf.n) > 0.0f)) return false;
+            if (!(dot(sc, sf.n) > 0.0f)) { out.ok = false; return out; }
             out.dir = sc;
             out.att = mk(m.color);
-            return true;
+            return out;
         }
         case 12: {                                                     // Clearcoat, material.rs:664-707
             V ud = unit(ray.d);
@@ -596,13 +608,13 @@ __device__ __noinline__ inline bool scatter_more(const MatDev& m, const Ray& ray
                 }
                 out.dir = d;
                 out.att = mk(1.f, 1.f, 1.f);
-                return true;
+                return out;
             }
             V d = sf.n + unit_vector(s.y, s.z);
             if (near_zero(d)) d = sf.n;
             out.dir = d;
             out.att = mk(m.color);
-            return true;
+            return out;
         }
         case 13: {                                                     // Velvet, material.rs:724-746
             V d = sf.n + unit_vector(s.x, s.y);
@@ -611,7 +623,7 @@ __device__ __noinline__ inline bool scatter_more(const MatDev& m, const Ray& ray
             float st = sqrtf(fmaxf(1.0f - ct * ct, 0.0f));
             out.dir = d;
             out.att = mk(m.color) * (1.0f + st * sqrtf(st) * m.extra[0]);
-            return true;
+            return out;
         }
         case 14: {                                                     // Translucent, material.rs:769-797
             V d;
@@ -625,7 +637,7 @@ __device__ __noinline__ inline bool scatter_more(const MatDev& m, const Ray& ray
             }
             out.dir = d;
             out.att = mk(m.color);
-            return true;
+            return out;
         }
         case 15: {                                                     // Subsurface, material.rs:823-864
             float fr = schlick(fabsf(dot(unit(ray.d), sf.n)), 1.0f / 1.4f);
@@ -634,28 +646,30 @@ __device__ __noinline__ inline bool scatter_more(const MatDev& m, const Ray& ray
                 if (near_zero(d)) d = sf.n;
                 out.dir = d;
                 out.att = mk(m.color);
-                return true;
+                return out;
             }
             const float mfp = m.extra[0];
             float step = -mfp * logf(fmaxf(s.y, 1e-10f));
             out.org = sf.p + unit_vector(s.z, s.w) * step;
-            float4 ex = draw4(R.key0, R.key1, pixel, stratum, bounce, CALL_EXTRA);
+            float4 ex = draw4(key0, key1, pixel, stratum, bounce, CALL_EXTRA);
             V d = sf.n + unit_vector(ex.x, ex.y);
             out.dir = near_zero(d) ? sf.n : unit(d);
             const float k = -step / mfp;
             out.att = mul(mk(m.color), mk(__expf(k * (1.0f - m.color2[0])), __expf(k * (1.0f - m.color2[1])),
                                           __expf(k * (1.0f - m.color2[2]))));
-            return true;
+            return out;
         }
         default:
-            return false;
+            { out.ok = false; return out; }
     }
 }
 
 // Material::scatter; draws s = (s0..s3) of CALL_SCATTER, extra for dispersion.
 // KIND >= 0 fixes the material kind at compile time (the material-sorted shading kernels of
 // the wavefront tracer); KIND = -1 dispatches on m.kind.  Both run the same arithmetic.
-template <int KIND = -1>
+// EXT = false leaves out the other materials (material.rs:396-865): kernels for scenes
+// without them carry none of their code (the megakernel is sensitive to its code size).
+template <int KIND = -1, bool EXT = true>
 __device__ __forceinline__ bool scatter(const MatDev& m, const Ray& ray, const Surface& sf, float hit_t, float4 s,
                                         const RenderDev& R, uint32_t pixel, uint32_t stratum, uint32_t bounce,
                                         Scatter& out) {
@@ -745,8 +759,16 @@ __device__ __forceinline__ bool scatter(const MatDev& m, const Ray& ray, const S
             out.att = mk(m.color);
             return true;
         }
-        case 8: case 9: case 10: case 11: case 12: case 13: case 14: case 15:
-            return scatter_more(m, ray, sf, s, R, pixel, stratum, bounce, out);
+        case 8: case 9: case 10: case 11: case 12: case 13: case 14: case 15: {
+            if constexpr (EXT) {
+                const ScatterMore r = scatter_more(&m, ray.d, sf.p, sf.n, s, R.key0, R.key1, pixel, stratum, bounce);
+                out.dir = r.dir;
+                out.att = r.att;
+                out.org = r.org;
+                return r.ok;
+            }
+            return false;
+        }
         default:                                                       // Emissive: no scatter
             return false;
     }
@@ -839,9 +861,9 @@ __device__ __forceinline__ bool sample_light(const SceneDev& S, V hp, V normal, 
 
 // Background::Starfield (render.rs:86-112): dark blue space plus stars hashed from the
 // direction quantised at 500 * density cells per unit.
-__device__ __noinline__ inline V starfield(const RenderDev& R, V ud, float t) {
+__device__ __forceinline__ V starfield(float density, float brightness, V ud, float t) {
     V space = mk(0.0f, 0.0f, 0.02f) * (1.0f - t) + mk(0.02f, 0.0f, 0.05f) * t;
-    const float scale = 500.0f * R.star_density;
+    const float scale = 500.0f * density;
     const long long ix = (long long)floorf(ud.x * scale), iy = (long long)floorf(ud.y * scale),
                     iz = (long long)floorf(ud.z * scale);
     const unsigned long long hash = ((unsigned long long)ix * 73856093ull) ^ ((unsigned long long)iy * 19349663ull) ^
@@ -850,29 +872,30 @@ __device__ __noinline__ inline V starfield(const RenderDev& R, V ud, float t) {
     if (!(star > 0.997f)) return space;
     const float rh = (float)((hash >> 8) % 100ull) / 100.0f;
     const V c = rh < 0.3f ? mk(1.0f, 0.9f, 0.8f) : (rh < 0.6f ? mk(0.9f, 0.9f, 1.0f) : mk(1.f, 1.f, 1.f));
-    return space + c * (star * R.star_brightness);
+    return space + c * (star * brightness);
 }
 
 // Background::EnvMap (render.rs:113-151): equirectangular lookup, bilinear, times intensity.
-__device__ __noinline__ inline V envmap(const SceneDev& S, const RenderDev& R, V ud) {
-    if (!S.env) return mk(0.f, 0.f, 0.f);
+__device__ __forceinline__ V envmap(const float* env, uint32_t env_w, uint32_t env_h, float intensity, V ud) {
+    if (!env) return mk(0.f, 0.f, 0.f);
     const float theta = acosf(-ud.y);
     const float phi = atan2f(-ud.z, ud.x) + CUDART_PI_F;
-    const float fx = phi * (0.5f / CUDART_PI_F) * (float)S.env_w - 0.5f;
-    const float fy = theta * (1.0f / CUDART_PI_F) * (float)S.env_h - 0.5f;
+    const float fx = phi * (0.5f / CUDART_PI_F) * (float)env_w - 0.5f;
+    const float fy = theta * (1.0f / CUDART_PI_F) * (float)env_h - 0.5f;
     const float flx = floorf(fx), fly = floorf(fy);
-    const int w = (int)S.env_w, h = (int)S.env_h;
+    const int w = (int)env_w, h = (int)env_h;
     int x0 = (int)flx % w;
     if (x0 < 0) x0 += w;
     const int y0 = (int)fminf(fmaxf(fly, 0.0f), (float)(h - 1));
     const int x1 = (x0 + 1) % w, y1 = min(y0 + 1, h - 1);
     const float tx = fx - flx, ty = fy - fly;
-    auto px = [&](int x, int y) { return mk(S.env + 3 * ((size_t)y * w + x)); };
+    auto px = [&](int x, int y) { return mk(env + 3 * ((size_t)y * w + x)); };
     const V c = px(x0, y0) * ((1.0f - tx) * (1.0f - ty)) + px(x1, y0) * (tx * (1.0f - ty)) +
                 px(x0, y1) * ((1.0f - tx) * ty) + px(x1, y1) * (tx * ty);
-    return c * R.bg_intensity;
+    return c * intensity;
 }
 
+template <bool EXT = true>
 __device__ __forceinline__ V background(const SceneDev& S, const RenderDev& R, const Ray& r) {  // render.rs:73-171
     if (R.background == 1) return mk(R.bg_color);
     V ud = unit(r.d);
@@ -888,8 +911,10 @@ __device__ __forceinline__ V background(const SceneDev& S, const RenderDev& R, c
         }
         return sky;
     }
-    if (R.background == 4) return starfield(R, ud, t);
-    if (R.background == 5) return envmap(S, R, ud);
+    if constexpr (EXT) {
+        if (R.background == 4) return starfield(R.star_density, R.star_brightness, ud, t);
+        if (R.background == 5) return envmap(S.env, S.env_w, S.env_h, R.bg_intensity, ud);
+    }
     return mk(1.f, 1.f, 1.f) * (1.0f - t) + mk(0.5f, 0.7f, 1.0f) * t;
 }
 
@@ -993,20 +1018,36 @@ enum : int { ST_IDLE = 0, ST_CLOSEST = 1, ST_SHADOW = 2, ST_DONE = 3 };
 
 // NEE shadow query pending after a bounce: direction from the new hit point, its t range
 // end, and the contribution B_j * (E albedo cos cos' A N / (pi d^2)) added if unoccluded.
+// The shadow ray starts at the path's origin (P.ray.o), the hit point.  When Subsurface moves
+// the next segment's origin to its exit point while a shadow query is pending, shade keeps the
+// hit point in P.ray.o, writes the exit point to the caller's stash and negates tmax; the
+// caller traces the shadow to |tmax| and then moves P.ray.o to the stashed point
+// (shadow_done).
 struct Pending {
     V dir;
     float tmax;
     V contrib;
 };
 
+// After a shadow query: the deferred Subsurface origin move, if any.
+template <bool EXT>
+__device__ __forceinline__ void shadow_done(Path& P, Pending& pend, const V* exit_stash) {
+    if constexpr (EXT) {
+        if (pend.tmax < 0.0f) {
+            P.ray.o = *exit_stash;
+            pend.tmax = -pend.tmax;
+        }
+    }
+}
+
 // Shading after the closest hit of segment j (ray_color, render.rs:1472-1537, iterative):
 // L += B_j e_j now, B_{j+1} = B_j att_j rrw_j, the NEE term B_j d_j once its shadow ray is
 // known to be unoccluded.  Returns the lane's next state.
-template <int KIND = -1>
+template <int KIND = -1, bool EXT = true>
 __device__ __forceinline__ int shade(const SceneDev& S, const RenderDev& R, uint32_t pixel, Path& P, bool found,
-                                     const Hit& h, Pending& pend) {
+                                     const Hit& h, Pending& pend, V* exit_stash = nullptr) {
     if (!found) {
-        P.L = P.L + mul(P.beta, background(S, R, P.ray));
+        P.L = P.L + mul(P.beta, background<EXT>(S, R, P.ray));
         return ST_DONE;
     }
     const uint32_t depth = R.max_depth - P.bounce;
@@ -1018,12 +1059,13 @@ __device__ __forceinline__ int shade(const SceneDev& S, const RenderDev& R, uint
     // (whose slab tests pass every box) out of the traversal.
     if (!isfinite(sf.p.x) || !isfinite(sf.p.y) || !isfinite(sf.p.z)) return ST_DONE;
     const MatDev& m = S.mats[sf.mat];
-    V e = P.skip_emission ? mk(0.f, 0.f, 0.f) : (KIND < 0 ? emitted_at(S, sf.mat, m, sf.p) : emitted(m, sf.p));
+    V e = P.skip_emission ? mk(0.f, 0.f, 0.f)
+                          : (EXT && KIND < 0 ? emitted_at(S, sf.mat, m, sf.p) : emitted(m, sf.p));
     float4 su = draw4(R.key0, R.key1, pixel, P.stratum, P.bounce, CALL_SCATTER);
     Scatter sc;
     sc.org = sf.p;
-    const MatDev& ms = KIND < 0 ? blend_leaf(S, m, R, pixel, P.stratum, P.bounce) : m;
-    if (!scatter<KIND>(ms, P.ray, sf, h.t, su, R, pixel, P.stratum, P.bounce, sc)) {
+    const MatDev& ms = EXT && KIND < 0 ? blend_leaf(S, m, R, pixel, P.stratum, P.bounce) : m;
+    if (!scatter<KIND, EXT>(ms, P.ray, sf, h.t, su, R, pixel, P.stratum, P.bounce, sc)) {
         P.L = P.L + mul(P.beta, e);
         return ST_DONE;
     }
@@ -1034,6 +1076,10 @@ __device__ __forceinline__ int shade(const SceneDev& S, const RenderDev& R, uint
         P.L = P.L + mul(P.beta, e);
         return ST_DONE;
     }
+    // the next segment (its origin and direction are dead past this point otherwise; a path
+    // that ends below no longer reads its ray)
+    P.ray.o = sc.org;
+    P.ray.d = sc.dir;
     float4 nu = draw4(R.key0, R.key1, pixel, P.stratum, P.bounce, CALL_NEE);
     float surv = fminf(fmaxf(fmaxf(fmaxf(sc.att.x, sc.att.y), sc.att.z), 0.05f), 1.0f);
     if (depth < 47 && nu.x > surv) {                                   // Russian roulette
@@ -1057,9 +1103,14 @@ __device__ __forceinline__ int shade(const SceneDev& S, const RenderDev& R, uint
     }
     P.beta = nb;
     P.skip_emission = use_nee;
-    P.ray.o = sc.org;
-    P.ray.d = sc.dir;
     ++P.bounce;
+    if constexpr (EXT) {
+        if (shadow && (P.ray.o.x != sf.p.x || P.ray.o.y != sf.p.y || P.ray.o.z != sf.p.z)) {
+            *exit_stash = P.ray.o;                     // Subsurface: the shadow starts at the hit point
+            P.ray.o = sf.p;
+            pend.tmax = -pend.tmax;
+        }
+    }
     if (shadow) return ST_SHADOW;
     return P.bounce >= R.max_depth ? ST_DONE : ST_CLOSEST;             // depth == 0 -> black
 }

@@ -65,7 +65,8 @@ struct Pool {
     uint4* ids;       // scene, RNG pixel key, output pixel, stratum | bounce << 24 | skip << 31
     float4* hit;      // t, prim (bits), b1, b2
     float4* sdir;     // shadow direction, t max
-    float4* scon;     // shadow contribution, finish-after-shadow flag
+    float4* scon;     // shadow contribution, flags (1: finish after the shadow, 2: origin in sorg)
+    float4* sorg;     // shadow origin when it is not the path's origin (Subsurface exit points)
     uint32_t* ext[2];
     uint32_t* freeq;
     uint32_t* shadowq;
@@ -246,12 +247,18 @@ __global__ void k_shade(Pool pl, Tables T, Ctl* ctl) {
         const RenderDev R = T.renders[id.x];
         int st;
         Pending pend;
+        V exit;                                                        // deferred Subsurface origin
         if (P.bounce >= R.max_depth) {
             st = ST_DONE;                                              // depth == 0 -> black
         } else {
             const SceneDev S = T.scenes[id.x];
-            st = shade<Q == 0 ? -1 : Q>(S, R, id.y, P, h.prim != -1, h, pend);
+            st = shade<Q == 0 ? -1 : Q>(S, R, id.y, P, h.prim != -1, h, pend, &exit);
         }
+        // a deferred Subsurface origin: the pool keeps the next segment's origin, the shadow
+        // query its own (sorg)
+        const bool moved = st == ST_SHADOW && pend.tmax < 0.0f;
+        const V shadow_org = P.ray.o;
+        if (moved) P.ray.o = exit;
         store_path(pl, slot, P, id.x, id.y, id.z);
         if (st == ST_DONE) {
             finish(T, ctl, R, id.x, id.z, P);
@@ -259,8 +266,10 @@ __global__ void k_shade(Pool pl, Tables T, Ctl* ctl) {
         } else {
             bool cont = st == ST_CLOSEST || P.bounce < R.max_depth;
             if (st == ST_SHADOW) {
-                pl.sdir[slot] = make_float4(pend.dir.x, pend.dir.y, pend.dir.z, pend.tmax);
-                pl.scon[slot] = make_float4(pend.contrib.x, pend.contrib.y, pend.contrib.z, cont ? 0.0f : 1.0f);
+                if (moved) pl.sorg[slot] = make_float4(shadow_org.x, shadow_org.y, shadow_org.z, 0.0f);
+                pl.sdir[slot] = make_float4(pend.dir.x, pend.dir.y, pend.dir.z, fabsf(pend.tmax));
+                pl.scon[slot] = make_float4(pend.contrib.x, pend.contrib.y, pend.contrib.z,
+                                            (cont ? 0.0f : 1.0f) + (moved ? 2.0f : 0.0f));
                 append(pl.shadowq, &ctl->shadow_n, slot, __activemask());
             }
             if (cont) append(pl.ext[nxt], &ctl->ext_n[nxt], slot, __activemask());
@@ -277,7 +286,9 @@ __global__ void k_shadow(Pool pl, Tables T, Ctl* ctl) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const uint32_t slot = pl.shadowq[i];
         const uint4 id = pl.ids[slot];
-        const float4 o = pl.o_t[slot], sd = pl.sdir[slot], sc = pl.scon[slot];
+        const float4 sd = pl.sdir[slot], sc = pl.scon[slot];
+        const int flags = (int)sc.w;
+        const float4 o = (flags & 2) ? pl.sorg[slot] : pl.o_t[slot];
         Ray r{xyz(o), xyz(sd), 0.0f};                                 // Ray::new (render.rs:1457)
         Hit h;
         h.t = sd.w;
@@ -292,7 +303,7 @@ __global__ void k_shadow(Pool pl, Tables T, Ctl* ctl) {
             l.z += sc.z;
             pl.L[slot] = l;
         }
-        if (sc.w != 0.0f) {
+        if (flags & 1) {
             Path P;
             uint4 id2;
             load_path(pl, slot, P, id2);
@@ -356,6 +367,7 @@ __global__ void __launch_bounds__(128, 5) k_render_multi(Tables T, const unsigne
     extern __shared__ int s_stack[];
     __shared__ unsigned long long s_acc[4][32][4];
     __shared__ uint32_t s_next[4];
+    __shared__ V s_exit[4][32];                  // deferred Subsurface origins
     int* stack = s_stack + threadIdx.x;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const unsigned long long total = task_prefix[T.n];
@@ -380,7 +392,8 @@ __global__ void __launch_bounds__(128, 5) k_render_multi(Tables T, const unsigne
         const uint32_t tw = min(8u, R.w - x0), th = min(4u, R.h - y0);
         const uint32_t s_lo = R.s_begin + group * grp.y;
         const uint32_t s_hi = min(R.s_end, s_lo + grp.y);
-        tile_task<false>(S, R, x0, y0, tw, th, s_lo, s_hi, s_acc[wid], &s_next[wid], stack, err, nseg, nsh, nullptr);
+        tile_task<false>(S, R, x0, y0, tw, th, s_lo, s_hi, s_acc[wid], &s_next[wid], s_exit[wid], stack, err, nseg,
+                         nsh, nullptr);
         if (lane < (int)(tw * th)) {
             const uint32_t i = x0 + lane % tw, j = y0 + lane / tw;
             unsigned long long* a = T.acc + 4 * (T.acc_off[s] + (size_t)j * R.w + i);
@@ -735,6 +748,7 @@ lum_status create_batch(lum_scene* const* scenes, const lum_render_params* param
     };
     size_t o_ot = take(16ull * Q), o_dj = take(16ull * Q), o_bj = take(16ull * Q), o_L = take(16ull * Q);
     size_t o_ids = take(16ull * Q), o_hit = take(16ull * Q), o_sd = take(16ull * Q), o_sc = take(16ull * Q);
+    size_t o_so = take(16ull * Q);
     size_t o_ext0 = take(4ull * Q), o_ext1 = take(4ull * Q), o_free = take(4ull * Q), o_shq = take(4ull * Q);
     size_t o_mq[kQueues];
     for (int k = 0; k < kQueues; ++k) o_mq[k] = take(4ull * Q);
@@ -756,7 +770,7 @@ lum_status create_batch(lum_scene* const* scenes, const lum_render_params* param
     Pool& pl = b->pool;
     pl.o_t = (float4*)(m + o_ot); pl.d_jx = (float4*)(m + o_dj); pl.beta_jy = (float4*)(m + o_bj);
     pl.L = (float4*)(m + o_L); pl.ids = (uint4*)(m + o_ids); pl.hit = (float4*)(m + o_hit);
-    pl.sdir = (float4*)(m + o_sd); pl.scon = (float4*)(m + o_sc);
+    pl.sdir = (float4*)(m + o_sd); pl.scon = (float4*)(m + o_sc); pl.sorg = (float4*)(m + o_so);
     pl.ext[0] = (uint32_t*)(m + o_ext0); pl.ext[1] = (uint32_t*)(m + o_ext1);
     pl.freeq = (uint32_t*)(m + o_free); pl.shadowq = (uint32_t*)(m + o_shq);
     for (int k = 0; k < kQueues; ++k) pl.matq[k] = (uint32_t*)(m + o_mq[k]);
