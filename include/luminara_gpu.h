@@ -337,7 +337,11 @@ lum_status lum_render(lum_scene* scene, const lum_render_params* params, float* 
                       lum_stats* stats);
 
 /* Same as lum_render but writes a caller-owned DEVICE buffer on the caller's CUDA stream
- * (cudaStream_t passed as void*, NULL = the scene's stream); no host copies. */
+ * (cudaStream_t passed as void*, NULL = the scene's stream); no host copies.  With stats, the
+ * call waits for the render and reports the kernel's error flags; with stats NULL it only
+ * enqueues the work and returns (back-to-back frames keep the GPU busy whatever the host is
+ * doing; kernel error flags are then not reported).  Asynchronous calls on one scene must use
+ * one stream: they share the scene's work counters. */
 lum_status lum_render_device(lum_scene* scene, const lum_render_params* params,
                              float* d_out_rgb, void* stream, lum_stats* stats);
 

@@ -139,9 +139,13 @@ class GpuScene:
         check(lib().lum_render(self.h, C.byref(p), out.ctypes.data, C.byref(st)))
         return out, st
 
-    def render_device(self, cfg: RenderConfig, d_out: int, stream: int = 0):
-        """Renders into a caller-owned device buffer (pointer as int) on `stream`."""
+    def render_device(self, cfg: RenderConfig, d_out: int, stream: int = 0, wait: bool = True):
+        """Renders into a caller-owned device buffer (pointer as int) on `stream`.  wait=False
+        only enqueues the render (no stats, no synchronisation) and returns None."""
         p = cfg.to_c()
+        if not wait:
+            check(lib().lum_render_device(self.h, C.byref(p), C.c_void_p(d_out), C.c_void_p(stream), None))
+            return None
         st = abi.LumStats()
         check(lib().lum_render_device(self.h, C.byref(p), C.c_void_p(d_out), C.c_void_p(stream), C.byref(st)))
         return st

@@ -628,8 +628,9 @@ lum_status check_params(const lum_render_params* p) {
     return LUM_OK;
 }
 
+// sync = false: enqueue only (no counter readback, no synchronisation, no error flags).
 lum_status run_render(lum_scene* s, const lum_render_params* params, float* d_out, cudaStream_t stream,
-                      lum_stats* stats) {
+                      lum_stats* stats, bool sync = true) {
     lum::RenderDev R;
     lum_status st = make_render_dev(s, *params, R);
     if (st != LUM_OK) return st;
@@ -654,6 +655,7 @@ lum_status run_render(lum_scene* s, const lum_render_params* params, float* d_ou
         CU(cudaMemsetAsync(d_out, 0, sizeof(float) * 3 * (size_t)R.w * R.h, stream), "cudaMemsetAsync");
     }
     CU(cudaEventRecord(s->ev1, stream), "cudaEventRecord");
+    if (!sync) return LUM_OK;
     lum::WorkCounters wc{};
     CU(cudaMemcpyAsync(&wc, s->d_work, sizeof wc, cudaMemcpyDeviceToHost, stream), "cudaMemcpyAsync");
     CU(cudaStreamSynchronize(stream), "render");
@@ -848,7 +850,7 @@ lum_status lum_render_device(lum_scene* s, const lum_render_params* params, floa
     std::lock_guard<std::mutex> lk(s->mu);
     CU(cudaSetDevice(s->device), "cudaSetDevice");
     cudaStream_t cs = stream ? (cudaStream_t)stream : s->stream;
-    return run_render(s, params, d_out, cs, stats);
+    return run_render(s, params, d_out, cs, stats, stats != nullptr);
 }
 
 lum_status lum_scene_set_envmap(lum_scene* s, const float* rgb, uint32_t width, uint32_t height) {

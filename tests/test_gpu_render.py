@@ -184,6 +184,13 @@ def test_render_device_matches_host_path():
     torch.cuda.synchronize()
     assert np.array_equal(out.cpu().numpy(), host)
     assert st.kernel_ms > 0
+    # without stats the call only enqueues: three frames back to back, the last one read
+    outs = [torch.full((24, 40, 3), -1.0, dtype=torch.float32, device="cuda") for _ in range(3)]
+    for o in outs:
+        assert sc.render_device(cfg, o.data_ptr(), stream.cuda_stream, wait=False) is None
+    torch.cuda.synchronize()
+    for o in outs:
+        assert np.array_equal(o.cpu().numpy(), host)
 
 
 def test_reference_render_entry_point():
