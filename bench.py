@@ -347,7 +347,8 @@ def run_ours(args):
         "unit": "GB/s" if frac_b >= frac_f else "TFLOP/s",
         "frac": max(frac_b, frac_f),
         "traffic": traffic,
-        "peak_kind": (f"HBM {peak_kind} (MEASURED_PEAKS.json)" if frac_b >= frac_f else
+        "peak_kind": ((f"HBM measured (MEASURED_PEAKS.json)" if peak_kind == "measured" else
+                       "HBM fallback 6650 GB/s (no MEASURED_PEAKS.json)") if frac_b >= frac_f else
                       "FP32 nominal: SMs x 128 lanes x 2 x max SM clock (no measured FP32 peak available)"),
         "bytes_per_launch": nbytes, "flops_per_launch": flops,
         "hbm": {"achieved_gbs": ach_gbs, "peak_gbs": hbm_peak, "frac": frac_b, "of": peak_kind},
