@@ -34,8 +34,9 @@ __device__ __forceinline__ void fixed_pixel(const unsigned long long* a, float e
 
 // Runs the task; on return acc[k][0..3] (k < tw * th, pixel (k % tw, k / tw) of the tile) hold
 // the sums.  acc (32 x 4) and *next are the warp's shared memory; the call zeroes them.
-// EXT: the scene may use the other materials or backgrounds (shade's EXT).
-template <bool COUNT, bool EXT = true>
+// EXT: the scene may use the other materials or backgrounds; NEE: it has lights (shade's
+// template flags).
+template <bool COUNT, bool EXT = true, bool NEE = true>
 __device__ __forceinline__ void tile_task(const SceneDev& S, const RenderDev& R, uint32_t x0, uint32_t y0,
                                           uint32_t tw, uint32_t th, uint32_t s_lo, uint32_t s_hi,
                                           unsigned long long (*acc)[4], uint32_t* next, V* exit_stash, int* stack,
@@ -82,7 +83,7 @@ __device__ __forceinline__ void tile_task(const SceneDev& S, const RenderDev& R,
                 state = P.bounce >= R.max_depth ? ST_DONE : ST_CLOSEST;
             } else {
                 ++nseg;
-                state = shade<-1, EXT>(S, R, pixel, P, found, h, pend, exit_stash + lane);
+                state = shade<-1, EXT, NEE>(S, R, pixel, P, found, h, pend, exit_stash + lane);
             }
         }
         if (state == ST_DONE) {
