@@ -112,12 +112,13 @@ class GpuScene:
         h = C.c_void_p()
         check(lib().lum_scene_create(self.desc.ref(), C.byref(h)))
         self.h = h
+        self._lib = lib()          # kept for close(): module globals may be gone at exit
         if getattr(world, "env_map", None) is not None:
             self.set_envmap(world.env_map)
 
     def close(self):
         if getattr(self, "h", None):
-            lib().lum_scene_destroy(self.h)
+            self._lib.lum_scene_destroy(self.h)
             self.h = None
 
     __del__ = close
@@ -251,6 +252,7 @@ class Batch:
         check(lib().lum_batch_create(C.cast(self._handles, C.POINTER(C.c_void_p)), self._params, n, cfg_ptr,
                                      C.byref(h)))
         self.h = h
+        self._lib = lib()
 
     def config(self):
         c = abi.LumBatchConfig()
@@ -278,7 +280,7 @@ class Batch:
 
     def close(self):
         if getattr(self, "h", None):
-            lib().lum_batch_destroy(self.h)
+            self._lib.lum_batch_destroy(self.h)
             self.h = None
 
     __del__ = close
