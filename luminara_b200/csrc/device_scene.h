@@ -107,7 +107,8 @@ struct SceneDev {
     int32_t n_lights;
     int32_t n_planes;
     int32_t n_mats;
-    int32_t pad;
+    int32_t spheres_basic;   // every primitive is a sphere and every material Lambertian / Metal /
+                             // Dielectric / Emissive (planes allowed): the SPH kernels apply
     const BlendEmit* blend_emit;   // emissive leaves of Blend materials
     const float* env;        // environment map, env_w * env_h RGB floats (or null)
     uint32_t env_w, env_h;

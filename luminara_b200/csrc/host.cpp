@@ -802,6 +802,12 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
     D.n_lights = (int32_t)lights.size();
     D.n_planes = (int32_t)F.planes.size();
     D.n_mats = (int32_t)mats.size();
+    // the sphere-and-basic-materials kernel class (planes are tested in the general way)
+    bool sph = true;
+    for (size_t k = 0; k < np && sph; ++k) sph = (meta[k] & 15) == lum::PT_SPHERE;
+    for (uint32_t i = 0; i < desc->n_materials && sph; ++i)
+        sph = desc->materials[i].kind >= LUM_MAT_LAMBERTIAN && desc->materials[i].kind <= LUM_MAT_EMISSIVE;
+    D.spheres_basic = sph ? 1 : 0;
     D.cam = make_camera(desc->camera);
     s->n_prims = (uint32_t)(np + F.planes.size());
     s->n_nodes = (uint32_t)bvh.nodes.size();

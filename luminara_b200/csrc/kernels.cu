@@ -51,7 +51,7 @@ __device__ __forceinline__ void flush_counters(WorkCounters* wc, uint32_t err, u
 // then writes its pixels; a grouped one adds its sums to the frame's fixed-point accumulators,
 // which k_fixed_finalize turns into pixels.  Integer sums make the image deterministic and the
 // same whether or not the frame was grouped.
-template <bool COUNT, bool EXT, bool NEE>
+template <bool COUNT, bool EXT, bool NEE, bool SPH>
 __global__ void __launch_bounds__(kRenderThreads, LUM_RENDER_MIN_BLOCKS) k_render(SceneDev S, RenderDev R, float* __restrict__ out,
                                                            WorkCounters* wc, unsigned long long* __restrict__ gacc,
                                                            uint32_t n_groups, uint32_t group_strata) {
@@ -73,7 +73,8 @@ __global__ void __launch_bounds__(kRenderThreads, LUM_RENDER_MIN_BLOCKS) k_rende
         const uint32_t tw = min(8u, R.w - x0), th = min(4u, R.h - y0);
         const uint32_t s_lo = R.s_begin + group * group_strata;
         const uint32_t s_hi = min(R.s_end, s_lo + group_strata);
-        tile_task<COUNT, EXT, NEE>(S, R, x0, y0, tw, th, s_lo, s_hi, s_acc[wid], &s_next[wid], s_exit[wid], stack, err,
+        tile_task<COUNT, EXT, NEE, SPH>(S, R, x0, y0, tw, th, s_lo, s_hi, s_acc[wid], &s_next[wid], s_exit[wid], stack,
+                                        err,
                               nseg, nsh, &tally);
         if (lane < (int)(tw * th)) {
             const uint32_t i = x0 + lane % tw, j = y0 + lane / tw;
@@ -211,10 +212,12 @@ static size_t stack_bytes(int threads) { return (size_t)kStackDepth * threads * 
 static int render_occupancy() {
     static int occ = -1;
     if (occ < 0) {
-        for (auto fn : {k_render<false, false, false>, k_render<false, false, true>, k_render<false, true, false>,
-                        k_render<false, true, true>, k_render<true, false, true>, k_render<true, true, true>})
+        for (auto fn : {k_render<false, false, false, false>, k_render<false, false, true, false>,
+                        k_render<false, true, false, false>, k_render<false, true, true, false>,
+                        k_render<false, false, false, true>, k_render<false, false, true, true>,
+                        k_render<true, false, true, false>, k_render<true, true, true, false>})
             cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stack_bytes(kRenderThreads));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_render<false, false, true>, kRenderThreads,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_render<false, false, true, false>, kRenderThreads,
                                                       stack_bytes(kRenderThreads));
         if (occ <= 0) occ = 4;
     }
@@ -254,11 +257,14 @@ static cudaError_t launch_render_t(const SceneDev& S, const RenderDev& R, float*
     const uint64_t tasks = (uint64_t)R.n_tasks * grp.n_groups;
     int blocks_needed = (int)((tasks + 3) / 4);   // 4 warps per block, one task per warp at least
     if (grid > blocks_needed) grid = blocks_needed > 0 ? blocks_needed : 1;
-    // scenes without the other materials and backgrounds, or without lights, run kernels built
-    // without that code (the counter build keeps NEE: the same paths either way)
+    // scenes without the other materials and backgrounds, without lights, or made of spheres
+    // with the basic materials run kernels built without the code they cannot reach (the
+    // counter build is the general one: the same paths either way)
     const bool nee = COUNT || S.n_lights > 0;
-    auto kernel = R.ext ? (nee ? k_render<COUNT, true, true> : k_render<COUNT, true, COUNT>)
-                        : (nee ? k_render<COUNT, false, true> : k_render<COUNT, false, COUNT>);
+    const bool sph = !COUNT && !R.ext && S.spheres_basic;
+    auto kernel = R.ext ? (nee ? k_render<COUNT, true, true, false> : k_render<COUNT, true, COUNT, false>)
+                : sph   ? (nee ? k_render<COUNT, false, true, !COUNT> : k_render<COUNT, false, COUNT, !COUNT>)
+                        : (nee ? k_render<COUNT, false, true, false> : k_render<COUNT, false, COUNT, false>);
     kernel<<<grid, kRenderThreads, stack_bytes(kRenderThreads), stream>>>(S, R, out, wc, gacc, grp.n_groups,
                                                                           grp.group_strata);
     cudaError_t e = cudaGetLastError();

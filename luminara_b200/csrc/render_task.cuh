@@ -34,9 +34,9 @@ __device__ __forceinline__ void fixed_pixel(const unsigned long long* a, float e
 
 // Runs the task; on return acc[k][0..3] (k < tw * th, pixel (k % tw, k / tw) of the tile) hold
 // the sums.  acc (32 x 4) and *next are the warp's shared memory; the call zeroes them.
-// EXT: the scene may use the other materials or backgrounds; NEE: it has lights (shade's
-// template flags).
-template <bool COUNT, bool EXT = true, bool NEE = true>
+// EXT: the scene may use the other materials or backgrounds; NEE: it has lights; SPH: its
+// primitives are spheres and its materials the basic four (shade's and trace's template flags).
+template <bool COUNT, bool EXT = true, bool NEE = true, bool SPH = false>
 __device__ __forceinline__ void tile_task(const SceneDev& S, const RenderDev& R, uint32_t x0, uint32_t y0,
                                           uint32_t tw, uint32_t th, uint32_t s_lo, uint32_t s_hi,
                                           unsigned long long (*acc)[4], uint32_t* next, V* exit_stash, int* stack,
@@ -75,7 +75,7 @@ __device__ __forceinline__ void tile_task(const SceneDev& S, const RenderDev& R,
             h.t = shadow ? (EXT ? fabsf(pend.tmax) : pend.tmax) : CUDART_INF_F;
             h.prim = -1;
             h.b1 = h.b2 = 0.0f;
-            const bool found = trace<COUNT>(S, r, 0.001f, shadow, h, stack, err, tally);
+            const bool found = trace<COUNT, SPH>(S, r, 0.001f, shadow, h, stack, err, tally);
             if (shadow) {
                 ++nsh;
                 if (!found) P.L = P.L + pend.contrib;
@@ -83,7 +83,7 @@ __device__ __forceinline__ void tile_task(const SceneDev& S, const RenderDev& R,
                 state = P.bounce >= R.max_depth ? ST_DONE : ST_CLOSEST;
             } else {
                 ++nseg;
-                state = shade<-1, EXT, NEE>(S, R, pixel, P, found, h, pend, exit_stash + lane);
+                state = shade<-1, EXT, NEE, SPH>(S, R, pixel, P, found, h, pend, exit_stash + lane);
             }
         }
         if (state == ST_DONE) {

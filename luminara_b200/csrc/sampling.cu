@@ -47,7 +47,7 @@ __device__ __forceinline__ V clamp_sample(V L) {
 // filter-weighted value to acc[tile pixel] in fixed point (tile_task's sums; the call zeroes
 // acc); without, its clamped sample goes to smp[stratum - st_lo][tile pixel].  One copy of
 // the traversal and shading code serves every kind of tile.
-template <bool EXT, bool NEE>
+template <bool EXT, bool NEE, bool SPH>
 __device__ __forceinline__ void sample_pool(const SceneDev& S, const RenderDev& R, uint32_t x0, uint32_t y0, uint32_t tw,
                             const uint32_t* slot_px, uint32_t n_slots, uint32_t st_lo, uint32_t n_st, bool centre,
                             unsigned long long (*acc)[4], float (*smp)[32][3], uint32_t* next, V* exit_stash,
@@ -87,7 +87,7 @@ __device__ __forceinline__ void sample_pool(const SceneDev& S, const RenderDev& 
             h.t = shadow ? (EXT ? fabsf(pend.tmax) : pend.tmax) : CUDART_INF_F;
             h.prim = -1;
             h.b1 = h.b2 = 0.0f;
-            const bool found = trace<false>(S, r, 0.001f, shadow, h, stack, err);
+            const bool found = trace<false, SPH>(S, r, 0.001f, shadow, h, stack, err);
             if (shadow) {
                 ++nsh;
                 if (!found) P.L = P.L + pend.contrib;
@@ -95,7 +95,7 @@ __device__ __forceinline__ void sample_pool(const SceneDev& S, const RenderDev& 
                 state = P.bounce >= R.max_depth ? ST_DONE : ST_CLOSEST;
             } else {
                 ++nseg;
-                state = shade<-1, EXT, NEE>(S, R, pixel, P, found, h, pend, exit_stash + lane);
+                state = shade<-1, EXT, NEE, SPH>(S, R, pixel, P, found, h, pend, exit_stash + lane);
             }
         }
         if (state == ST_DONE) {
@@ -119,7 +119,7 @@ __device__ __forceinline__ void sample_pool(const SceneDev& S, const RenderDev& 
 
 __global__ void k_stamp(WorkCounters* wc) { wc->t0_ns = globaltimer(); }
 
-template <bool ADAPTIVE, bool EXT, bool NEE>
+template <bool ADAPTIVE, bool EXT, bool NEE, bool SPH>
 __global__ void __launch_bounds__(kSampThreads, ADAPTIVE ? 4 : 5) k_render_sampled(SceneDev S, RenderDev R, SamplingDev A,
                                                                     float* __restrict__ out, WorkCounters* wc) {
     extern __shared__ int s_stack[];
@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(kSampThreads, ADAPTIVE ? 4 : 5) k_render_sampl
             if (active) s_slot[wid][__popc(act & ((1u << lane) - 1u))] = lane;
             const uint32_t st_lo = expired ? 0u : ADAPTIVE ? lo : R.s_begin;
             const uint32_t n_st = expired ? 1u : ADAPTIVE ? min(kRoundStrata, total - lo) : R.s_end - R.s_begin;
-            sample_pool<EXT, NEE>(S, R, x0, y0, tw, s_slot[wid], __popc(act), st_lo, n_st, expired != 0,
+            sample_pool<EXT, NEE, SPH>(S, R, x0, y0, tw, s_slot[wid], __popc(act), st_lo, n_st, expired != 0,
                         fixed_sums ? s_acc[wid] : nullptr, s_smp[wid], &s_next[wid], s_exit[wid], stack, err, nseg,
                         nsh);
             if (active) {
@@ -214,14 +214,14 @@ __global__ void __launch_bounds__(kSampThreads, ADAPTIVE ? 4 : 5) k_render_sampl
 
 int g_sms = 0;
 
-template <bool ADAPTIVE, bool EXT, bool NEE>
+template <bool ADAPTIVE, bool EXT, bool NEE, bool SPH>
 cudaError_t launch_t(const SceneDev& S, const RenderDev& R, const SamplingDev& A, float* out, WorkCounters* wc,
                      cudaStream_t stream) {
     const size_t stack = (size_t)kStackDepth * kSampThreads * sizeof(int);
     static int occ = -1;
     if (occ < 0) {
-        cudaFuncSetAttribute(k_render_sampled<ADAPTIVE, EXT, NEE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stack);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_render_sampled<ADAPTIVE, EXT, NEE>, kSampThreads, stack);
+        cudaFuncSetAttribute(k_render_sampled<ADAPTIVE, EXT, NEE, SPH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stack);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_render_sampled<ADAPTIVE, EXT, NEE, SPH>, kSampThreads, stack);
         if (occ <= 0) occ = 1;
     }
     if (g_sms <= 0) {
@@ -234,7 +234,7 @@ cudaError_t launch_t(const SceneDev& S, const RenderDev& R, const SamplingDev& A
     int grid = g_sms * occ;
     const int needed = (int)std::min<uint64_t>(((uint64_t)R.n_tasks + kSampWarps - 1) / kSampWarps, 1u << 30);
     grid = std::max(1, std::min(grid, needed));
-    k_render_sampled<ADAPTIVE, EXT, NEE><<<grid, kSampThreads, stack, stream>>>(S, R, A, out, wc);
+    k_render_sampled<ADAPTIVE, EXT, NEE, SPH><<<grid, kSampThreads, stack, stream>>>(S, R, A, out, wc);
     return cudaGetLastError();
 }
 
@@ -242,21 +242,28 @@ cudaError_t launch_t(const SceneDev& S, const RenderDev& R, const SamplingDev& A
 
 cudaError_t launch_render_sampled(const SceneDev& S, const RenderDev& R, const SamplingDev& A, float* out,
                                   WorkCounters* wc, cudaStream_t stream) {
-    // scenes without the other materials and backgrounds, or without lights, run kernels built
-    // without that code
+    // scenes without the other materials and backgrounds, without lights, or made of spheres
+    // with the basic materials run kernels built without the code they cannot reach
     const bool nee = S.n_lights > 0;
     if (R.ext) {
         if (nee)
-            return A.adaptive ? launch_t<true, true, true>(S, R, A, out, wc, stream)
-                              : launch_t<false, true, true>(S, R, A, out, wc, stream);
-        return A.adaptive ? launch_t<true, true, false>(S, R, A, out, wc, stream)
-                          : launch_t<false, true, false>(S, R, A, out, wc, stream);
+            return A.adaptive ? launch_t<true, true, true, false>(S, R, A, out, wc, stream)
+                              : launch_t<false, true, true, false>(S, R, A, out, wc, stream);
+        return A.adaptive ? launch_t<true, true, false, false>(S, R, A, out, wc, stream)
+                          : launch_t<false, true, false, false>(S, R, A, out, wc, stream);
+    }
+    if (S.spheres_basic) {
+        if (nee)
+            return A.adaptive ? launch_t<true, false, true, true>(S, R, A, out, wc, stream)
+                              : launch_t<false, false, true, true>(S, R, A, out, wc, stream);
+        return A.adaptive ? launch_t<true, false, false, true>(S, R, A, out, wc, stream)
+                          : launch_t<false, false, false, true>(S, R, A, out, wc, stream);
     }
     if (nee)
-        return A.adaptive ? launch_t<true, false, true>(S, R, A, out, wc, stream)
-                          : launch_t<false, false, true>(S, R, A, out, wc, stream);
-    return A.adaptive ? launch_t<true, false, false>(S, R, A, out, wc, stream)
-                      : launch_t<false, false, false>(S, R, A, out, wc, stream);
+        return A.adaptive ? launch_t<true, false, true, false>(S, R, A, out, wc, stream)
+                          : launch_t<false, false, true, false>(S, R, A, out, wc, stream);
+    return A.adaptive ? launch_t<true, false, false, false>(S, R, A, out, wc, stream)
+                      : launch_t<false, false, false, false>(S, R, A, out, wc, stream);
 }
 
 }  // namespace lum

@@ -230,13 +230,20 @@ __device__ __forceinline__ bool hit_fog(int type, float4 a, float4 b, float4 c, 
 }
 
 // One primitive test; updates the closest hit when t is within [tmin, hit.t].
-template <bool COUNT = false>
+// SPH: the scene's primitives are all spheres (SceneDev::spheres_basic), so the other
+// primitive tests are left out of the kernel.
+template <bool COUNT = false, bool SPH = false>
 __device__ __forceinline__ bool test_prim(const SceneDev& S, int i, const Ray& ray, float tmin, Hit& hit,
                                           TestTally* tl = nullptr) {
-    int type = __ldg(S.meta + i) & 15;
-    if constexpr (COUNT) tl->prim[type]++;
     float4 a = ldp(S, i, 0);
     float t;
+    if constexpr (SPH && !COUNT) {
+        float4 b = ldp(S, i, 1);
+        if (hit_sphere(a, b, ray, tmin, hit.t, t)) { hit.t = t; hit.prim = i; return true; }
+        return false;
+    }
+    int type = __ldg(S.meta + i) & 15;
+    if constexpr (COUNT) tl->prim[type]++;
     switch (type) {
         case PT_SPHERE: {
             float4 b = ldp(S, i, 1);
@@ -295,7 +302,7 @@ __device__ __forceinline__ bool hit_plane(const PlaneDev& P, const Ray& ray, flo
 // (scene.rs:826-831).
 constexpr int kSentinel = 0x7fffffff;
 
-template <bool COUNT = false>
+template <bool COUNT = false, bool SPH = false>
 __device__ __forceinline__ bool trace(const SceneDev& S, const Ray& ray, float tmin, bool any, Hit& hit, int* stack,
                                       uint32_t& err, TestTally* tl = nullptr) {
     bool found = false;
@@ -355,7 +362,7 @@ __device__ __forceinline__ bool trace(const SceneDev& S, const Ray& ray, float t
             while (leaf < 0) {
                 const int first = (~leaf) >> 3, cnt = ((~leaf) & 7) + 1;
                 for (int k = 0; k < cnt; ++k) {
-                    if (test_prim<COUNT>(S, first + k, ray, tmin, hit, tl)) {
+                    if (test_prim<COUNT, SPH>(S, first + k, ray, tmin, hit, tl)) {
                         found = true;
                         if (any) return true;
                     }
@@ -390,6 +397,7 @@ struct Surface {
 };
 
 // Point, outward normal, face orientation and material of a hit (hit.rs:19-43).
+template <bool SPH = false>
 __device__ __forceinline__ Surface surface_of(const SceneDev& S, const Ray& ray, const Hit& h) {
     Surface s;
     s.p = fma3(ray.d, h.t, ray.o);
@@ -400,7 +408,7 @@ __device__ __forceinline__ Surface surface_of(const SceneDev& S, const Ray& ray,
         s.mat = P.material;
     } else {
         int meta = __ldg(S.meta + h.prim);
-        int type = meta & 15;
+        int type = SPH ? (int)PT_SPHERE : meta & 15;
         s.mat = meta >> 4;
         float4 a = ldp(S, h.prim, 0);
         switch (type) {
@@ -670,10 +678,14 @@ __device__ __forceinline__ ScatterMore scatter_more(const MatDev* mp, V rd, V hp
 // the wavefront tracer); KIND = -1 dispatches on m.kind.  Both run the same arithmetic.
 // EXT = false leaves out the other materials (material.rs:396-865): kernels for scenes
 // without them carry none of their code (the megakernel is sensitive to its code size).
-template <int KIND = -1, bool EXT = true>
+// SPH: the scene's materials are Lambertian / Metal / Dielectric / Emissive only.
+template <int KIND = -1, bool EXT = true, bool SPH = false>
 __device__ __forceinline__ bool scatter(const MatDev& m, const Ray& ray, const Surface& sf, float hit_t, float4 s,
                                         const RenderDev& R, uint32_t pixel, uint32_t stratum, uint32_t bounce,
                                         Scatter& out) {
+    if constexpr (SPH) {
+        if (KIND < 0 && m.kind > 3) return false;                      // Emissive: no scatter
+    }
     switch (KIND >= 0 ? KIND : m.kind) {
         case 1: {                                                      // material.rs:59-71
             V d = sf.n + unit_vector(s.x, s.y);
@@ -1046,7 +1058,7 @@ __device__ __forceinline__ void shadow_done(Path& P, Pending& pend, const V* exi
 // known to be unoccluded.  Returns the lane's next state.
 // NEE = false builds the shading step of scenes without lights: no light-sampling code in the
 // kernel (the megakernel runs ~11% faster on a light-free scene without it: instruction fetch).
-template <int KIND = -1, bool EXT = true, bool NEE = true>
+template <int KIND = -1, bool EXT = true, bool NEE = true, bool SPH = false>
 __device__ __forceinline__ int shade(const SceneDev& S, const RenderDev& R, uint32_t pixel, Path& P, bool found,
                                      const Hit& h, Pending& pend, V* exit_stash = nullptr) {
     if (!found) {
@@ -1054,7 +1066,7 @@ __device__ __forceinline__ int shade(const SceneDev& S, const RenderDev& R, uint
         return ST_DONE;
     }
     const uint32_t depth = R.max_depth - P.bounce;
-    Surface sf = surface_of(S, P.ray, h);
+    Surface sf = surface_of<SPH>(S, P.ray, h);
     // A non-finite hit point (e.g. a fog hit at t = inf along a zero-length direction, where
     // the reference's distance test compares against NaN) makes this level's result NaN in
     // the reference, which its guard turns into zero for the level and everything deeper
@@ -1068,7 +1080,7 @@ __device__ __forceinline__ int shade(const SceneDev& S, const RenderDev& R, uint
     Scatter sc;
     sc.org = sf.p;
     const MatDev& ms = EXT && KIND < 0 ? blend_leaf(S, m, R, pixel, P.stratum, P.bounce) : m;
-    if (!scatter<KIND, EXT>(ms, P.ray, sf, h.t, su, R, pixel, P.stratum, P.bounce, sc)) {
+    if (!scatter<KIND, EXT, SPH>(ms, P.ray, sf, h.t, su, R, pixel, P.stratum, P.bounce, sc)) {
         P.L = P.L + mul(P.beta, e);
         return ST_DONE;
     }
