@@ -12,6 +12,8 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <utility>
+#include <vector>
 
 #include "kernels.h"
 #include "scene_access.h"
@@ -51,8 +53,11 @@ __device__ __forceinline__ void flush_counters(WorkCounters* wc, uint32_t err, u
 // then writes its pixels; a grouped one adds its sums to the frame's fixed-point accumulators,
 // which k_fixed_finalize turns into pixels.  Integer sums make the image deterministic and the
 // same whether or not the frame was grouped.
+// The SPH builds are small enough for more blocks per SM without spills (72 registers without
+// NEE, 80 with); their shared memory then fits when the traversal stack is sized to the scene's
+// BVH (SceneDev::stack_depth).
 template <bool COUNT, bool EXT, bool NEE, bool SPH>
-__global__ void __launch_bounds__(kRenderThreads, LUM_RENDER_MIN_BLOCKS) k_render(SceneDev S, RenderDev R, float* __restrict__ out,
+__global__ void __launch_bounds__(kRenderThreads, SPH ? (NEE ? 6 : 7) : LUM_RENDER_MIN_BLOCKS) k_render(SceneDev S, RenderDev R, float* __restrict__ out,
                                                            WorkCounters* wc, unsigned long long* __restrict__ gacc,
                                                            uint32_t n_groups, uint32_t group_strata) {
     extern __shared__ int s_stack[];
@@ -224,6 +229,20 @@ static int render_occupancy() {
     return occ;
 }
 
+// Resident blocks per SM of a megakernel build with `smem` bytes of stack (cached).
+static int kernel_occupancy(const void* fn, size_t smem) {
+    static std::mutex mu;
+    static std::vector<std::pair<std::pair<const void*, size_t>, int>> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    for (const auto& e : cache)
+        if (e.first.first == fn && e.first.second == smem) return e.second;
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kRenderThreads, smem);
+    if (occ <= 0) occ = render_occupancy();
+    cache.push_back({{fn, smem}, occ});
+    return occ;
+}
+
 RenderGroups render_groups(const RenderDev& R) {
     RenderGroups g{1, R.s_end > R.s_begin ? R.s_end - R.s_begin : 0};
     const uint32_t n_st = g.group_strata;
@@ -253,19 +272,22 @@ static cudaError_t launch_render_t(const SceneDev& S, const RenderDev& R, float*
         cudaError_t e = cudaMemsetAsync(gacc, 0, 32 * n_px, stream);
         if (e != cudaSuccess) return e;
     }
-    int grid = num_sms() * blocks_per_sm;
-    const uint64_t tasks = (uint64_t)R.n_tasks * grp.n_groups;
-    int blocks_needed = (int)((tasks + 3) / 4);   // 4 warps per block, one task per warp at least
-    if (grid > blocks_needed) grid = blocks_needed > 0 ? blocks_needed : 1;
-    // scenes without the other materials and backgrounds, without lights, or made of spheres
-    // with the basic materials run kernels built without the code they cannot reach (the
-    // counter build is the general one: the same paths either way)
     const bool nee = COUNT || S.n_lights > 0;
     const bool sph = !COUNT && !R.ext && S.spheres_basic;
     auto kernel = R.ext ? (nee ? k_render<COUNT, true, true, false> : k_render<COUNT, true, COUNT, false>)
                 : sph   ? (nee ? k_render<COUNT, false, true, !COUNT> : k_render<COUNT, false, COUNT, !COUNT>)
                         : (nee ? k_render<COUNT, false, true, false> : k_render<COUNT, false, COUNT, false>);
-    kernel<<<grid, kRenderThreads, stack_bytes(kRenderThreads), stream>>>(S, R, out, wc, gacc, grp.n_groups,
+    // the traversal stack sized to the scene's BVH; resident blocks for that size
+    const size_t smem = (size_t)S.stack_depth * kRenderThreads * sizeof(int);
+    if (blocks_per_sm == occ) blocks_per_sm = kernel_occupancy((const void*)kernel, smem);
+    int grid = num_sms() * blocks_per_sm;
+    const uint64_t tasks = (uint64_t)R.n_tasks * grp.n_groups;
+    int blocks_needed = (int)((tasks + 3) / 4);   // 4 warps per block, one task per warp at least
+    if (grid > blocks_needed) grid = blocks_needed > 0 ? blocks_needed : 1;
+    // (kernel above: scenes without the other materials and backgrounds, without lights, or
+    // made of spheres with the basic materials run builds without the code they cannot reach;
+    // the counter build is the general one: the same paths either way)
+    kernel<<<grid, kRenderThreads, smem, stream>>>(S, R, out, wc, gacc, grp.n_groups,
                                                                           grp.group_strata);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || grp.n_groups <= 1) return e;

@@ -346,7 +346,7 @@ __device__ __forceinline__ bool trace(const SceneDev& S, const Ray& ray, float t
                     const bool first0 = h0 && (!h1 || en0 <= en1);
                     node = first0 ? c0e : c1e;
                     if (h0 && h1) {
-                        if (sp < kStackDepth) {
+                        if (sp < S.stack_depth) {
                             stack[sp++ * stride] = first0 ? c1e : c0e;
                         } else {
                             err |= LUM_KERR_STACK_OVERFLOW;
