@@ -296,8 +296,16 @@ def run_ours(args):
     t2 = time.perf_counter()
     clocks = ClockSampler(dev)
     clocks.start()
+    # warm-up steps are timed steps: the same flush, events and enqueue-only renders, so lazily
+    # loaded kernel modules (torch's fill kernel) and first-call host work stay out of the timed
+    # region
     for _ in range(args.warmup):
-        sc.render_device(cfg, out.data_ptr(), stream.cuda_stream)
+        w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.zero_()
+        w0.record(stream)
+        sc.render_device(cfg, out.data_ptr(), stream.cuda_stream, wait=False)
+        w1.record(stream)
+    torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
     log(f"scene build {build_s:.3f}s, counter build {t2 - t1:.3f}s, warmup {time.perf_counter() - t2:.3f}s")
@@ -368,7 +376,8 @@ def run_ours(args):
             s2.close()
             return img, st2
 
-        e2e_step()
+        for _ in range(max(1, args.warmup)):
+            e2e_step()
         barrier()
         t1 = time.perf_counter()
         for _ in range(args.steps):
@@ -450,8 +459,9 @@ def tonemap_block(L, hdr, H, Wd, stream, hbm_peak, flush):
             times.append(e0.elapsed_time(e1))
         ms = statistics.median(times)
         nbytes = H * Wd * (16 + (12 if auto else 0))
-        out[name] = {"ms": ms, "gbs": nbytes / ms / 1e6, "frac_of_measured_hbm": nbytes / ms / 1e6 / hbm_peak,
+        out[name] = {"ms": ms, "gbs": nbytes / ms / 1e6, "frac_of_hbm_peak": nbytes / ms / 1e6 / hbm_peak,
                      "bytes_per_call": nbytes}
+    out["hbm_peak"] = {"gbs": hbm_peak, "of": measured_peaks()[2]}
     out["pixels"] = H * Wd
     out["l2"] = "flushed (256 MiB write) before each timed call"
     return out
