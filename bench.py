@@ -370,14 +370,21 @@ def run_ours(args):
     # end to end through the public C ABI with host buffers: scene upload + render + readback
     e2e = None
     if not args.no_e2e:
+        phases = []
+
         def e2e_step():
+            t = time.perf_counter()
             s2 = L.GpuScene(world)
+            ta = time.perf_counter()
             img, st2 = s2.render(cfg)
+            tb = time.perf_counter()
             s2.close()
+            phases.append((ta - t, tb - ta, time.perf_counter() - tb, st2.kernel_ms / 1e3))
             return img, st2
 
         for _ in range(max(1, args.warmup)):
             e2e_step()
+        phases.clear()
         barrier()
         t1 = time.perf_counter()
         for _ in range(args.steps):
@@ -387,7 +394,9 @@ def run_ours(args):
         barrier()
         e2e = {"value": world_size * paths_per_step * args.steps / e2e_s / 1e6, "unit": "Mpaths/s",
                "h2d_bytes_per_step": int(info["device_bytes"]), "d2h_bytes_per_step": int(H * Wd * 3 * 4),
-               "path": "lum_scene_create (flatten + BVH + H2D) + lum_render (render + D2H) + lum_scene_destroy"}
+               "path": "lum_scene_create (flatten + BVH + H2D) + lum_render (render + D2H) + lum_scene_destroy",
+               "median_ms": {k: 1e3 * statistics.median(ph[i] for ph in phases) for i, k in
+                             enumerate(("scene_create", "render", "scene_destroy", "render_kernel"))}}
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
