@@ -23,11 +23,12 @@
 namespace lum {
 
 constexpr int kRenderThreads = 128;
-// Minimum resident blocks per SM requested from the register allocator for the megakernel
-// (5 -> 96 registers, no spills; the fastest of 4/5/6/8 on the random-spheres and box-room
-// frames measured on B200).
+// Minimum resident blocks per SM requested from the register allocator for the general
+// megakernel builds (6 -> 80 registers, 24-58 bytes of spills; on B200 3-6% faster than 5 blocks
+// at 93 registers without spills on the box-room, diff-quads and dense-mesh frames).  The
+// sphere builds use 7 blocks without lights (72 registers, no spills) and 6 with them.
 #ifndef LUM_RENDER_MIN_BLOCKS
-#define LUM_RENDER_MIN_BLOCKS 5
+#define LUM_RENDER_MIN_BLOCKS 6
 #endif
 constexpr unsigned kFull = 0xffffffffu;
 

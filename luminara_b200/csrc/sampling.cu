@@ -20,6 +20,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
+#include <utility>
+#include <vector>
 
 #include "kernels.h"
 #include "render_task.cuh"
@@ -217,12 +220,27 @@ int g_sms = 0;
 template <bool ADAPTIVE, bool EXT, bool NEE, bool SPH>
 cudaError_t launch_t(const SceneDev& S, const RenderDev& R, const SamplingDev& A, float* out, WorkCounters* wc,
                      cudaStream_t stream) {
-    const size_t stack = (size_t)kStackDepth * kSampThreads * sizeof(int);
-    static int occ = -1;
-    if (occ < 0) {
-        cudaFuncSetAttribute(k_render_sampled<ADAPTIVE, EXT, NEE, SPH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stack);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_render_sampled<ADAPTIVE, EXT, NEE, SPH>, kSampThreads, stack);
-        if (occ <= 0) occ = 1;
+    // the traversal stack sized to the scene's BVH; resident blocks per stack size (cached)
+    const size_t stack = (size_t)S.stack_depth * kSampThreads * sizeof(int);
+    static std::mutex mu;
+    static bool attr = false;
+    static std::vector<std::pair<size_t, int>> occ_of;
+    int occ = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!attr) {
+            cudaFuncSetAttribute(k_render_sampled<ADAPTIVE, EXT, NEE, SPH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)((size_t)kStackDepth * kSampThreads * sizeof(int)));
+            attr = true;
+        }
+        for (const auto& e : occ_of)
+            if (e.first == stack) occ = e.second;
+        if (occ <= 0) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_render_sampled<ADAPTIVE, EXT, NEE, SPH>, kSampThreads,
+                                                          stack);
+            if (occ <= 0) occ = 1;
+            occ_of.push_back({stack, occ});
+        }
     }
     if (g_sms <= 0) {
         int dev = 0;
