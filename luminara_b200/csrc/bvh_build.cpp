@@ -183,14 +183,14 @@ void linearize(TNode* t, int index, std::vector<NodeDev>& out, uint32_t depth, B
     }
     for (int c = 0; c < 2; ++c) {
         if (t->count[c] > 0) {
-            out[index].child[c] = t->first[c];
+            out[index].link[c] = ~((t->first[c] << 3) | (t->count[c] - 1));
             out[index].count[c] = t->count[c];
             res.n_leaves++;
             res.max_depth = std::max(res.max_depth, depth + 1);
         } else {
             int k = (int)out.size();
             out.emplace_back();
-            out[index].child[c] = k;
+            out[index].link[c] = k;
             out[index].count[c] = 0;
             linearize(t->kid[c].get(), k, out, depth + 1, res);
         }
@@ -199,8 +199,11 @@ void linearize(TNode* t, int index, std::vector<NodeDev>& out, uint32_t depth, B
 
 }  // namespace
 
-BvhResult build_bvh(const std::vector<BuildBox>& boxes, const BvhOptions& opt) {
+BvhResult build_bvh(const std::vector<BuildBox>& boxes, const BvhOptions& options) {
     BvhResult res;
+    BvhOptions opt = options;
+    opt.max_leaf = std::max(1, std::min(opt.max_leaf, 8));        // a link holds count - 1 in 3 bits
+    opt.force_leaf = std::max(1, std::min(opt.force_leaf, opt.max_leaf));
     const int n = (int)boxes.size();
     res.order.resize(n);
     for (int i = 0; i < n; ++i) res.order[i] = (uint32_t)i;

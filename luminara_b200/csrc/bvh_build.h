@@ -16,19 +16,22 @@ struct BuildBox {
 //   [0] c0.lo.x c0.hi.x c0.lo.y c0.hi.y
 //   [1] c1.lo.x c1.hi.x c1.lo.y c1.hi.y
 //   [2] c0.lo.z c0.hi.z c1.lo.z c1.hi.z
-//   [3] child0 child1 count0 count1   (count > 0: leaf of `count` primitives starting at child)
+//   [3] link0 link1 count0 count1
+// A link is the inner child's node index (>= 0), or for a leaf of `count` primitives starting at
+// slot `first`, ~(first << 3 | count - 1) (< 0): the traversal reads the two links as they are.
+// count (0 for inner children) is kept for the host.
 struct alignas(16) NodeDev {
     float n0[4];
     float n1[4];
     float n2[4];
-    int32_t child[2];
+    int32_t link[2];
     int32_t count[2];
 };
 static_assert(sizeof(NodeDev) == 64, "node layout");
 
 struct BvhOptions {
     int bins = 16;          // SAH bins per axis
-    int max_leaf = 4;       // largest leaf the SAH may choose
+    int max_leaf = 4;       // largest leaf the SAH may choose (at most 8: three bits of a link)
     int force_leaf = 1;     // ranges this small always become leaves
     float cost_node = 1.0f; // traversal cost of one node visit (two box tests)
     float cost_prim = 1.0f; // cost of one primitive test

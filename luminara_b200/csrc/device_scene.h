@@ -107,8 +107,8 @@ struct SceneDev {
     int32_t n_lights;
     int32_t n_planes;
     int32_t n_mats;
-    int32_t spheres_basic;   // every primitive is a sphere and every material Lambertian / Metal /
-                             // Dielectric / Emissive (planes allowed): the SPH kernels apply
+    int32_t spheres_basic;   // every primitive is a static sphere and every material Lambertian /
+                             // Metal / Dielectric / Emissive (planes allowed): the SPH kernels apply
     int32_t stack_depth;     // traversal stack entries this BVH can need (<= kStackDepth)
     int32_t pad;
     const BlendEmit* blend_emit;   // emissive leaves of Blend materials

@@ -804,7 +804,8 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
     D.n_mats = (int32_t)mats.size();
     // the sphere-and-basic-materials kernel class (planes are tested in the general way)
     bool sph = true;
-    for (size_t k = 0; k < np && sph; ++k) sph = (meta[k] & 15) == lum::PT_SPHERE;
+    for (size_t k = 0; k < np && sph; ++k)   // static spheres: record 1's w (moving flag) is 0
+        sph = (meta[k] & 15) == lum::PT_SPHERE && prims[16 * k + 7] == 0.0f;
     for (uint32_t i = 0; i < desc->n_materials && sph; ++i)
         sph = desc->materials[i].kind >= LUM_MAT_LAMBERTIAN && desc->materials[i].kind <= LUM_MAT_EMISSIVE;
     D.spheres_basic = sph ? 1 : 0;

@@ -230,16 +230,19 @@ __device__ __forceinline__ bool hit_fog(int type, float4 a, float4 b, float4 c, 
 }
 
 // One primitive test; updates the closest hit when t is within [tmin, hit.t].
-// SPH: the scene's primitives are all spheres (SceneDev::spheres_basic), so the other
-// primitive tests are left out of the kernel.
+// SPH: the scene's primitives are all static spheres (SceneDev::spheres_basic), so the other
+// primitive tests are left out of the kernel and a test reads only record 0 (centre, radius).
 template <bool COUNT = false, bool SPH = false>
 __device__ __forceinline__ bool test_prim(const SceneDev& S, int i, const Ray& ray, float tmin, Hit& hit,
                                           TestTally* tl = nullptr) {
     float4 a = ldp(S, i, 0);
     float t;
     if constexpr (SPH && !COUNT) {
-        float4 b = ldp(S, i, 1);
-        if (hit_sphere(a, b, ray, tmin, hit.t, t)) { hit.t = t; hit.prim = i; return true; }
+        if (hit_sphere(a, make_float4(0.0f, 0.0f, 0.0f, 0.0f), ray, tmin, hit.t, t)) {
+            hit.t = t;
+            hit.prim = i;
+            return true;
+        }
         return false;
     }
     int type = __ldg(S.meta + i) & 15;
@@ -324,7 +327,7 @@ __device__ __forceinline__ bool trace(const SceneDev& S, const Ray& ray, float t
                 float4 n0 = __ldg(nodes + 4 * node + 0);
                 float4 n1 = __ldg(nodes + 4 * node + 1);
                 float4 n2 = __ldg(nodes + 4 * node + 2);
-                int4 n3 = __ldg(reinterpret_cast<const int4*>(nodes) + 4 * node + 3);
+                const int2 n3 = __ldg(reinterpret_cast<const int2*>(nodes + 4 * node + 3));
                 if constexpr (COUNT) tl->node++;
                 // slab tests of both children (aabb.rs:18-56)
                 float a0 = fmaf(n0.x, ix, ox), a1 = fmaf(n0.y, ix, ox);
@@ -338,8 +341,7 @@ __device__ __forceinline__ bool trace(const SceneDev& S, const Ray& ray, float t
                 float en1 = fmaxf(fmaxf(fminf(d0, d1), fminf(e0, e1)), fmaxf(fminf(f0, f1), tmin));
                 float ex1 = fminf(fminf(fmaxf(d0, d1), fmaxf(e0, e1)), fminf(fmaxf(f0, f1), hit.t));
                 const bool h0 = en0 < ex0, h1 = en1 < ex1;
-                const int c0e = n3.z > 0 ? ~((n3.x << 3) | (n3.z - 1)) : n3.x;
-                const int c1e = n3.w > 0 ? ~((n3.y << 3) | (n3.w - 1)) : n3.y;
+                const int c0e = n3.x, c1e = n3.y;   // links: inner node or encoded leaf
                 if (!h0 && !h1) {
                     node = sp > 0 ? stack[--sp * stride] : kSentinel;
                 } else {
@@ -413,9 +415,11 @@ __device__ __forceinline__ Surface surface_of(const SceneDev& S, const Ray& ray,
         float4 a = ldp(S, h.prim, 0);
         switch (type) {
             case PT_SPHERE: {
-                float4 b = ldp(S, h.prim, 1);
                 V c = xyz(a);
-                if (b.w != 0.0f) c = fma3(xyz(b) - c, ray.time, c);
+                if constexpr (!SPH) {
+                    float4 b = ldp(S, h.prim, 1);
+                    if (b.w != 0.0f) c = fma3(xyz(b) - c, ray.time, c);
+                }
                 on = (s.p - c) * (1.0f / a.w);
                 break;
             }

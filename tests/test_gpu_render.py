@@ -198,3 +198,14 @@ def test_reference_render_entry_point():
     res = L.render(cfg, world.camera, world, world.lights)
     assert res.hdr_data.shape == (20, 20, 3) and res.total_rays == 20 * 20 * 4
     assert np.isfinite(res.hdr_data).all() and res.hdr_data.mean() > 0
+
+
+def test_sphere_scene_classes_match_oracle():
+    # Static spheres with the basic materials run the sphere-only kernel build; one moving
+    # sphere moves the same scene to the general build.  Both follow the keyed oracle.
+    world, cfg = W.random_spheres(width=64, height=36, spp=4, grid=4)
+    world.camera.aspect_ratio = 64 / 36
+    keyed_compare(world, cfg)
+    world.add(S.MovingSphere((-2.0, 0.5, 2.0), (-2.0, 0.9, 2.0), 0.5, S.Lambertian((0.7, 0.3, 0.3))))
+    world.add(S.MovingSphere((2.0, 0.5, 2.5), (2.4, 0.5, 2.5), 0.5, S.Metal((0.8, 0.8, 0.8), 0.1)))
+    keyed_compare(world, cfg)
