@@ -110,7 +110,7 @@ struct SceneDev {
     int32_t spheres_basic;   // every primitive is a static sphere and every material Lambertian /
                              // Metal / Dielectric / Emissive (planes allowed): the SPH kernels apply
     int32_t stack_depth;     // traversal stack entries this BVH can need (<= kStackDepth)
-    int32_t pad;
+    int32_t moving;          // some sphere moves: camera rays draw their time
     const BlendEmit* blend_emit;   // emissive leaves of Blend materials
     const float* env;        // environment map, env_w * env_h RGB floats (or null)
     uint32_t env_w, env_h;

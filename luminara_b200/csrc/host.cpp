@@ -809,6 +809,9 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
     for (uint32_t i = 0; i < desc->n_materials && sph; ++i)
         sph = desc->materials[i].kind >= LUM_MAT_LAMBERTIAN && desc->materials[i].kind <= LUM_MAT_EMISSIVE;
     D.spheres_basic = sph ? 1 : 0;
+    D.moving = 0;
+    for (size_t k = 0; k < np && !D.moving; ++k)
+        D.moving = (meta[k] & 15) == lum::PT_SPHERE && prims[16 * k + 7] != 0.0f ? 1 : 0;
     // a traversal holds at most one pushed entry per level above its node
     D.stack_depth = (int32_t)std::min<uint32_t>((uint32_t)lum::kStackDepth, bvh.max_depth + 1);
     D.cam = make_camera(desc->camera);

@@ -1006,7 +1006,9 @@ __device__ __forceinline__ void start_path_at(const SceneDev& S, const RenderDev
     }
     P.ray.o = mk(C.origin) + off;
     P.ray.d = mk(C.llc) + mk(C.hor) * uc + mk(C.ver) * vc - mk(C.origin) - off;
-    P.ray.time = draw4(R.key0, R.key1, pixel, st, 0, CALL_CAMERA2).x;
+    // time matters only to moving spheres; a static scene skips the draw (the keyed draws of
+    // the other calls do not depend on it)
+    P.ray.time = S.moving ? draw4(R.key0, R.key1, pixel, st, 0, CALL_CAMERA2).x : 0.0f;
     P.beta = mk(1.f, 1.f, 1.f);
     P.L = mk(0.f, 0.f, 0.f);
     P.stratum = st;
