@@ -201,32 +201,30 @@ __global__ void __launch_bounds__(kRenderThreads) k_occluded(SceneDev S, const l
 }
 
 // ------------------------------------------------------------------------------ launchers
-static int g_num_sms = 0;
-
 static int num_sms() {
-    if (g_num_sms == 0) {
-        int dev = 0;
+    static const int n = [] {   // initialised once, thread-safe
+        int dev = 0, sms = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-        if (g_num_sms <= 0) g_num_sms = 148;
-    }
-    return g_num_sms;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        return sms > 0 ? sms : 148;
+    }();
+    return n;
 }
 
 static size_t stack_bytes(int threads) { return (size_t)kStackDepth * threads * sizeof(int); }
 
 static int render_occupancy() {
-    static int occ = -1;
-    if (occ < 0) {
+    static const int occ = [] {   // initialised once, thread-safe
         for (auto fn : {k_render<false, false, false, false>, k_render<false, false, true, false>,
                         k_render<false, true, false, false>, k_render<false, true, true, false>,
                         k_render<false, false, false, true>, k_render<false, false, true, true>,
                         k_render<true, false, true, false>, k_render<true, true, true, false>})
             cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stack_bytes(kRenderThreads));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_render<false, false, true, false>, kRenderThreads,
+        int o = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_render<false, false, true, false>, kRenderThreads,
                                                       stack_bytes(kRenderThreads));
-        if (occ <= 0) occ = 4;
-    }
+        return o > 0 ? o : 4;
+    }();
     return occ;
 }
 

@@ -215,7 +215,15 @@ __global__ void __launch_bounds__(kSampThreads, ADAPTIVE ? 4 : 5) k_render_sampl
     }
 }
 
-int g_sms = 0;
+int num_sms() {
+    static const int n = [] {   // initialised once, thread-safe
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        return sms > 0 ? sms : 148;
+    }();
+    return n;
+}
 
 template <bool ADAPTIVE, bool EXT, bool NEE, bool SPH>
 cudaError_t launch_t(const SceneDev& S, const RenderDev& R, const SamplingDev& A, float* out, WorkCounters* wc,
@@ -242,14 +250,8 @@ cudaError_t launch_t(const SceneDev& S, const RenderDev& R, const SamplingDev& A
             occ_of.push_back({stack, occ});
         }
     }
-    if (g_sms <= 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
-        if (g_sms <= 0) g_sms = 148;
-    }
     k_stamp<<<1, 1, 0, stream>>>(wc);
-    int grid = g_sms * occ;
+    int grid = num_sms() * occ;
     const int needed = (int)std::min<uint64_t>(((uint64_t)R.n_tasks + kSampWarps - 1) / kSampWarps, 1u << 30);
     grid = std::max(1, std::min(grid, needed));
     k_render_sampled<ADAPTIVE, EXT, NEE, SPH><<<grid, kSampThreads, stack, stream>>>(S, R, A, out, wc);
