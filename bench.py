@@ -396,7 +396,8 @@ def run_ours(args):
                "h2d_bytes_per_step": int(info["device_bytes"]), "d2h_bytes_per_step": int(H * Wd * 3 * 4),
                "path": "lum_scene_create (flatten + BVH + H2D) + lum_render (render + D2H) + lum_scene_destroy",
                "median_ms": {k: 1e3 * statistics.median(ph[i] for ph in phases) for i, k in
-                             enumerate(("scene_create", "render", "scene_destroy", "render_kernel"))}}
+                             enumerate(("scene_create", "render", "scene_destroy", "render_kernel"))},
+               "step_ms": [round(1e3 * sum(ph[:3]), 2) for ph in phases]}
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
