@@ -50,9 +50,10 @@ struct Builder {
     const BvhOptions& opt;
     std::vector<uint32_t>& order;
     std::vector<float> cent;            // 3 per primitive
+    const float* pcost;                 // per-primitive test weight, or null (all 1)
 
-    Builder(const std::vector<BuildBox>& b, const BvhOptions& o, std::vector<uint32_t>& ord)
-        : boxes(b), opt(o), order(ord) {
+    Builder(const std::vector<BuildBox>& b, const BvhOptions& o, std::vector<uint32_t>& ord, const float* pc)
+        : boxes(b), opt(o), order(ord), pcost(pc) {
         cent.resize(3 * b.size());
         for (size_t i = 0; i < b.size(); ++i)
             for (int k = 0; k < 3; ++k) cent[3 * i + k] = 0.5f * (b[i].lo[k] + b[i].hi[k]);
@@ -64,51 +65,64 @@ struct Builder {
         return b;
     }
 
+    float weight(uint32_t p) const { return pcost ? pcost[p] : 1.0f; }
+
     // Splits [begin, end) in place; returns mid, or -1 when the range should be a leaf.
     int split(int begin, int end, int depth, const Box& nb) {
         const int n = end - begin;
         if (n <= opt.force_leaf) return -1;
         Box cb;
+        float leaf_cost = 0.0f;             // tests of the whole range as one leaf
         for (int i = begin; i < end; ++i) {
             const float* c = &cent[3 * order[i]];
             cb.grow(c, c);
+            leaf_cost += weight(order[i]);
         }
         int best_axis = -1, best_bin = -1;
         float best_cost = std::numeric_limits<float>::infinity();
         if (depth < kMedianDepth) {
             const int B = opt.bins;
             std::vector<int> cnt(B);
+            std::vector<float> wsum(B);
             std::vector<Box> bb(B);
             std::vector<float> rarea(B);
             std::vector<int> rcnt(B);
+            std::vector<float> rw(B);
             for (int ax = 0; ax < 3; ++ax) {
                 float ext = cb.hi[ax] - cb.lo[ax];
                 if (!(ext > 0.0f)) continue;
                 float scale = (float)B / ext;
                 std::fill(cnt.begin(), cnt.end(), 0);
+                std::fill(wsum.begin(), wsum.end(), 0.0f);
                 std::fill(bb.begin(), bb.end(), Box());
                 for (int i = begin; i < end; ++i) {
                     uint32_t p = order[i];
                     int k = std::min(B - 1, (int)((cent[3 * p + ax] - cb.lo[ax]) * scale));
                     cnt[k]++;
+                    wsum[k] += weight(p);
                     bb[k].grow(boxes[p].lo, boxes[p].hi);
                 }
                 Box acc;
                 int c = 0;
+                float cw = 0.0f;
                 for (int k = B - 1; k > 0; --k) {
                     acc.grow(bb[k]);
                     c += cnt[k];
+                    cw += wsum[k];
                     rarea[k] = acc.area();
                     rcnt[k] = c;
+                    rw[k] = cw;
                 }
                 Box lacc;
                 int lc = 0;
+                float lw = 0.0f;
                 float inv = 1.0f / std::max(nb.area(), 1e-30f);
                 for (int k = 1; k < B; ++k) {
                     lacc.grow(bb[k - 1]);
                     lc += cnt[k - 1];
+                    lw += wsum[k - 1];
                     if (lc == 0 || rcnt[k] == 0) continue;
-                    float cost = opt.cost_node + opt.cost_prim * (lacc.area() * lc + rarea[k] * rcnt[k]) * inv;
+                    float cost = opt.cost_node + opt.cost_prim * (lacc.area() * lw + rarea[k] * rw[k]) * inv;
                     if (cost < best_cost) {
                         best_cost = cost;
                         best_axis = ax;
@@ -116,7 +130,7 @@ struct Builder {
                     }
                 }
             }
-            if (n <= opt.max_leaf && (best_axis < 0 || opt.cost_prim * n <= best_cost)) return -1;
+            if (n <= opt.max_leaf && (best_axis < 0 || opt.cost_prim * leaf_cost <= best_cost)) return -1;
             if (best_axis >= 0) {
                 const int B2 = opt.bins;
                 float ext = cb.hi[best_axis] - cb.lo[best_axis];
@@ -199,7 +213,8 @@ void linearize(TNode* t, int index, std::vector<NodeDev>& out, uint32_t depth, B
 
 }  // namespace
 
-BvhResult build_bvh(const std::vector<BuildBox>& boxes, const BvhOptions& options) {
+BvhResult build_bvh(const std::vector<BuildBox>& boxes, const BvhOptions& options,
+                    const std::vector<float>* prim_cost) {
     BvhResult res;
     BvhOptions opt = options;
     opt.max_leaf = std::max(1, std::min(opt.max_leaf, 8));        // a link holds count - 1 in 3 bits
@@ -208,7 +223,8 @@ BvhResult build_bvh(const std::vector<BuildBox>& boxes, const BvhOptions& option
     res.order.resize(n);
     for (int i = 0; i < n; ++i) res.order[i] = (uint32_t)i;
     if (n == 0) return res;
-    Builder b(boxes, opt, res.order);
+    const float* pc = prim_cost && prim_cost->size() == boxes.size() ? prim_cost->data() : nullptr;
+    Builder b(boxes, opt, res.order, pc);
     std::unique_ptr<TNode> root;
     Box nb = b.range_box(0, n);
     int mid = b.split(0, n, 0, nb);

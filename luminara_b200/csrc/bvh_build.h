@@ -34,7 +34,7 @@ struct BvhOptions {
     int max_leaf = 4;       // largest leaf the SAH may choose (at most 8: three bits of a link)
     int force_leaf = 1;     // ranges this small always become leaves
     float cost_node = 1.0f; // traversal cost of one node visit (two box tests)
-    float cost_prim = 1.0f; // cost of one primitive test
+    float cost_prim = 1.0f; // cost of one primitive test (times the primitive's own weight)
 };
 
 struct BvhResult {
@@ -44,8 +44,10 @@ struct BvhResult {
     uint32_t n_leaves = 0;
 };
 
-// Builds a binned-SAH BVH over `boxes` (centroids are box centres).  Deterministic for a
-// given input regardless of the thread count.
-BvhResult build_bvh(const std::vector<BuildBox>& boxes, const BvhOptions& opt);
+// Builds a binned-SAH BVH over `boxes` (centroids are box centres).  `prim_cost`, if given,
+// holds one weight per box: the relative cost of that primitive's intersection test in the SAH
+// (1 when absent).  Deterministic for a given input regardless of the thread count.
+BvhResult build_bvh(const std::vector<BuildBox>& boxes, const BvhOptions& opt,
+                    const std::vector<float>* prim_cost = nullptr);
 
 }  // namespace lum

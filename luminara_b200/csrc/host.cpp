@@ -708,8 +708,13 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
 
     std::vector<lum::BuildBox> boxes(F.prims.size());
     for (size_t i = 0; i < F.prims.size(); ++i) boxes[i] = F.prims[i].box;
+    // relative test costs in the SAH: a quad test reads four 16-byte records against one to
+    // three for the others; weighting quads 2 made the box-room frame 6% faster, while sphere
+    // and triangle scenes measured best at the plain weight 1
+    std::vector<float> weights(F.prims.size());
+    for (size_t i = 0; i < F.prims.size(); ++i) weights[i] = F.prims[i].type == lum::PT_QUAD ? 2.0f : 1.0f;
     lum::BvhOptions opt;
-    lum::BvhResult bvh = lum::build_bvh(boxes, opt);
+    lum::BvhResult bvh = lum::build_bvh(boxes, opt, &weights);
     if (bvh.max_depth > (uint32_t)lum::kMaxBvhDepth)
         return fail(LUM_ERR_TOO_LARGE, "BVH depth %u exceeds the traversal stack", bvh.max_depth);
 
