@@ -2,7 +2,9 @@
 //
 // Everything the kernels read is flattened into structure-of-arrays buffers in HBM:
 //   nodes   BVH2 nodes, 64 B each (both child boxes inline, so one node fetch tests two boxes)
-//   prims   world-space primitive records, 64 B each (transforms already applied)
+//   prims   world-space primitive records 0-2, 48 B per primitive (transforms already applied):
+//           what the sphere, triangle, disk and fog tests read
+//   prims3  record 3, 16 B per primitive: the quad test's plane and a triangle's shading normal
 //   meta    per-primitive (material << 4 | type)
 //   orig    per-primitive id in description order (for hit records)
 //   planes  unbounded planes, tested linearly after the BVH (src/scene.rs:826-831)
@@ -95,7 +97,8 @@ struct CameraDev {
 // Device scene: raw pointers into the scene's device allocation.
 struct SceneDev {
     const void* nodes;       // float4[4 * n_nodes]
-    const void* prims;       // float4[4 * n_prims]
+    const void* prims;       // float4[3 * n_prims]: records 0-2
+    const void* prims3;      // float4[n_prims]: record 3
     const int32_t* meta;     // n_prims
     const int32_t* orig;     // n_prims
     const float* smooth_n;   // 9 floats per smooth triangle (n0, n1, n2)

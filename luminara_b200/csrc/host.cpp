@@ -763,8 +763,16 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
         return cleanup(cuda_fail(ce, "cudaEventCreate"));
 
     size_t off_nodes = 0;
+    // records 0-2 (the hit tests' 48 bytes) apart from record 3: the traversal's working set
+    // of a large triangle mesh shrinks by a quarter
+    std::vector<float> prims012(12 * np), prims3(4 * np);
+    for (size_t k = 0; k < np; ++k) {
+        std::memcpy(&prims012[12 * k], &prims[16 * k], 12 * sizeof(float));
+        std::memcpy(&prims3[4 * k], &prims[16 * k + 12], 4 * sizeof(float));
+    }
     size_t off_prims = align256(off_nodes + bvh.nodes.size() * sizeof(lum::NodeDev));
-    size_t off_meta = align256(off_prims + prims.size() * sizeof(float));
+    size_t off_prims3 = align256(off_prims + prims012.size() * sizeof(float));
+    size_t off_meta = align256(off_prims3 + prims3.size() * sizeof(float));
     size_t off_orig = align256(off_meta + meta.size() * 4);
     size_t off_smooth = align256(off_orig + orig.size() * 4);
     size_t off_mats = align256(off_smooth + F.smooth.size() * 4);
@@ -782,7 +790,8 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
         return cudaMemcpy(base + off, src, bytes, cudaMemcpyHostToDevice);
     };
     if ((ce = up(off_nodes, bvh.nodes.data(), bvh.nodes.size() * sizeof(lum::NodeDev))) != cudaSuccess ||
-        (ce = up(off_prims, prims.data(), prims.size() * 4)) != cudaSuccess ||
+        (ce = up(off_prims, prims012.data(), prims012.size() * 4)) != cudaSuccess ||
+        (ce = up(off_prims3, prims3.data(), prims3.size() * 4)) != cudaSuccess ||
         (ce = up(off_meta, meta.data(), meta.size() * 4)) != cudaSuccess ||
         (ce = up(off_orig, orig.data(), orig.size() * 4)) != cudaSuccess ||
         (ce = up(off_smooth, F.smooth.data(), F.smooth.size() * 4)) != cudaSuccess ||
@@ -795,6 +804,7 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
     lum::SceneDev& D = s->dev;
     D.nodes = base + off_nodes;
     D.prims = base + off_prims;
+    D.prims3 = base + off_prims3;
     D.meta = (const int32_t*)(base + off_meta);
     D.orig = (const int32_t*)(base + off_orig);
     D.smooth_n = (const float*)(base + off_smooth);

@@ -90,8 +90,10 @@ struct Hit {
     float b1, b2; // triangle barycentrics (u, v)
 };
 
+// Record k (0-3, a constant at every call site) of primitive i.
 __device__ __forceinline__ float4 ldp(const SceneDev& S, int i, int k) {
-    return __ldg(reinterpret_cast<const float4*>(S.prims) + 4 * i + k);
+    return k < 3 ? __ldg(reinterpret_cast<const float4*>(S.prims) + 3 * i + k)
+                 : __ldg(reinterpret_cast<const float4*>(S.prims3) + i);
 }
 
 // Robust sphere roots (Haines et al., "Precision Improvements for Ray/Sphere Intersection",
