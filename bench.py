@@ -230,7 +230,7 @@ def run_reference(args):
         rows += r
     value = paths / secs / 1e6
     sample = (f"{rows} image rows (evenly spaced, {cfg.width} px x {strata(cfg)} strata each) over {args.steps} "
-              f"steps of ~{per_step:.0f} s")
+              f"steps of at most ~{per_step:.0f} s ({secs:.1f} s of CPU work in all)")
     line = {
         "impl": "reference", "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
