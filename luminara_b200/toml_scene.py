@@ -22,9 +22,9 @@ What is kept from the reference, on purpose:
 
 Post-processing settings (tone_map, gamma, bloom, ...) are returned in `post` untouched: they
 act on the finished image, after the sample loop.  Anything the device path does not
-render (other primitives, procedural/image textures, other materials, bump/normal maps,
-non-uniform box scale, starfield/env-map backgrounds, panorama camera) raises
-UnsupportedSceneError naming every such item, instead of rendering a different scene.
+render (other primitives, procedural/image textures, bump/normal maps, non-uniform box scale,
+panorama camera) raises UnsupportedSceneError naming every such item, instead of rendering a
+different scene.
 """
 from __future__ import annotations
 
