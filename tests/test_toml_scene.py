@@ -392,4 +392,5 @@ def test_reference_example_scenes_load_or_are_rejected_by_name():
                            bg_intensity=cfg.bg_intensity), mode=O.MODE_KEYED)
         assert np.isfinite(img).all()
     print("loaded:", loaded)
-    assert "cornell.toml" in loaded and len(loaded) >= 5, loaded
+    assert {"cornell.toml", "distortion.toml", "pbr_showcase.toml", "prism.toml", "retro.toml",
+            "toon.toml"} <= set(loaded), loaded
