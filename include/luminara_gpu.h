@@ -320,7 +320,12 @@ const char* lum_last_error(void);
 
 /* Replaces scene::load_scene's world construction + SceneWorld::from_list
  * (src/scene.rs:846-1645, 786-808): flattens transforms, builds the BVH on the host and
- * uploads structure-of-arrays device buffers.  An empty scene is valid (every ray misses). */
+ * uploads structure-of-arrays device buffers.  An empty scene is valid (every ray misses).
+ * Returns LUM_ERR_INVALID_ARGUMENT, naming the object, for a parameter that is not finite in
+ * f32 (objects, mesh vertices and normals, transforms, materials, lights, camera), for a
+ * degenerate quad or rect (u x v = 0) or disk (radius 0), and for a negative medium density;
+ * no ray hits such a quad or disk in the reference, whose loader reads only finite numbers.
+ * Zero-area sides of a box (a box flat along one axis) are left out, keeping their ids. */
 lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out_scene);
 
 /* Frees the scene's device buffers and stream. */
@@ -362,19 +367,30 @@ lum_status lum_render_aov(lum_scene* scene, const lum_render_params* params, flo
 
 /* Allocation-free render.  Same image as lum_render into the same caller-owned HOST buffer,
  * but it allocates no device memory, ever: the device image and the kernel's work counters
- * live in one fixed array of LUM_NOALLOC_MAX_PIXELS * 12 + 256 bytes (12 MiB) that every GPU
- * loading the library reserves until the process exits.  It is for callers that cannot call
- * cudaMalloc at render time -- services that reserve all device memory at start-up, or whose
- * free memory is held by another allocator's pool, where a render-time cudaMalloc would fail
- * or stall on device-wide synchronisation.  lum_render, by contrast, allocates its device image
- * on first use and whenever the image grows.
+ * live in one fixed array of LUM_NOALLOC_MAX_PIXELS * 12 + 256 bytes (12 MiB), part of the
+ * render kernels' module, which each device holds from the moment that module is loaded there
+ * until the process exits.  It is for callers that cannot call cudaMalloc at render time --
+ * services that reserve all device memory at start-up, or whose free memory is held by another
+ * allocator's pool, where a render-time cudaMalloc would fail or stall on device-wide
+ * synchronisation.  lum_render, by contrast, allocates its device image on first use and
+ * whenever the image grows.
  *   - Images of more than LUM_NOALLOC_MAX_PIXELS pixels (after crop) are rejected with
  *     LUM_ERR_TOO_LARGE.
- *   - The first call on a device looks up the array's device address (cudaGetSymbolAddress);
- *     make that first call before any stream capture.
+ *   - lum_scene_create loads the render kernels' module on its device and looks up the array's
+ *     device address (cudaGetSymbolAddress) there, so a scene created before the caller
+ *     reserves device memory is all the set-up a device needs.  (Under CUDA's lazy module
+ *     loading the module would otherwise load -- and need 12 MiB -- at the first render.)  If
+ *     that look-up failed, the first lum_render_noalloc call on the device repeats it; make
+ *     that call before any stream capture.
+ *   - The address is cached per device for the life of the process: after cudaDeviceReset
+ *     (or anything else that destroys the device's primary context) do not call this entry
+ *     point again in the same process.
  *   - All calls share the one array: calls that overlap on the GPU (e.g. from several host
- *     threads at once) race on it.  Each call clears the counters it needs and overwrites the
+ *     threads at once, on different scenes) race on it.  Calls on one scene handle are
+ *     serialised like lum_render's.  Each call clears the counters it needs and overwrites the
  *     image region it returns.
+ *   - Adaptive sampling and the time limit (params->adaptive, params->time_limit) are not
+ *     available here: they return LUM_ERR_UNSUPPORTED.
  *   - stats->kernel_ms is 0 (no events are created); total_ms is the host wall time.
  * No counterpart in the reference. */
 #define LUM_NOALLOC_MAX_PIXELS (1u << 20)

@@ -757,6 +757,7 @@ lum_status lum_backward(lum_scene* scene, const lum_render_params* params, const
     auto t0 = std::chrono::steady_clock::now();
     if (!scene || !params || !dL_dimage || !d_albedo || !d_roughness || !d_emission)
         return set_error(LUM_ERR_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lk(scene_mutex(scene));
     SceneDev dev;
     RenderDev R;
     cudaStream_t stream;

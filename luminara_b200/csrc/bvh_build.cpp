@@ -67,6 +67,14 @@ struct Builder {
 
     float weight(uint32_t p) const { return pcost ? pcost[p] : 1.0f; }
 
+    // Bin of a centroid coordinate, clamped to [0, B-1] before the integer conversion (a
+    // float-to-int conversion of a value outside the int range, or of NaN, is undefined).
+    static int bin_of(float c, float lo, float scale, int B) {
+        const float f = (c - lo) * scale;
+        if (!(f > 0.0f)) return 0;
+        return f >= (float)(B - 1) ? B - 1 : (int)f;
+    }
+
     // Splits [begin, end) in place; returns mid, or -1 when the range should be a leaf.
     int split(int begin, int end, int depth, const Box& nb) {
         const int n = end - begin;
@@ -97,7 +105,7 @@ struct Builder {
                 std::fill(bb.begin(), bb.end(), Box());
                 for (int i = begin; i < end; ++i) {
                     uint32_t p = order[i];
-                    int k = std::min(B - 1, (int)((cent[3 * p + ax] - cb.lo[ax]) * scale));
+                    int k = bin_of(cent[3 * p + ax], cb.lo[ax], scale, B);
                     cnt[k]++;
                     wsum[k] += weight(p);
                     bb[k].grow(boxes[p].lo, boxes[p].hi);
@@ -139,7 +147,7 @@ struct Builder {
                 const float* cp = cent.data();
                 int ax = best_axis, bin = best_bin;
                 auto it = std::stable_partition(order.begin() + begin, order.begin() + end, [&](uint32_t p) {
-                    return std::min(B2 - 1, (int)((cp[3 * p + ax] - lo) * scale)) < bin;
+                    return bin_of(cp[3 * p + ax], lo, scale, B2) < bin;
                 });
                 int mid = (int)(it - order.begin());
                 if (mid > begin && mid < end) return mid;

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <mutex>
@@ -67,6 +68,34 @@ double length(D3 a) { return std::sqrt(dot(a, a)); }
 D3 unit(D3 a) { return a * (1.0 / length(a)); }
 bool near_zero(D3 a) { return std::fabs(a.x) < 1e-8 && std::fabs(a.y) < 1e-8 && std::fabs(a.z) < 1e-8; }
 
+// Input validation.  The device computes in f32, so a parameter must be finite after the
+// conversion to float; a NaN or an infinity would reach the BVH builder's bin index (an
+// out-of-range integer conversion) and every ray's arithmetic.  The reference has no such
+// checks (its scene loader parses finite TOML numbers, scene.rs:846), so these rejections
+// only turn undefined behaviour into LUM_ERR_INVALID_ARGUMENT.
+bool finite32(double x) { return std::isfinite(x) && std::fabs(x) <= 3.0e38; }
+int first_nonfinite(const double* p, int n) {
+    for (int k = 0; k < n; ++k)
+        if (!finite32(p[k])) return k;
+    return -1;
+}
+// Parameters lum_object.p[] holds for each object kind (include/luminara_gpu.h).
+int object_param_count(int kind) {
+    switch (kind) {
+        case LUM_OBJ_SPHERE: return 4;
+        case LUM_OBJ_MOVING_SPHERE: return 7;
+        case LUM_OBJ_QUAD: return 9;
+        case LUM_OBJ_RECT_XY: case LUM_OBJ_RECT_XZ: case LUM_OBJ_RECT_YZ: return 5;
+        case LUM_OBJ_TRIANGLE: return 9;
+        case LUM_OBJ_DISK: return 7;
+        case LUM_OBJ_PLANE: return 6;
+        case LUM_OBJ_BOX: return 6;
+        case LUM_OBJ_FOG_SPHERE: return 5;
+        case LUM_OBJ_FOG_BOX: return 7;
+        default: return 0;
+    }
+}
+
 // Composite of the transform wrappers, object -> world: p' = M p + T.
 struct Xf {
     double M[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
@@ -96,6 +125,8 @@ lum_status make_xf(const lum_transform& t, Xf& xf) {
     if (t.n_ops < 0 || t.n_ops > LUM_MAX_XF_OPS) return fail(LUM_ERR_INVALID_ARGUMENT, "transform has %d ops", t.n_ops);
     for (int i = 0; i < t.n_ops; ++i) {
         const double* a = t.arg[i];
+        if (first_nonfinite(a, t.op[i] == LUM_XF_TRANSLATE ? 3 : 1) >= 0)
+            return fail(LUM_ERR_INVALID_ARGUMENT, "transform op %d: non-finite argument", i);
         switch (t.op[i]) {
             case LUM_XF_TRANSLATE:                                      // transform.rs:18-29
                 xf.T = xf.T + d3(a);
@@ -187,6 +218,20 @@ PrimH make_quad(D3 q, D3 u, D3 v, double sign, int mat, int orig) {
     return p;
 }
 
+// A quad whose plane is undefined: u x v is zero, or so small that w = n / |n|^2 leaves the f32
+// range.  No ray hits it in the reference (its normal and planar coordinates are NaN).
+bool degenerate_quad(D3 u, D3 v) {
+    const D3 n = cross(u, v);
+    const double l2 = dot(n, n);
+    return !(l2 > 0.0) || !finite32(std::sqrt(l2)) || !finite32(1.0 / std::sqrt(l2));
+}
+
+bool box_finite(const lum::BuildBox& b) {
+    for (int k = 0; k < 3; ++k)
+        if (!std::isfinite(b.lo[k]) || !std::isfinite(b.hi[k])) return false;
+    return true;
+}
+
 struct Flat {
     std::vector<PrimH> prims;
     std::vector<lum::PlaneDev> planes;
@@ -211,6 +256,11 @@ lum_status flatten(const lum_scene_desc& d, Flat& F) {
         const lum_object& o = d.objects[i];
         if (o.material < 0 || (uint32_t)o.material >= d.n_materials)
             return fail(LUM_ERR_INVALID_ARGUMENT, "object %u: material %d out of range", i, o.material);
+        const int n_par = object_param_count(o.kind);
+        if (n_par == 0) return fail(LUM_ERR_INVALID_ARGUMENT, "object %u: unknown kind %d", i, o.kind);
+        const int bad = first_nonfinite(o.p, n_par);
+        if (bad >= 0) return fail(LUM_ERR_INVALID_ARGUMENT, "object %u: parameter p[%d] is not finite", i, bad);
+        const size_t first_prim = F.prims.size();
         Xf xf;
         bool has_xf = o.transform >= 0;
         if (has_xf) {
@@ -242,6 +292,7 @@ lum_status flatten(const lum_scene_desc& d, Flat& F) {
             }
             case LUM_OBJ_QUAD: {
                 D3 q = xf.point(d3(p)), u = xf.vec(d3(p + 3)), v = xf.vec(d3(p + 6));
+                if (degenerate_quad(u, v)) return fail(LUM_ERR_INVALID_ARGUMENT, "object %u: degenerate quad (u x v = 0)", i);
                 F.prims.push_back(make_quad(q, u, v, 1.0, o.material, id++));
                 break;
             }
@@ -251,6 +302,8 @@ lum_status flatten(const lum_scene_desc& d, Flat& F) {
                 D3 q, u, v;
                 double sg;
                 rect_quad(o.kind - LUM_OBJ_RECT_XY, p[0], p[1], p[2], p[3], p[4], q, u, v, sg);
+                if (degenerate_quad(xf.vec(u), xf.vec(v)))
+                    return fail(LUM_ERR_INVALID_ARGUMENT, "object %u: degenerate rect (zero extent)", i);
                 F.prims.push_back(make_quad(xf.point(q), xf.vec(u), xf.vec(v), sg, o.material, id++));
                 break;
             }
@@ -264,6 +317,12 @@ lum_status flatten(const lum_scene_desc& d, Flat& F) {
                     D3 q, u, v;
                     double sg;
                     rect_quad(r.plane, r.a0, r.a1, r.b0, r.b1, r.k, q, u, v, sg);
+                    // a box flat along one axis (a panel) has four zero-area sides, which no ray
+                    // hits in the reference either: they keep their primitive ids but are left out
+                    if (degenerate_quad(xf.vec(u), xf.vec(v))) {
+                        ++id;
+                        continue;
+                    }
                     F.prims.push_back(make_quad(xf.point(q), xf.vec(u), xf.vec(v), sg, o.material, id++));
                 }
                 break;
@@ -298,6 +357,7 @@ lum_status flatten(const lum_scene_desc& d, Flat& F) {
                 n = unit(xf.vec(n));
                 D3 c = xf.point(d3(p));
                 double r = p[6] * std::fabs(xf.scale);
+                if (r == 0.0) return fail(LUM_ERR_INVALID_ARGUMENT, "object %u: degenerate disk (radius 0)", i);
                 set4(k.rec, 0, c, (float)r);
                 set4(k.rec, 1, n, 0.0f);
                 D3 rr{r, r, r};
@@ -326,6 +386,8 @@ lum_status flatten(const lum_scene_desc& d, Flat& F) {
             case LUM_OBJ_FOG_SPHERE:
             case LUM_OBJ_FOG_BOX: {                                     // constant_medium.rs:15-22
                 if (has_xf) return fail(LUM_ERR_UNSUPPORTED, "object %u: transformed constant medium", i);
+                if (p[o.kind == LUM_OBJ_FOG_SPHERE ? 4 : 6] < 0.0)
+                    return fail(LUM_ERR_INVALID_ARGUMENT, "object %u: negative medium density", i);
                 PrimH f{};
                 f.material = o.material;
                 f.orig = id++;
@@ -350,10 +412,23 @@ lum_status flatten(const lum_scene_desc& d, Flat& F) {
             default:
                 return fail(LUM_ERR_INVALID_ARGUMENT, "object %u: unknown kind %d", i, o.kind);
         }
+        // a transform can take finite parameters out of the f32 range
+        for (size_t k = first_prim; k < F.prims.size(); ++k)
+            if (!box_finite(F.prims[k].box))
+                return fail(LUM_ERR_INVALID_ARGUMENT, "object %u: geometry outside the f32 range", i);
+        if (o.kind == LUM_OBJ_PLANE) {
+            const lum::PlaneDev& pl = F.planes.back();
+            for (int k = 0; k < 3; ++k)
+                if (!std::isfinite(pl.p[k]) || !std::isfinite(pl.n[k]))
+                    return fail(LUM_ERR_INVALID_ARGUMENT, "object %u: geometry outside the f32 range", i);
+        }
     }
     for (uint32_t mi = 0; mi < d.n_meshes; ++mi) {
         const lum_mesh& m = d.meshes[mi];
         if (!m.positions || !m.indices) return fail(LUM_ERR_INVALID_ARGUMENT, "mesh %u: null arrays", mi);
+        for (size_t k = 0; k < 3 * (size_t)m.n_vertices; ++k)
+            if (!finite32(m.positions[k]) || (m.normals && !finite32(m.normals[k])))
+                return fail(LUM_ERR_INVALID_ARGUMENT, "mesh %u vertex %zu: position or normal is not finite", mi, k / 3);
         for (uint32_t t = 0; t < m.n_triangles; ++t) {
             const uint32_t* ix = m.indices + 3 * (size_t)t;
             if (ix[0] >= m.n_vertices || ix[1] >= m.n_vertices || ix[2] >= m.n_vertices)
@@ -695,11 +770,28 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
         int t = desc->materials[i].texture;
         if (t != LUM_TEX_SOLID && t != LUM_TEX_CHECKER)
             return fail(LUM_ERR_INVALID_ARGUMENT, "material %u: unknown texture %d", i, t);
+        const lum_material& m = desc->materials[i];
+        const double scalars[] = {m.tex_scale, m.fuzz, m.ior, m.roughness, m.metallic, m.intensity, m.dispersion,
+                                  m.extra[0], m.extra[1], m.extra[2], m.extra[3]};
+        if (first_nonfinite(m.color, 3) >= 0 || first_nonfinite(m.color2, 3) >= 0 || first_nonfinite(m.tint, 3) >= 0 ||
+            first_nonfinite(scalars, (int)(sizeof scalars / sizeof scalars[0])) >= 0)
+            return fail(LUM_ERR_INVALID_ARGUMENT, "material %u: a parameter is not finite", i);
     }
     for (uint32_t i = 0; i < desc->n_lights; ++i) {
-        int k = desc->lights[i].kind;
+        const lum_light& l = desc->lights[i];
+        int k = l.kind;
         if (k < LUM_LIGHT_SPHERE || k > LUM_LIGHT_DISK)
             return fail(LUM_ERR_INVALID_ARGUMENT, "light %u: unknown kind %d", i, k);
+        if (first_nonfinite(l.p0, 3) >= 0 || first_nonfinite(l.u, 3) >= 0 || first_nonfinite(l.v, 3) >= 0 ||
+            first_nonfinite(l.normal, 3) >= 0 || first_nonfinite(l.emission, 3) >= 0 || !finite32(l.radius))
+            return fail(LUM_ERR_INVALID_ARGUMENT, "light %u: a parameter is not finite", i);
+    }
+    {
+        const lum_camera& c = desc->camera;
+        const double scalars[] = {c.vfov_degrees, c.aspect_ratio, c.aperture, c.focus_dist};
+        if (first_nonfinite(c.look_from, 3) >= 0 || first_nonfinite(c.look_at, 3) >= 0 ||
+            first_nonfinite(c.vup, 3) >= 0 || first_nonfinite(scalars, 4) >= 0)
+            return fail(LUM_ERR_INVALID_ARGUMENT, "camera: a parameter is not finite");
     }
     Flat F;
     lum_status st = flatten(*desc, F);
@@ -829,12 +921,23 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
         D.moving = (meta[k] & 15) == lum::PT_SPHERE && prims[16 * k + 7] != 0.0f ? 1 : 0;
     // a traversal holds at most one pushed entry per level above its node
     D.stack_depth = (int32_t)std::min<uint32_t>((uint32_t)lum::kStackDepth, bvh.max_depth + 1);
+    // Diagnostic: LUM_STACK_BUDGET=n caps the traversal stack below what the tree needs, so the
+    // overflow path (LUM_KERR_STACK_OVERFLOW, the far subtree skipped) can be exercised; the push
+    // is bounds-checked against this value.
+    if (const char* sb = std::getenv("LUM_STACK_BUDGET")) {
+        const long b = std::strtol(sb, nullptr, 10);
+        if (b >= 1 && b < D.stack_depth) D.stack_depth = (int32_t)b;
+    }
     D.cam = make_camera(desc->camera);
     s->n_prims = (uint32_t)(np + F.planes.size());
     s->n_nodes = (uint32_t)bvh.nodes.size();
     s->n_lights = (uint32_t)lights.size();
     s->bvh_depth = bvh.max_depth;
     for (uint32_t i = 0; i < desc->n_materials; ++i) s->max_mat_kind = std::max(s->max_mat_kind, desc->materials[i].kind);
+    // With lazy module loading the render kernels' module (and the allocation-free render's
+    // fixed array in it) would load at the first render on this device; load it now, while the
+    // caller evidently can still allocate.
+    lum::noalloc_preload();
     *out = s;
     return LUM_OK;
 }
@@ -1091,6 +1194,8 @@ lum_status prepare_render(lum_scene* s, const lum_render_params* params, SceneDe
 }
 
 int scene_max_material_kind(const lum_scene* s) { return s ? s->max_mat_kind : 0; }
+
+std::mutex& scene_mutex(lum_scene* s) { return s->mu; }
 
 lum_status scene_view(lum_scene* s, const lum_render_params* params, SceneDev& dev, RenderDev& R, int& device) {
     if (!s) return fail(LUM_ERR_INVALID_ARGUMENT, "scene is null");

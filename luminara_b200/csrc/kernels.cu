@@ -371,6 +371,16 @@ lum_status noalloc_scratch(void** out) {
     return LUM_OK;
 }
 
+}  // namespace
+
+// Called by lum_scene_create with the scene's device current.
+void lum::noalloc_preload() {
+    void* unused = nullptr;
+    if (noalloc_scratch(&unused) != LUM_OK) lum::set_error(LUM_OK, "");   // reported again by the render
+}
+
+namespace {
+
 lum_status noalloc_cuda(cudaError_t e, const char* what) {
     char msg[256];
     snprintf(msg, sizeof msg, "%s: %s", what, cudaGetErrorString(e));
@@ -383,6 +393,7 @@ extern "C" lum_status lum_render_noalloc(lum_scene* scene, const lum_render_para
                                          lum_stats* stats) {
     auto t0 = std::chrono::steady_clock::now();
     if (!scene || !params || !out_rgb) return lum::set_error(LUM_ERR_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lk(lum::scene_mutex(scene));
     lum::SceneDev dev;
     lum::RenderDev R;
     cudaStream_t stream;

@@ -627,7 +627,13 @@ lum_status run_batch(lum_batch* b, float* const* d_outs, double* scene_done_ms, 
     for (const auto& r : b->R) max_depth = std::max(max_depth, r.max_depth);
     const unsigned long long refills = (b->total_work + b->pool.Q - 1) / b->pool.Q;
     const unsigned long long cap_iters = (refills + 2) * (2ull * max_depth + 4) + 64;
-    const unsigned long long cap_launches = cap_iters / b->cfg.iters_per_graph + 2;
+    unsigned long long cap_launches = cap_iters / b->cfg.iters_per_graph + 2;
+    // Diagnostic: LUM_BATCH_MAX_LAUNCHES=n lowers the cap, so the cap's error path
+    // (LUM_KERR_ITERATION_CAP) can be exercised without a runaway loop.
+    if (const char* ml = std::getenv("LUM_BATCH_MAX_LAUNCHES")) {
+        const long long m = std::strtoll(ml, nullptr, 10);
+        if (m >= 1 && (unsigned long long)m < cap_launches) cap_launches = (unsigned long long)m;
+    }
     uint32_t launches = 0;
     bool done = false;
     while (!done) {

@@ -222,7 +222,7 @@ inline V3 random_in_unit_disk(Sampler& s) {
 }
 
 // ---------------------------------------------------------------------------------------
-// Ray, AABB (src/ray.rs, src/aabb.rs:7-190)
+// Ray, AABB (src/ray.rs, src/aabb.rs:7-88)
 // ---------------------------------------------------------------------------------------
 struct Ray {
     V3 o, d;

@@ -34,7 +34,7 @@ def gpu_hit1(world, o, d, tmin=0.001, tmax=np.inf):
 
 
 # ---------------------------------------------------------------- reference known answers
-def test_kat_quad_center():                                 # quad.rs:330-346
+def test_kat_quad_center():                                 # quad.rs:85-101
     w = S.World()
     w.add(S.Quad((0, 0, 0), (1, 0, 0), (0, 0, 1), S.Lambertian(GRAY)))
     h = gpu_hit1(w, (0.5, 1.0, 0.5), (0, -1, 0))
@@ -44,7 +44,7 @@ def test_kat_quad_center():                                 # quad.rs:330-346
     assert gpu_hit1(w, (0.5, 1.0, 0.5), (1, 0, 0)) is None
 
 
-def test_kat_plane_t5():                                    # plane.rs:470-477
+def test_kat_plane_t5():                                    # plane.rs:86-93
     w = S.World()
     w.add(S.Plane((0, 0, 0), (0, 1, 0), S.Lambertian(GRAY)))
     h = gpu_hit1(w, (0, 5, 0), (0, -1, 0))
@@ -66,7 +66,7 @@ def test_kat_transforms():                                  # transform.rs:365-4
 
 def test_kat_primitives_and_bvh():
     w = S.World()
-    for i in range(50):                                     # bvh.rs:452-471
+    for i in range(50):                                     # bvh.rs:199-218
         w.add(S.Sphere((i * 2.0, 0, 0), 0.5, S.Lambertian(GRAY)))
     h = gpu_hit1(w, (0, 0, -2), (0, 0, 1))
     assert h is not None and h["prim_id"] == 0

@@ -67,14 +67,14 @@ def test_refract_normal_incidence():
     assert abs(r[0]) < 1e-6 and r[1] < 0.0
 
 
-# ---------------------------------------------------------------- aabb.rs:197-224
+# ---------------------------------------------------------------- aabb.rs:94-121
 def test_aabb_hit_miss_negative():
     assert O.aabb_hit([-1, -1, -1], [1, 1, 1], [0, 0, -5], [0, 0, 1])
     assert not O.aabb_hit([-1, -1, -1], [1, 1, 1], [0, 5, -5], [0, 0, 1])
     assert O.aabb_hit([-1, -1, -1], [1, 1, 1], [0, 0, 5], [0, 0, -1])
 
 
-# ---------------------------------------------------------------- bvh.rs:437-471
+# ---------------------------------------------------------------- bvh.rs:184-218
 def test_bvh_basic_hit():
     sc = world_of(S.Sphere((0, 0, -1), 0.5, S.Lambertian(GRAY)), S.Sphere((2, 0, -1), 0.5, S.Lambertian(GRAY)))
     assert hit1(sc, (0, 0, 0), (0, 0, -1)) is not None
@@ -120,7 +120,7 @@ def test_sphere_miss():
     assert hit1(sc, (100, 100, 100), (0, 0, -1)) is None
 
 
-# ---------------------------------------------------------------- quad.rs:330-403
+# ---------------------------------------------------------------- quad.rs:85-158
 def test_quad_hit_center_known_answer():
     sc = world_of(S.Quad((0, 0, 0), (1, 0, 0), (0, 0, 1), S.Lambertian(GRAY)))
     h = hit1(sc, (0.5, 1.0, 0.5), (0, -1, 0))
@@ -153,7 +153,7 @@ def test_xz_rect_hit_miss_and_box():
     assert first == 0 and w.n_prims() == 6
 
 
-# ---------------------------------------------------------------- triangle.rs:251-287
+# ---------------------------------------------------------------- triangle.rs:79-115
 def test_triangle_hit_miss_bbox():
     tri = S.Triangle((0, 0, 0), (1, 0, 0), (0, 1, 0), S.Lambertian(GRAY))
     sc = world_of(tri)
@@ -165,14 +165,14 @@ def test_triangle_hit_miss_bbox():
     assert bb[0] < 0.001 and bb[3] > 0.999 and bb[4] > 0.999
 
 
-# ---------------------------------------------------------------- disk.rs:361-383
+# ---------------------------------------------------------------- disk.rs:73-95
 def test_disk_hit_and_miss_outside_radius():
     sc = world_of(S.Disk((0, 0, 0), (0, 1, 0), 1.0, S.Lambertian(GRAY)))
     assert hit1(sc, (0, 1, 0), (0, -1, 0)) is not None
     assert hit1(sc, (5, 1, 0), (0, -1, 0)) is None
 
 
-# ---------------------------------------------------------------- plane.rs:470-507
+# ---------------------------------------------------------------- plane.rs:86-123
 def test_plane_known_answers():
     sc = world_of(S.Plane((0, 0, 0), (0, 1, 0), S.Lambertian(GRAY)))
     h = hit1(sc, (0, 5, 0), (0, -1, 0))
@@ -225,7 +225,7 @@ def test_constant_medium_bbox_and_dense_hit():
     assert hit1(sc, (0, 0, -10), (0, 0, 1)) is not None
 
 
-# ---------------------------------------------------------------- camera.rs:480-548
+# ---------------------------------------------------------------- camera.rs:111-179
 def test_camera_center_and_corners():
     cam = S.CameraConfig(look_from=(0, 0, 0), look_at=(0, 0, -1), vfov_degrees=90.0, aspect_ratio=2.0)
     _, d, _ = O.camera_ray(cam, 0.5, 0.5, seed=0)
@@ -328,7 +328,7 @@ def _nee_scene(blocker: bool):
     return O.OracleScene(w)
 
 
-# ---------------------------------------------------------------- material.rs:396-865, tests :1063-1298
+# ---------------------------------------------------------------- material.rs:396-865, tests :1063-1266
 def test_blend_chooses_between_materials():                      # material.rs:1063-1088
     mat = S.Blend(S.Lambertian((1.0, 0.0, 0.0)), S.Metal((0.0, 0.0, 1.0), 0.0), 0.5)
     out = O.scatter(mat, seed=42, n_iter=100, **HIT)

@@ -372,10 +372,13 @@ material = { type = "marble", color = [0.5, 0.5, 0.5] }
         assert any(want in it for it in items), (want, items)
 
 
-REF_SCENES = "/root/reference/examples/scenes"
+# The reference project's example scene directory (examples/scenes of a Luminara checkout),
+# named by LUM_REFERENCE_SCENES; the test is skipped when it is unset.
+REF_SCENES = os.environ.get("LUM_REFERENCE_SCENES", "")
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_SCENES), reason="reference example scenes not present")
+@pytest.mark.skipif(not REF_SCENES or not os.path.isdir(REF_SCENES),
+                    reason="LUM_REFERENCE_SCENES (the reference's examples/scenes) not set")
 def test_reference_example_scenes_load_or_are_rejected_by_name():
     loaded = []
     for f in sorted(glob.glob(os.path.join(REF_SCENES, "*.toml"))):

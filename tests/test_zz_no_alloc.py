@@ -7,8 +7,9 @@ lum_render_noalloc keeps the device image and the kernel's counters in one fixed
 (LUM_NOALLOC_MAX_PIXELS pixels) instead of allocating.  This file checks, through the C ABI,
 that two calls in a row return the same image as lum_render, bit for bit (same kernel and
 seeds; pixel sums in 64-bit fixed point do not depend on path order), that the shared array is
-reused cleanly by a call with another scene and size, and that images beyond the maximum are
-rejected.  It is named to be collected last.
+reused cleanly by a call with another scene and size, that renders leave the device's free
+memory unchanged, and that images beyond the maximum and the adaptive / time-limited sample
+loop are rejected.  It is named to be collected last.
 """
 import ctypes as C
 
@@ -73,3 +74,42 @@ def test_noalloc_rejects_images_beyond_the_maximum():
     rc, _, _ = _call(sc, cfg)
     assert rc == abi.LUM_ERR_TOO_LARGE
     assert b"maximum" in L.lib().lum_last_error()
+
+
+def test_noalloc_allocates_no_device_memory():
+    """The property the entry point exists for: once a device is set up (scenes created, which
+    loads the module holding the fixed array), renders of other scenes and sizes leave the
+    device's free memory unchanged.  Both scenes render once first, so each kernel build has
+    been launched (a first launch may grow the driver's per-context local-memory reserve)."""
+    import torch
+
+    w1, c1 = W.box_room(width=64, height=64, spp=4)
+    w2, c2 = W.random_spheres(width=96, height=54, spp=4)
+    s1, s2 = L.GpuScene(w1), L.GpuScene(w2)
+    for sc, cfg in ((s1, c1), (s2, c2)):
+        rc, _, _ = _call(sc, cfg)
+        assert rc == abi.LUM_OK, L.lib().lum_last_error()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    c1.width, c1.height, c1.samples_per_pixel = 512, 384, 9
+    w1.camera.aspect_ratio = 512 / 384
+    c2.width, c2.height = 1024, 1024                     # the maximum size
+    c2.crop = None
+    for sc, cfg in ((s1, c1), (s2, c2), (s1, c1)):
+        rc, out, st = _call(sc, cfg)
+        assert rc == abi.LUM_OK, L.lib().lum_last_error()
+        assert np.isfinite(out).all() and st.error_flags == 0
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, f"free device memory moved by {free0 - free1} bytes"
+
+
+def test_noalloc_rejects_adaptive_sampling_and_time_limit():
+    world, cfg = W.box_room(width=32, height=32, spp=16)
+    sc = L.GpuScene(world)
+    cfg.adaptive = True
+    rc, _, _ = _call(sc, cfg)
+    assert rc == abi.LUM_ERR_UNSUPPORTED
+    cfg.adaptive = False
+    cfg.time_limit = 1.0
+    rc, _, _ = _call(sc, cfg)
+    assert rc == abi.LUM_ERR_UNSUPPORTED
