@@ -59,6 +59,8 @@ def parse_args():
     ap.add_argument("--adjoint-spp", type=int, default=64, help="adjoint block: samples per pixel (workload: 64)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-workload block")
     ap.add_argument("--no-sampling", action="store_true", help="skip the adaptive / time-limit block")
+    ap.add_argument("--no-rmse", action="store_true", help="skip the RMSE block (reference-estimator rows)")
+    ap.add_argument("--no-configs", action="store_true", help="skip the box-room / dense-mesh / diff-quads records")
     ap.add_argument("--scenes", type=int, default=64, help="batched workload: number of scenes")
     ap.add_argument("--max-res", type=int, default=1024, help="batched workload: largest resolution")
     ap.add_argument("--batch-config", default="auto", help="batched workload: auto | default | k=v,k=v")
@@ -169,49 +171,50 @@ def measured_peaks():
     return 6650.0, 1965.0, "fallback"
 
 
-def ncu_traffic(kernel="k_render", workload=None):
-    """DRAM bytes per launch recorded in profiles/<kernel>_<workload>.md by the ncu summary."""
-    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
-    if not os.path.exists(path):
-        return None
-    for line in open(path):
-        if line.startswith("dram_bytes_per_full_launch:"):
-            try:
-                return int(float(line.split(":")[1].strip()))
-            except ValueError:
-                return None
-    return None
-
-
 # ------------------------------------------------------------------------------ CPU baseline
-def cpu_sample(world, cfg, target_s, threads=0):
-    """Reference estimator (oracle stream mode) on evenly spaced image rows, sized so the
-    sample takes about target_s seconds.  Returns (paths, seconds, rows, threads)."""
+def spread_rows(h, n, offset=0.5, exclude=()):
+    """n distinct image rows spread evenly over [0, h), not in `exclude`."""
+    ex = set(exclude)
+    rows = []
+    for k in range(n):
+        j = min(h - 1, int((k + offset) * h / max(n, 1)))
+        while j in ex or j in rows:
+            j = (j + 1) % h
+        rows.append(j)
+    return rows
+
+
+def cpu_sample(world, cfg, target_s, threads=0, scene=None):
+    """Reference estimator (oracle stream mode) on image rows spread over the frame, rendered
+    with OpenMP over the row list so that every host thread is busy, sized to take about
+    target_s seconds of wall time.  Returns (paths, wall seconds, rows, threads)."""
     import oracle as O
 
-    sc = O.OracleScene(world)
+    sc = scene or O.OracleScene(world)
+    nt = threads or os.cpu_count() or 1
     h = cfg.height
-    total_paths, total_s, rows = 0, 0.0, []
-    # calibrate on two rows, then choose the row count for the target time
-    probe = [h // 3, (2 * h) // 3]
-    for j in probe:
-        _, st = sc.render(cfg, mode=O.MODE_STREAM, threads=threads, rows=(j, j + 1))
+    rows0 = spread_rows(h, min(h, 2 * nt), 0.25)              # calibration: two rows per thread
+    _, st = sc.render_row_list(cfg, rows0, mode=O.MODE_STREAM, threads=threads)
+    total_paths, total_s, used = st.paths, st.seconds, st.threads
+    n_rows = len(rows0)
+    per_row = st.seconds / len(rows0)
+    n_more = int((target_s - total_s) / max(per_row, 1e-9))
+    n_more = min(h - len(rows0), (n_more // used) * used)   # whole waves of rows
+    if n_more > 0:
+        rows1 = spread_rows(h, n_more, 0.75, exclude=rows0)
+        _, st = sc.render_row_list(cfg, rows1, mode=O.MODE_STREAM, threads=threads)
         total_paths += st.paths
         total_s += st.seconds
-        rows.append(j)
-        used = st.threads
-    per_row = total_s / len(probe)
-    n_more = max(0, int((target_s - total_s) / max(per_row, 1e-6)))
-    n_more = min(n_more, h - len(probe))
-    if n_more > 0:
-        step = h / n_more
-        for k in range(n_more):
-            j = int(k * step + step / 2)
-            _, st = sc.render(cfg, mode=O.MODE_STREAM, threads=threads, rows=(j, j + 1))
-            total_paths += st.paths
-            total_s += st.seconds
-            rows.append(j)
-    return total_paths, total_s, len(rows), used
+        n_rows += len(rows1)
+    return total_paths, total_s, n_rows, used
+
+
+def config_dict(args, cfg):
+    """The workload description shared by both arms' JSON lines."""
+    return {"workload": workload_name(args, cfg), "width": cfg.width, "height": cfg.height, "spp": strata(cfg),
+            "max_depth": cfg.max_depth, "paths_per_step_per_gpu": cfg.width * cfg.height * strata(cfg),
+            "l2": "GPU arm: L2 flushed before every timed step (256 MiB device write inside the timed region)",
+            "parallelism": "one independent frame per GPU (seed offset by rank), no data-path collective"}
 
 
 def run_reference(args):
@@ -219,33 +222,214 @@ def run_reference(args):
     if rank != 0:
         return 0
     world, cfg = workload(args)
+    import oracle as O
+
+    sc = O.OracleScene(world)
     per_step = max(2.0, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
     for _ in range(args.warmup):
-        cpu_sample(world, cfg, per_step / 4)
+        cpu_sample(world, cfg, per_step / 4, scene=sc)
     paths, secs, rows, threads = 0, 0.0, 0, 0
     for _ in range(args.steps):
-        p, s, r, threads = cpu_sample(world, cfg, per_step)
+        p, s, r, threads = cpu_sample(world, cfg, per_step, scene=sc)
         paths += p
         secs += s
         rows += r
     value = paths / secs / 1e6
-    sample = (f"{rows} image rows (evenly spaced, {cfg.width} px x {strata(cfg)} strata each) over {args.steps} "
-              f"steps of at most ~{per_step:.0f} s ({secs:.1f} s of CPU work in all)")
+    sample = (f"{rows} image rows spread over the frame ({cfg.width} px x {strata(cfg)} strata each) over "
+              f"{args.steps} steps of about {per_step:.0f} s ({secs:.1f} s of wall time, {threads} threads, "
+              f"OpenMP over the rows)")
     line = {
         "impl": "reference", "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_name(args, cfg)},
+        "config": config_dict(args, cfg),
         "cpu_baseline": {"value": value, "unit": "Mpaths/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "Rust reference not buildable on this machine (no cargo/rustc); timed its C++ f64 restatement "
-                "(oracle/, the reference's per-row SmallRng estimator) with OpenMP over rows",
+                "(oracle/, the reference's per-row SmallRng estimator) with OpenMP over rows, all host threads",
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
 # ------------------------------------------------------------------------------ our arm
+def profile_figures(kernel="k_render", workload=None):
+    """Figures recorded in profiles/<kernel>_<workload>.md by its ncu summary (lines 'key: value')."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
+    out = {}
+    if not os.path.exists(path):
+        return out
+    for line in open(path):
+        if ":" not in line or line.startswith((" ", "|", "#")):
+            continue
+        k, v = line.split(":", 1)
+        if k in ("dram_bytes_per_full_launch", "issue_active", "simt_lanes_per_inst", "l1_hit_rate", "l2_hit_rate"):
+            try:
+                out[k] = float(v.strip())
+            except ValueError:
+                pass
+    return out
+
+
+def l1_peaks(L):
+    """L1 load throughput of this device (lum_diag_l1_throughput): coalesced and 64-byte gather."""
+    try:
+        return {"coalesced_gbs": L.diag_l1_throughput(0), "gather_gbs": L.diag_l1_throughput(1)}
+    except Exception as e:                              # reported in the line, never fatal
+        return {"error": str(e)}
+
+
+def roofline(counts, avg_kernel_s, l1, workload_key=None):
+    """Roofline of one k_render launch from its counted tests (COST per test).  The algorithmic
+    bytes are node and primitive records, which L1 and L2 serve (ncu: DRAM traffic per launch
+    is ~1e-6 of them on the sphere field), so the bound reported is the L1 gather throughput of
+    64-byte records measured in this run; the HBM and FP32 fractions are given beside it."""
+    flops = sum(getattr(counts, k) * c[0] for k, c in COST.items())
+    nbytes = sum(getattr(counts, k) * c[1] for k, c in COST.items())
+    hbm_peak, sm_max_mhz, peak_kind = measured_peaks()
+    import torch
+
+    props = torch.cuda.get_device_properties(torch.cuda.current_device())
+    fp32_peak = props.multi_processor_count * 128 * 2 * sm_max_mhz * 1e6 / 1e12
+    ach_gbs = nbytes / avg_kernel_s / 1e9
+    ach_tflops = flops / avg_kernel_s / 1e12
+    prof = profile_figures("k_render", workload_key) if workload_key else {}
+    gather = l1.get("gather_gbs")
+    roof = {
+        "kernel": "k_render",
+        "bound": "l1" if gather else "hbm",
+        "achieved": ach_gbs, "unit": "GB/s",
+        "peak": gather if gather else hbm_peak,
+        "frac": ach_gbs / gather if gather else ach_gbs / hbm_peak,
+        "traffic": int(prof["dram_bytes_per_full_launch"]) if "dram_bytes_per_full_launch" in prof else None,
+        "peak_kind": ("L1 gather of 64-byte records, measured in this run (lum_diag_l1_throughput pattern 1); "
+                      "the algorithmic bytes are served from L1/L2, `traffic` is the DRAM bytes of one launch"
+                      if gather else "HBM " + peak_kind),
+        "bytes_per_launch": nbytes, "flops_per_launch": flops,
+        "l1": {**l1, "frac_gather": ach_gbs / gather if gather else None,
+               "frac_coalesced": ach_gbs / l1["coalesced_gbs"] if l1.get("coalesced_gbs") else None,
+               "of": "builder-measured (lum_diag_l1_throughput)"},
+        "hbm": {"achieved_gbs": ach_gbs, "peak_gbs": hbm_peak, "frac": ach_gbs / hbm_peak, "of": peak_kind,
+                "note": "algorithmic bytes against the HBM copy rate; they are served from L1/L2, not DRAM"},
+        "fp32": {"achieved_tflops": ach_tflops, "peak_tflops": fp32_peak, "frac": ach_tflops / fp32_peak,
+                 "of": "nominal (SMs x 128 lanes x 2 x max SM clock)"},
+        "avg_launch_ms": avg_kernel_s * 1e3,
+        "counts_per_launch": {k: int(getattr(counts, k)) for k in
+                              ("node_visits", "sphere_tests", "quad_tests", "triangle_tests", "disk_tests",
+                               "fog_tests", "plane_tests", "segments", "shadow_rays", "paths")},
+    }
+    if "issue_active" in prof:
+        roof["issue"] = {"issue_active": prof["issue_active"], "simt_lanes_per_inst": prof.get("simt_lanes_per_inst"),
+                         "of": f"ncu, small case of the same kernel (profiles/k_render_{workload_key}.md)"}
+    return roof
+
+
+def time_frames(sc, cfg, out, flush, stream, steps, warmup, barrier=lambda: None):
+    """Warm-up steps are timed steps: the same flush, events and enqueue-only renders, so lazily
+    loaded kernel modules (torch's fill kernel) and first-call host work stay out of the timed
+    region.  A checked render before and after the timed steps supplies the segment counts and
+    confirms no kernel error flags.  The timed steps are enqueued back to back (render_device
+    without waiting), each bracketed by CUDA events on the launching stream for the kernel's own
+    time.  Returns (timed-region seconds, per-step kernel ms, checked stats)."""
+    import torch
+
+    for _ in range(warmup):
+        w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.zero_()
+        w0.record(stream)
+        sc.render_device(cfg, out.data_ptr(), stream.cuda_stream, wait=False)
+        w1.record(stream)
+    torch.cuda.synchronize()
+    st0 = sc.render_device(cfg, out.data_ptr(), stream.cuda_stream)
+    assert st0.error_flags == 0
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    step_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    ev0.record(stream)
+    for k in range(steps):
+        flush.zero_()
+        step_ev[k][0].record(stream)
+        sc.render_device(cfg, out.data_ptr(), stream.cuda_stream, wait=False)
+        step_ev[k][1].record(stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    st1 = sc.render_device(cfg, out.data_ptr(), stream.cuda_stream)      # the last frame's flags
+    assert st1.error_flags == 0 and st1.segments == st0.segments
+    return ev0.elapsed_time(ev1) / 1e3, [a.elapsed_time(b) for a, b in step_ev], st0
+
+
+def rmse_block(world, cfg, out, rate_mpaths, target_s=25.0, ref_spp=4096):
+    """Per-pixel RMSE of the device frame against the reference estimator (oracle stream mode)
+    at ref_spp samples per pixel, on rows spread over the frame, beside the RMSE of an
+    independent reference-estimator render at the frame's own spp (another seed) against the same
+    high-spp rows: equal RMSE at equal spp is what 'at matched RMSE' asks.  Also the mean
+    luminance difference in standard errors."""
+    from dataclasses import replace
+
+    import numpy as np
+
+    import oracle as O
+
+    sc = O.OracleScene(world)
+    per_row_paths = cfg.width * ref_spp
+    n_rows = int(max(4, min(32, rate_mpaths * 1e6 * target_s / per_row_paths)))
+    rows = spread_rows(cfg.height, n_rows, 0.5)
+    t0 = time.perf_counter()
+    ref, _ = sc.render_row_list(replace(cfg, samples_per_pixel=ref_spp, seed=cfg.seed + 1000003), rows)
+    cpu, _ = sc.render_row_list(replace(cfg, seed=cfg.seed + 2000003), rows)
+    secs = time.perf_counter() - t0
+    gpu = out[rows].float().cpu().numpy().astype(np.float64)
+    rm = lambda a: float(np.sqrt(np.mean((a - ref) ** 2)))
+    lum = lambda a: 0.2126 * a[..., 0] + 0.7152 * a[..., 1] + 0.0722 * a[..., 2]
+    d = (lum(gpu) - lum(ref)).ravel()
+    dc = (lum(cpu) - lum(ref)).ravel()
+    return {"rmse": rm(gpu), "rmse_cpu_same_spp": rm(cpu), "ratio": rm(gpu) / max(rm(cpu), 1e-30),
+            "mean_lum_bias_z": float(d.mean() / (d.std(ddof=1) / np.sqrt(d.size))),
+            "mean_lum_bias_z_cpu": float(dc.mean() / (dc.std(ddof=1) / np.sqrt(dc.size))),
+            "reference": f"oracle stream mode (the reference's estimator, f64) at {ref_spp} spp",
+            "rows": rows, "pixels": len(rows) * cfg.width, "cpu_seconds": secs}
+
+
+def config_record(L, name, flush, stream, l1, steps=5, warmup=3, cpu_s=4.0):
+    """One of the other configurations (box room, dense mesh, differentiable quads): the same
+    frame timing, roofline and CPU baseline as the headline, at the configuration's own size."""
+    import torch
+
+    from luminara_b200 import workloads as W
+
+    world, cfg = W.CONFIGS[name]()
+    t0 = time.perf_counter()
+    sc = L.GpuScene(world)
+    build_s = time.perf_counter() - t0
+    info = sc.info()
+    H, Wd = cfg.out_shape()[:2]
+    out = torch.empty((H, Wd, 3), dtype=torch.float32, device="cuda")
+    counts = sc.count_tests(cfg)
+    region_s, kernel_ms, st0 = time_frames(sc, cfg, out, flush, stream, steps, warmup)
+    paths = H * Wd * strata(cfg)
+    rec = {"workload": f"{name} {cfg.width}x{cfg.height} {cfg.samples_per_pixel}spp ({strata(cfg)} strata) "
+                       f"depth {cfg.max_depth}",
+           "value": paths * steps / region_s / 1e6, "unit": "Mpaths/s", "ms_per_step": region_s * 1e3 / steps,
+           "steps": steps, "warmup": warmup, "paths_per_step": paths,
+           "mrays_per_s": (st0.segments + st0.shadow_rays) * steps / region_s / 1e6,
+           "prims": info["prims"], "bvh_nodes": info["nodes"], "scene_build_s": build_s,
+           "roofline": roofline(counts, statistics.mean(kernel_ms) / 1e3, l1, name)}
+    import oracle as O
+
+    t1 = time.perf_counter()
+    osc = O.OracleScene(world)
+    oracle_build = time.perf_counter() - t1
+    p, s_, rows, threads = cpu_sample(world, cfg, cpu_s, scene=osc)
+    rec["cpu_baseline"] = {"value": p / s_ / 1e6, "unit": "Mpaths/s", "cores": threads, "kind": "port",
+                           "sample": f"{rows} rows spread over the frame ({p} paths, {s_:.1f} s wall, OpenMP over "
+                                     f"rows; oracle scene + BVH build {oracle_build:.1f} s not timed)"}
+    sc.close()
+    return rec
+
+
 def run_ours(args):
     import torch
 
@@ -290,82 +474,22 @@ def run_ours(args):
     # scene's stream, and the events below must be on the stream the renders run on
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
+    l1 = l1_peaks(L)
 
     t1 = time.perf_counter()
     counts = sc.count_tests(cfg)                   # counter build, same seeds (not timed)
     t2 = time.perf_counter()
     clocks = ClockSampler(dev)
     clocks.start()
-    # warm-up steps are timed steps: the same flush, events and enqueue-only renders, so lazily
-    # loaded kernel modules (torch's fill kernel) and first-call host work stay out of the timed
-    # region
-    for _ in range(args.warmup):
-        w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        flush.zero_()
-        w0.record(stream)
-        sc.render_device(cfg, out.data_ptr(), stream.cuda_stream, wait=False)
-        w1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    torch.cuda.synchronize()
-    log(f"scene build {build_s:.3f}s, counter build {t2 - t1:.3f}s, warmup {time.perf_counter() - t2:.3f}s")
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    # Every step renders the same frame (same seeds): its traced segment and shadow-ray counts,
-    # and the absence of kernel error flags, are those of a checked render outside the timed
-    # region.  The timed steps are enqueued back to back (render_device without waiting), each
-    # bracketed by CUDA events on the launching stream for the kernel's own time.
-    st0 = sc.render_device(cfg, out.data_ptr(), stream.cuda_stream)
-    assert st0.error_flags == 0
-    torch.cuda.synchronize()
-    step_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    ev0.record(stream)
-    for k in range(args.steps):
-        flush.zero_()
-        step_ev[k][0].record(stream)
-        sc.render_device(cfg, out.data_ptr(), stream.cuda_stream, wait=False)
-        step_ev[k][1].record(stream)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
+    region_s, kernel_ms, st0 = time_frames(sc, cfg, out, flush, stream, args.steps, args.warmup, barrier)
     clock_info = clocks.stop()
-    st_check = sc.render_device(cfg, out.data_ptr(), stream.cuda_stream)      # the last frame's flags
-    assert st_check.error_flags == 0 and st_check.segments == st0.segments
-    kernel_ms = [a.elapsed_time(b) for a, b in step_ev]
+    log(f"scene build {build_s:.3f}s, counter build {t2 - t1:.3f}s, frames {time.perf_counter() - t2:.3f}s")
     segs, shadows = st0.segments * args.steps, st0.shadow_rays * args.steps
-    region_s = allmax(ev0.elapsed_time(ev1) / 1e3)
+    region_s = allmax(region_s)
     value = world_size * paths_per_step * args.steps / region_s / 1e6
     avg_kernel_s = statistics.mean(kernel_ms) / 1e3
-
-    # roofline of the dominant kernel (k_render) from the counted tests of one launch
-    flops = sum(getattr(counts, k) * c[0] for k, c in COST.items())
-    nbytes = sum(getattr(counts, k) * c[1] for k, c in COST.items())
-    hbm_peak, sm_max_mhz, peak_kind = measured_peaks()
-    props = torch.cuda.get_device_properties(dev)
-    fp32_peak_tflops = props.multi_processor_count * 128 * 2 * sm_max_mhz * 1e6 / 1e12
-    ach_gbs = nbytes / avg_kernel_s / 1e9
-    ach_tflops = flops / avg_kernel_s / 1e12
-    frac_b, frac_f = ach_gbs / hbm_peak, ach_tflops / fp32_peak_tflops
-    traffic = ncu_traffic("k_render", args.config) if (not args.width and not args.spp) else None
-    roof = {
-        "kernel": "k_render",
-        "bound": "hbm" if frac_b >= frac_f else "fp32",
-        "achieved": ach_gbs if frac_b >= frac_f else ach_tflops,
-        "peak": hbm_peak if frac_b >= frac_f else fp32_peak_tflops,
-        "unit": "GB/s" if frac_b >= frac_f else "TFLOP/s",
-        "frac": max(frac_b, frac_f),
-        "traffic": traffic,
-        "peak_kind": ((f"HBM measured (MEASURED_PEAKS.json)" if peak_kind == "measured" else
-                       "HBM fallback 6650 GB/s (no MEASURED_PEAKS.json)") if frac_b >= frac_f else
-                      "FP32 nominal: SMs x 128 lanes x 2 x max SM clock (no measured FP32 peak available)"),
-        "bytes_per_launch": nbytes, "flops_per_launch": flops,
-        "hbm": {"achieved_gbs": ach_gbs, "peak_gbs": hbm_peak, "frac": frac_b, "of": peak_kind},
-        "fp32": {"achieved_tflops": ach_tflops, "peak_tflops": fp32_peak_tflops, "frac": frac_f, "of": "nominal"},
-        "avg_launch_ms": avg_kernel_s * 1e3,
-        "counts_per_launch": {k: int(getattr(counts, k)) for k in
-                              ("node_visits", "sphere_tests", "quad_tests", "triangle_tests", "disk_tests",
-                               "fog_tests", "plane_tests", "segments", "shadow_rays", "paths")},
-    }
+    default_frame = not args.width and not args.height and not args.spp and not args.depth
+    roof = roofline(counts, avg_kernel_s, l1, args.config if default_frame else None)
 
     # end to end through the public C ABI with host buffers: scene upload + render + readback
     e2e = None
@@ -399,24 +523,32 @@ def run_ours(args):
                              enumerate(("scene_create", "render", "scene_destroy", "render_kernel"))},
                "step_ms": [round(1e3 * sum(ph[:3]), 2) for ph in phases]}
 
+    solo = rank == 0 and world_size == 1
     cpu = None
-    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+    if solo and not args.no_cpu_baseline:
         p, s, rows, threads = cpu_sample(world, cfg, args.cpu_seconds)
         cpu = {"value": p / s / 1e6, "unit": "Mpaths/s", "cores": threads, "kind": "port",
-               "sample": f"{rows} evenly spaced rows of the same frame ({rows * Wd * strata(cfg)} paths, {s:.1f} s), "
-                         f"reference estimator restated in C++ f64 (oracle/, stream RNG), OpenMP over rows"}
-
+               "sample": f"{rows} rows spread over the same frame ({p} paths, {s:.1f} s wall), reference estimator "
+                         f"restated in C++ f64 (oracle/, stream RNG), OpenMP over the rows"}
+    rmse = None
+    if solo and not args.no_rmse and default_frame:
+        rmse = rmse_block(world, cfg, out, cpu["value"] if cpu else 1.0)
+    hbm_peak = measured_peaks()[0]
     tone = tonemap_block(L, out, H, Wd, stream, hbm_peak, flush) if rank == 0 else None
-    sampling = (sampling_block(L, sc, cfg, out, stream)
-                if (rank == 0 and world_size == 1 and not args.no_sampling) else None)
-    adjoint = (adjoint_block(L, args.adjoint_res, args.adjoint_spp)
-               if (rank == 0 and world_size == 1 and not args.no_adjoint) else None)
+    sampling = sampling_block(L, sc, cfg, out, stream) if (solo and not args.no_sampling) else None
+    others = None
+    if solo and not args.no_configs and default_frame:
+        others = {}
+        for name in ("box_room", "dense_mesh", "diff_quads"):
+            if name != args.config:
+                others[name] = config_record(L, name, flush, stream, l1)
+    adjoint = adjoint_block(L, args.adjoint_res, args.adjoint_spp) if (solo and not args.no_adjoint) else None
     batched = None
-    if rank == 0 and world_size == 1 and not args.no_batched:
+    if solo and not args.no_batched:
         b = batched_measure(args, 2, 3, with_clocks=False)
         batched = {k: b[k] for k in ("value", "unit", "ms_per_step", "batch_mode", "sequential_megakernel",
                                      "speedup_vs_sequential", "max_rel_diff_vs_megakernel", "autotune",
-                                     "scene_done_ms")}
+                                     "scene_done_ms", "modes")}
         batched["workload"] = b["config"]["workload"]
 
     if rank == 0:
@@ -424,16 +556,14 @@ def run_ours(args):
             "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": world_size, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": region_s * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
-            "config": {"workload": workload_name(args, cfg), "width": cfg.width, "height": cfg.height,
-                       "spp": strata(cfg), "max_depth": cfg.max_depth, "paths_per_step_per_gpu": paths_per_step,
-                       "prims": info["prims"], "bvh_nodes": info["nodes"], "scene_build_s": build_s,
-                       "l2": "L2 flushed before every timed step (256 MiB device write inside the timed region)",
-                       "parallelism": "one independent frame per GPU (seed offset by rank), no data-path collective"},
+            "config": config_dict(args, cfg),
+            "scene": {"prims": info["prims"], "bvh_nodes": info["nodes"], "scene_build_s": build_s},
             "mrays_per_s": world_size * (segs + shadows) / region_s / 1e6,
             "segments_per_path": segs / (paths_per_step * args.steps),
             "shadow_rays_per_path": shadows / (paths_per_step * args.steps),
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps,
-            "clocks": clock_info, "tonemap": tone, "sampling": sampling, "adjoint": adjoint, "batched": batched,
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "rmse": rmse, "gpu_launches": args.steps,
+            "clocks": clock_info, "configs": others, "tonemap": tone, "sampling": sampling, "adjoint": adjoint,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -608,6 +738,24 @@ def batched_measure(args, steps, warmup, with_clocks=True):
     clock_info = clocks.stop() if clocks else None
     max_rel = max(float(((a - b).abs() / (b.abs() + 1e-3)).max()) for a, b in zip(outs, seq_imgs))
     value = paths * steps / bat_s / 1e6
+    batch_mode = {0: "wavefront", 1: "megakernel", 2: "streams"}[batch.config().get("mode")]
+    batch.close()
+    # each batch mode on its own (default configuration otherwise), the same images
+    modes = {}
+    for m, mname in ((0, "wavefront"), (1, "megakernel"), (2, "streams")):
+        bm = L.Batch(scenes, cfgs, config={"mode": m})
+        bm.render_device([o.data_ptr() for o in outs])
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(steps):
+            bm.render_device([o.data_ptr() for o in outs])
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        m_s = ev0.elapsed_time(ev1) / 1e3
+        same = all(torch.equal(a, b) for a, b in zip(outs, seq_imgs))
+        modes[mname] = {"value": paths * steps / m_s / 1e6, "ms_per_step": m_s * 1e3 / steps,
+                        "speedup_vs_sequential": seq_s / m_s, "config": bm.config(), "images_equal": same}
+        bm.close()
     done_ms = done_all[-1]
     line = {
         "metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": 1, "steps": steps,
@@ -616,7 +764,7 @@ def batched_measure(args, steps, warmup, with_clocks=True):
         "config": {"workload": f"batched: {len(cfgs)} uneven scenes, {paths} paths per step",
                    "scenes": len(cfgs), "prims": sum(w.n_prims() for w, _ in items),
                    "l2": "working set of the batch exceeds L2 (pool, queues, 64 scenes)"},
-        "batch_mode": {0: "wavefront", 1: "megakernel", 2: "streams"}[batch.config().get("mode")],
+        "batch_mode": batch_mode,
         "sequential_megakernel": {"value": paths * steps / seq_s / 1e6, "unit": "Mpaths/s",
                                   "ms_per_step": seq_s * 1e3 / steps},
         "speedup_vs_sequential": seq_s / bat_s,
@@ -624,9 +772,8 @@ def batched_measure(args, steps, warmup, with_clocks=True):
         "autotune": {"config": tuned, "best_ms": tune_ms, "seconds": tune_s},
         "scene_done_ms": {"min": min(done_ms), "median": statistics.median(done_ms), "max": max(done_ms)},
         "iterations": bstats[-1].iterations, "graph_launches": bstats[-1].graph_launches,
-        "gpu_launches": None, "clocks": clock_info,
+        "modes": modes, "gpu_launches": None, "clocks": clock_info,
     }
-    batch.close()
     return line
 
 

@@ -559,6 +559,18 @@ lum_status lum_tonemap_device(const float* d_hdr_rgb, uint32_t width, uint32_t h
 lum_status lum_render_ldr(lum_scene* scene, const lum_render_params* params, const lum_tonemap_params* tm,
                           uint8_t* out_rgba, lum_stats* stats);
 
+/* ------------------------------------------------------------------------------------
+ * Diagnostics
+ * ---------------------------------------------------------------------------------- */
+
+/* L1 load throughput of the current device in GB/s, the roof of the megakernel's node and
+ * primitive fetches (which L1 and L2 serve; DRAM sees almost none of them): 128-bit loads from
+ * a 32 KiB table by every SM at full occupancy, independent loads only.  pattern 0: coalesced
+ * (512 contiguous bytes per warp load); pattern 1: each lane one 64-byte record at a hashed
+ * index, as a BVH node visit reads.  Allocates and frees its own small buffers and
+ * synchronises the device.  No counterpart in the reference. */
+lum_status lum_diag_l1_throughput(int32_t pattern, double* gbs);
+
 #ifdef __cplusplus
 }
 #endif

@@ -91,7 +91,7 @@ def lib():
                  "lum_tonemap_device", "lum_render_ldr", "lum_scene_set_envmap", "lum_render_aov",
                  "lum_batch_default_config",
                  "lum_batch_autotune", "lum_batch_create", "lum_batch_config_of", "lum_batch_render",
-                 "lum_batch_render_device", "lum_batch_destroy"):
+                 "lum_batch_render_device", "lum_batch_destroy", "lum_diag_l1_throughput"):
         getattr(L, name).restype = C.c_int32
     if L.lum_abi_version() != abi.LUM_ABI_VERSION:
         raise ImportError("libluminara_b200.so ABI version mismatch")
@@ -284,6 +284,14 @@ class Batch:
             self.h = None
 
     __del__ = close
+
+
+def diag_l1_throughput(pattern: int = 0) -> float:
+    """lum_diag_l1_throughput: the device's L1 load throughput in GB/s (pattern 0 coalesced,
+    1 gather of 64-byte records), the roof of the megakernel's node and primitive fetches."""
+    v = C.c_double()
+    check(lib().lum_diag_l1_throughput(int(pattern), C.byref(v)))
+    return v.value
 
 
 def autotune(scenes, configs):

@@ -65,6 +65,8 @@ def lib():
         L.orc_render_aov.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.c_int, vp, vp, vp]
         L.orc_render_rows.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.c_int, C.c_int, C.c_uint32,
                                       C.c_uint32, dp, C.POINTER(OrcStats)]
+        L.orc_render_row_list.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.c_int, C.c_int, vp, C.c_uint32,
+                                          dp, C.POINTER(OrcStats)]
         L.orc_adjoint.argtypes = [vp, C.POINTER(abi.LumRenderParams), dp, vp, C.c_int, C.c_int, dp, dp, dp, dp]
         L.orc_adjoint_dir.argtypes = [vp, C.POINTER(abi.LumRenderParams), dp, vp, C.c_int, C.c_int, dp, dp]
         L.orc_scatter.argtypes = [C.POINTER(abi.LumMaterial), dp, dp, dp, C.c_double, C.c_double, C.c_double,
@@ -156,6 +158,20 @@ class OracleScene:
                                        out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(st))
         if rc != 0:
             raise RuntimeError(f"orc_render failed: {rc}")
+        return out, st
+
+    def render_row_list(self, cfg, rows, mode=MODE_STREAM, threads=0):
+        """Renders the image rows `rows` (OpenMP over the list); returns (array (len(rows), W, 3)
+        with row k = image row rows[k], stats)."""
+        p = cfg.to_c()
+        r = np.ascontiguousarray(rows, dtype=np.uint32)
+        w = cfg.out_shape()[1]
+        out = np.zeros((len(r), w, 3), dtype=np.float64)
+        st = OrcStats()
+        rc = lib().orc_render_row_list(self.h, C.byref(p), mode, threads, r.ctypes.data, len(r),
+                                       out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(st))
+        if rc != 0:
+            raise RuntimeError(f"orc_render_row_list failed: {rc}")
         return out, st
 
     def set_envmap(self, rgb):

@@ -1900,8 +1900,11 @@ namespace {
 
 // The sample loop of render.rs:1598-1706.  expire: 0 = the wall-clock time limit of the
 // params (checked when a row starts, render.rs:1601-1605), 1 = every row starts after it.
+// row_list (n_list entries, output row index = position in the list) renders an arbitrary set
+// of rows in parallel instead of the range [row_begin, row_end).
 int render_rows(const orc_scene* sc, const lum_render_params* pp, int mode, int threads, uint32_t row_begin,
-                uint32_t row_end, double* out, orc_stats* stats, int expire) {
+                uint32_t row_end, double* out, orc_stats* stats, int expire, const uint32_t* row_list = nullptr,
+                uint32_t n_list = 0) {
     if (!sc || !pp || !out) return 1;
     const lum_render_params& p = *pp;
     Frame f = frame_of(p);
@@ -1912,6 +1915,12 @@ int render_rows(const orc_scene* sc, const lum_render_params* pp, int mode, int 
     const uint32_t min_samples = p.adaptive ? std::max<uint32_t>(actual_spp / 4, 16) : 0;
     std::atomic<bool> expired{expire != 0};
     row_end = std::min<uint32_t>(row_end, (uint32_t)f.h);
+    if (row_list) {
+        for (uint32_t k = 0; k < n_list; ++k)
+            if (row_list[k] >= (uint32_t)f.h) return 4;
+        row_begin = 0;
+        row_end = n_list;
+    }
     uint64_t segs = 0, shadows = 0, paths = 0;
     auto t0 = std::chrono::steady_clock::now();
 #ifdef _OPENMP
@@ -1920,8 +1929,9 @@ int render_rows(const orc_scene* sc, const lum_render_params* pp, int mode, int 
     int nt = 1;
 #endif
 #pragma omp parallel for schedule(dynamic, 1) num_threads(nt) reduction(+ : segs, shadows, paths)
-    for (int64_t j = row_begin; j < (int64_t)row_end; ++j) {
-        size_t gj = (size_t)j + f.crop_y;
+    for (int64_t k = row_begin; k < (int64_t)row_end; ++k) {
+        const int64_t j = k;                                            // output row
+        size_t gj = (size_t)(row_list ? row_list[k] : k) + f.crop_y;
         Xoshiro rng((uint64_t)gj * p.seed);                             // render.rs:1608 (wrapping)
         Sampler s;
         s.mode = mode;
@@ -1993,6 +2003,12 @@ extern "C" {
 int orc_render_rows(const orc_scene* sc, const lum_render_params* pp, int mode, int threads, uint32_t row_begin,
                     uint32_t row_end, double* out, orc_stats* stats) {
     return render_rows(sc, pp, mode, threads, row_begin, row_end, out, stats, 0);
+}
+
+int orc_render_row_list(const orc_scene* sc, const lum_render_params* pp, int mode, int threads,
+                        const uint32_t* rows, uint32_t n_rows, double* out, orc_stats* stats) {
+    if (!rows && n_rows) return 1;
+    return render_rows(sc, pp, mode, threads, 0, 0, out, stats, 0, rows, n_rows);
 }
 
 int orc_render(const orc_scene* sc, const lum_render_params* p, int mode, int threads, double* out, orc_stats* st) {

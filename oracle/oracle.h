@@ -76,6 +76,11 @@ int orc_render_expired(const orc_scene* s, const lum_render_params* p, int mode,
  * same index; used for bounded CPU-baseline samples. */
 int orc_render_rows(const orc_scene* s, const lum_render_params* p, int mode, int threads,
                     uint32_t row_begin, uint32_t row_end, double* out_rgb, orc_stats* stats);
+/* Renders the image rows rows[0..n_rows) (any order, OpenMP over the list) into out_rgb, row k of
+ * the output holding image row rows[k]: a bounded sample of a frame spread over its height that
+ * still keeps every host thread busy. */
+int orc_render_row_list(const orc_scene* s, const lum_render_params* p, int mode, int threads,
+                        const uint32_t* rows, uint32_t n_rows, double* out_rgb, orc_stats* stats);
 
 /* Environment map of LUM_BG_ENVMAP: width*height*3 floats, top row first (NULL removes it). */
 int orc_scene_set_envmap(orc_scene* s, const float* rgb, uint32_t width, uint32_t height);

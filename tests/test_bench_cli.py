@@ -34,3 +34,32 @@ def test_reference_arm_other_ranks_do_no_work():
     lines = run_bench(["--impl", "reference", "--steps", "1", "--warmup", "1", "--width", "48", "--height", "27",
                        "--spp", "4"], {"RANK": "1", "WORLD_SIZE": "2"})
     assert lines == []
+
+
+def test_reference_arm_config_matches_our_arm():
+    """Both arms print the same config dict for the same workload (built by one function)."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    lines = run_bench(["--impl", "reference", "--steps", "1", "--warmup", "1", "--width", "48", "--height", "27",
+                       "--spp", "4"])
+    d = json.loads(lines[0])
+    assert set(d["config"]) == {"workload", "width", "height", "spp", "max_depth", "paths_per_step_per_gpu", "l2",
+                                "parallelism"}
+    assert d["config"]["width"] == 48 and d["config"]["spp"] == 4 and d["config"]["paths_per_step_per_gpu"] == 48 * 27 * 4
+
+
+def test_cpu_sample_spreads_rows_and_uses_every_thread():
+    """The CPU baseline renders a list of rows spread over the frame with OpenMP over the list,
+    so all host threads work (one row per call would keep a single thread busy)."""
+    sys.path.insert(0, ROOT)
+    import bench
+    from luminara_b200 import workloads as W
+
+    rows = bench.spread_rows(100, 10, 0.25)
+    assert len(set(rows)) == 10 and all(0 <= r < 100 for r in rows)
+    more = bench.spread_rows(100, 10, 0.75, exclude=rows)
+    assert not set(rows) & set(more)
+    world, cfg = W.random_spheres(width=64, height=36, spp=4)
+    paths, secs, n_rows, threads = bench.cpu_sample(world, cfg, 0.5, threads=4)
+    assert threads == 4 and n_rows >= 8 and paths == n_rows * 64 * 4 and secs > 0
