@@ -350,6 +350,26 @@ lum_status lum_render(lum_scene* scene, const lum_render_params* params, float* 
 lum_status lum_render_device(lum_scene* scene, const lum_render_params* params,
                              float* d_out_rgb, void* stream, lum_stats* stats);
 
+/* The render's raw per-pixel sums, before the division of render.rs:1705, into a caller-owned
+ * DEVICE buffer of width*height*4 int64 values (crop size when has_crop) on `stream` (NULL =
+ * the scene's stream): for each pixel the sums over its rendered strata of the filter-weighted,
+ * luminance-clamped radiance (R, G, B) and of the filter weight (render.rs:1692-1704), in fixed
+ * point with 2^-32 units, each path's value rounded once.  Sums of disjoint stratum ranges
+ * (sample_begin / sample_count) add exactly, so a frame split across devices or calls combines
+ * with one integer sum (an all-reduce) and lum_sums_finalize_device then gives the
+ * single-device lum_render image bit for bit, for every pixel filter.  Adaptive sampling and
+ * the time limit return LUM_ERR_UNSUPPORTED.  With stats the call waits and reports error flags;
+ * with stats NULL it only enqueues. */
+lum_status lum_render_sums_device(lum_scene* scene, const lum_render_params* params, int64_t* d_sums,
+                                  void* stream, lum_stats* stats);
+
+/* Pixels of raw sums (lum_render_sums_device, possibly summed over several calls): for each of
+ * width*height pixels, rgb = (sum_rgb / sum_w) * exposure (sum_rgb itself where sum_w is 0), as
+ * float32 linear RGB into a DEVICE buffer, on `stream` (NULL = the default stream).  Allocates
+ * nothing; does not synchronise. */
+lum_status lum_sums_finalize_device(const int64_t* d_sums, uint32_t width, uint32_t height, double exposure,
+                                    float* d_rgb, void* stream);
+
 /* Environment map of LUM_BG_ENVMAP (Background::EnvMap, src/render.rs:113-151): an
  * equirectangular linear RGB image, width*height*3 floats, top row first, copied to the
  * scene's device memory (replacing any previous map; rgb NULL removes it). */

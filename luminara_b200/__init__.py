@@ -91,7 +91,8 @@ def lib():
                  "lum_tonemap_device", "lum_render_ldr", "lum_scene_set_envmap", "lum_render_aov",
                  "lum_batch_default_config",
                  "lum_batch_autotune", "lum_batch_create", "lum_batch_config_of", "lum_batch_render",
-                 "lum_batch_render_device", "lum_batch_destroy", "lum_diag_l1_throughput"):
+                 "lum_batch_render_device", "lum_batch_destroy", "lum_diag_l1_throughput",
+                 "lum_render_sums_device", "lum_sums_finalize_device"):
         getattr(L, name).restype = C.c_int32
     if L.lum_abi_version() != abi.LUM_ABI_VERSION:
         raise ImportError("libluminara_b200.so ABI version mismatch")
@@ -149,6 +150,15 @@ class GpuScene:
             return None
         st = abi.LumStats()
         check(lib().lum_render_device(self.h, C.byref(p), C.c_void_p(d_out), C.c_void_p(stream), C.byref(st)))
+        return st
+
+    def render_sums_device(self, cfg: RenderConfig, d_sums: int, stream: int = 0):
+        """lum_render_sums_device: the raw per-pixel fixed-point sums (H, W, 4) int64 into a
+        caller-owned device buffer (pointer as int); waits and returns the stats."""
+        p = cfg.to_c()
+        st = abi.LumStats()
+        check(lib().lum_render_sums_device(self.h, C.byref(p), C.c_void_p(d_sums), C.c_void_p(stream),
+                                           C.byref(st)))
         return st
 
     def set_envmap(self, rgb: Optional[np.ndarray]):
@@ -284,6 +294,12 @@ class Batch:
             self.h = None
 
     __del__ = close
+
+
+def sums_finalize_device(d_sums: int, width: int, height: int, exposure: float, d_rgb: int, stream: int = 0):
+    """lum_sums_finalize_device: pixels of (summed) raw sums, device to device."""
+    check(lib().lum_sums_finalize_device(C.c_void_p(d_sums), int(width), int(height), C.c_double(exposure),
+                                         C.c_void_p(d_rgb), C.c_void_p(stream)))
 
 
 def diag_l1_throughput(pattern: int = 0) -> float:

@@ -983,6 +983,55 @@ lum_status lum_render_device(lum_scene* s, const lum_render_params* params, floa
     return run_render(s, params, d_out, cs, stats, stats != nullptr);
 }
 
+lum_status lum_render_sums_device(lum_scene* s, const lum_render_params* params, int64_t* d_sums, void* stream,
+                                  lum_stats* stats) {
+    if (!s || !d_sums) return fail(LUM_ERR_INVALID_ARGUMENT, "null argument");
+    lum_status st = check_params(params);
+    if (st != LUM_OK) return st;
+    if (sampled(*params))
+        return fail(LUM_ERR_UNSUPPORTED, "raw sums are not defined for adaptive sampling or the time limit");
+    std::lock_guard<std::mutex> lk(s->mu);
+    CU(cudaSetDevice(s->device), "cudaSetDevice");
+    cudaStream_t cs = stream ? (cudaStream_t)stream : s->stream;
+    lum::RenderDev R;
+    st = make_render_dev(s, *params, R);
+    if (st != LUM_OK) return st;
+    auto t0 = std::chrono::steady_clock::now();
+    auto* sums = reinterpret_cast<unsigned long long*>(d_sums);
+    CU(cudaMemsetAsync(s->d_work, 0, sizeof(lum::WorkCounters), cs), "cudaMemsetAsync");
+    CU(cudaEventRecord(s->ev0, cs), "cudaEventRecord");
+    if (R.n_tasks > 0 && R.s_end > R.s_begin) {
+        CU(lum::launch_render_sums(s->dev, R, sums, s->d_work, cs), "render launch");
+    } else if (R.w > 0 && R.h > 0) {
+        CU(cudaMemsetAsync(sums, 0, 32 * (size_t)R.w * R.h, cs), "cudaMemsetAsync");
+    }
+    CU(cudaEventRecord(s->ev1, cs), "cudaEventRecord");
+    if (!stats) return LUM_OK;
+    lum::WorkCounters wc{};
+    CU(cudaMemcpyAsync(&wc, s->d_work, sizeof wc, cudaMemcpyDeviceToHost, cs), "cudaMemcpyAsync");
+    CU(cudaStreamSynchronize(cs), "render");
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+    stats->paths = (uint64_t)R.w * R.h * (R.s_end - R.s_begin);
+    stats->segments = wc.segments;
+    stats->shadow_rays = wc.shadow_rays;
+    stats->kernel_ms = ms;
+    stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    stats->error_flags = wc.error_flags;
+    if (wc.error_flags) return fail(LUM_ERR_KERNEL, "render kernel reported error flags 0x%x", wc.error_flags);
+    return LUM_OK;
+}
+
+lum_status lum_sums_finalize_device(const int64_t* d_sums, uint32_t width, uint32_t height, double exposure,
+                                    float* d_rgb, void* stream) {
+    if ((!d_sums || !d_rgb) && (uint64_t)width * height > 0) return fail(LUM_ERR_INVALID_ARGUMENT, "null argument");
+    if (!std::isfinite(exposure)) return fail(LUM_ERR_INVALID_ARGUMENT, "exposure is not finite");
+    CU(lum::launch_fixed_finalize(reinterpret_cast<const unsigned long long*>(d_sums), (size_t)width * height,
+                                  (float)exposure, d_rgb, (cudaStream_t)stream),
+       "finalize launch");
+    return LUM_OK;
+}
+
 lum_status lum_scene_set_envmap(lum_scene* s, const float* rgb, uint32_t width, uint32_t height) {
     if (!s) return fail(LUM_ERR_INVALID_ARGUMENT, "scene is null");
     if (rgb && (width == 0 || height == 0)) return fail(LUM_ERR_INVALID_ARGUMENT, "empty environment map");

@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(kRenderThreads, SPH ? (NEE ? 6 : 7) : LUM_REND
         if (lane < (int)(tw * th)) {
             const uint32_t i = x0 + lane % tw, j = y0 + lane / tw;
             const unsigned long long* a = s_acc[wid][lane];
-            if (n_groups > 1) {
+            if (gacc) {                   // grouped frames and raw-sum renders
                 unsigned long long* g = gacc + 4 * ((size_t)j * R.w + i);
                 for (int c = 0; c < 4; ++c) atomicAdd(g + c, a[c]);
             } else {
@@ -260,14 +260,18 @@ RenderGroups render_groups(const RenderDev& R) {
     return g;
 }
 
+// sums_only: the launch leaves the frame's fixed-point sums in gacc (zeroed first) and writes no
+// pixels.  Otherwise gacc is non-null only for a grouped frame (n_groups > 1).
 template <bool COUNT>
 static cudaError_t launch_render_t(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
-                                   cudaStream_t stream, int blocks_per_sm, unsigned long long* gacc, RenderGroups grp) {
+                                   cudaStream_t stream, int blocks_per_sm, unsigned long long* gacc, RenderGroups grp,
+                                   bool sums_only = false) {
     const int occ = render_occupancy();
     if (blocks_per_sm <= 0) blocks_per_sm = occ;
     if (!gacc || grp.n_groups < 1) grp = RenderGroups{1, R.s_end > R.s_begin ? R.s_end - R.s_begin : 0};
+    if (!sums_only && grp.n_groups <= 1) gacc = nullptr;
     const size_t n_px = (size_t)R.w * R.h;
-    if (grp.n_groups > 1) {
+    if (gacc) {
         cudaError_t e = cudaMemsetAsync(gacc, 0, 32 * n_px, stream);
         if (e != cudaSuccess) return e;
     }
@@ -289,9 +293,22 @@ static cudaError_t launch_render_t(const SceneDev& S, const RenderDev& R, float*
     kernel<<<grid, kRenderThreads, smem, stream>>>(S, R, out, wc, gacc, grp.n_groups,
                                                                           grp.group_strata);
     cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess || grp.n_groups <= 1) return e;
+    if (e != cudaSuccess || grp.n_groups <= 1 || sums_only) return e;
     const int cgrid = (int)std::min<size_t>((n_px + 255) / 256, (size_t)num_sms() * 8);
     k_fixed_finalize<<<cgrid, 256, 0, stream>>>(gacc, n_px, R.exposure, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_render_sums(const SceneDev& S, const RenderDev& R, unsigned long long* sums, WorkCounters* wc,
+                               cudaStream_t stream) {
+    return launch_render_t<false>(S, R, nullptr, wc, stream, 0, sums, render_groups(R), true);
+}
+
+cudaError_t launch_fixed_finalize(const unsigned long long* sums, size_t n_px, float exposure, float* out,
+                                  cudaStream_t stream) {
+    if (n_px == 0) return cudaSuccess;
+    const int cgrid = (int)std::min<size_t>((n_px + 255) / 256, (size_t)num_sms() * 8);
+    k_fixed_finalize<<<cgrid, 256, 0, stream>>>(sums, n_px, exposure, out);
     return cudaGetLastError();
 }
 

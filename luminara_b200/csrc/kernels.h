@@ -23,6 +23,14 @@ RenderGroups render_groups(const RenderDev& R);
 // (zeroed by the launch), which a second kernel turns into `out`.
 cudaError_t launch_render_grouped(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
                                   cudaStream_t stream, unsigned long long* gacc, RenderGroups groups);
+// The megakernel leaving the frame's raw per-pixel sums (4 u64 fixed-point values per pixel:
+// filter-weighted R, G, B and the filter weight, 2^-32 units) in `sums`, zeroed by the launch;
+// no pixels are written.  Sums of disjoint stratum ranges add.
+cudaError_t launch_render_sums(const SceneDev& S, const RenderDev& R, unsigned long long* sums, WorkCounters* wc,
+                               cudaStream_t stream);
+// Pixels (exposure applied) of n_px fixed-point sums.
+cudaError_t launch_fixed_finalize(const unsigned long long* sums, size_t n_px, float exposure, float* out,
+                                  cudaStream_t stream);
 // Counter build of the megakernel: same image, plus node/primitive test tallies in wc->tally.
 cudaError_t launch_render_counted(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
                                   cudaStream_t stream);

@@ -65,6 +65,7 @@ def lib():
         L.orc_render_aov.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.c_int, vp, vp, vp]
         L.orc_render_rows.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.c_int, C.c_int, C.c_uint32,
                                       C.c_uint32, dp, C.POINTER(OrcStats)]
+        L.orc_render_sums.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.c_int, C.c_int, dp, C.POINTER(OrcStats)]
         L.orc_render_row_list.argtypes = [vp, C.POINTER(abi.LumRenderParams), C.c_int, C.c_int, vp, C.c_uint32,
                                           dp, C.POINTER(OrcStats)]
         L.orc_adjoint.argtypes = [vp, C.POINTER(abi.LumRenderParams), dp, vp, C.c_int, C.c_int, dp, dp, dp, dp]
@@ -158,6 +159,19 @@ class OracleScene:
                                        out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(st))
         if rc != 0:
             raise RuntimeError(f"orc_render failed: {rc}")
+        return out, st
+
+    def render_sums(self, cfg, mode=MODE_KEYED, threads=0):
+        """Per-pixel sums before the division (H, W, 4): filter-weighted clamped R, G, B and the
+        filter weight (render.rs:1692-1704)."""
+        p = cfg.to_c()
+        h, w, _ = cfg.out_shape()
+        out = np.zeros((h, w, 4), dtype=np.float64)
+        st = OrcStats()
+        rc = lib().orc_render_sums(self.h, C.byref(p), mode, threads, out.ctypes.data_as(C.POINTER(C.c_double)),
+                                   C.byref(st))
+        if rc != 0:
+            raise RuntimeError(f"orc_render_sums failed: {rc}")
         return out, st
 
     def render_row_list(self, cfg, rows, mode=MODE_STREAM, threads=0):

@@ -1902,9 +1902,11 @@ namespace {
 // params (checked when a row starts, render.rs:1601-1605), 1 = every row starts after it.
 // row_list (n_list entries, output row index = position in the list) renders an arbitrary set
 // of rows in parallel instead of the range [row_begin, row_end).
+// sums (4 doubles per pixel): the pixel's filter-weighted clamped radiance and filter-weight
+// sums before the division of render.rs:1705 (plain sample loop only).
 int render_rows(const orc_scene* sc, const lum_render_params* pp, int mode, int threads, uint32_t row_begin,
                 uint32_t row_end, double* out, orc_stats* stats, int expire, const uint32_t* row_list = nullptr,
-                uint32_t n_list = 0) {
+                uint32_t n_list = 0, double* sums = nullptr) {
     if (!sc || !pp || !out) return 1;
     const lum_render_params& p = *pp;
     Frame f = frame_of(p);
@@ -1977,6 +1979,13 @@ int render_rows(const orc_scene* sc, const lum_render_params* pp, int mode, int 
                 tw += w;
             }
             paths += f.s_end - f.s_begin;
+            if (sums) {
+                double* q = sums + ((size_t)j * f.w + i) * 4;
+                q[0] = color.x;
+                q[1] = color.y;
+                q[2] = color.z;
+                q[3] = tw;
+            }
             V3 px = tw > 0.0 ? color / tw : color;
             o[0] = px.x * p.exposure;
             o[1] = px.y * p.exposure;
@@ -2003,6 +2012,14 @@ extern "C" {
 int orc_render_rows(const orc_scene* sc, const lum_render_params* pp, int mode, int threads, uint32_t row_begin,
                     uint32_t row_end, double* out, orc_stats* stats) {
     return render_rows(sc, pp, mode, threads, row_begin, row_end, out, stats, 0);
+}
+
+int orc_render_sums(const orc_scene* sc, const lum_render_params* p, int mode, int threads, double* sums,
+                    orc_stats* st) {
+    if (!sums || (p && (p->adaptive || p->time_limit > 0.0))) return 1;
+    Frame f = frame_of(*p);
+    std::vector<double> img((size_t)f.w * f.h * 3);
+    return render_rows(sc, p, mode, threads, 0, (uint32_t)f.h, img.data(), st, 0, nullptr, 0, sums);
 }
 
 int orc_render_row_list(const orc_scene* sc, const lum_render_params* pp, int mode, int threads,

@@ -76,6 +76,11 @@ int orc_render_expired(const orc_scene* s, const lum_render_params* p, int mode,
  * same index; used for bounded CPU-baseline samples. */
 int orc_render_rows(const orc_scene* s, const lum_render_params* p, int mode, int threads,
                     uint32_t row_begin, uint32_t row_end, double* out_rgb, orc_stats* stats);
+/* The sample loop's per-pixel sums before the division of render.rs:1705: W*H*4 doubles
+ * (filter-weighted clamped R, G, B and the filter weight).  Sums of disjoint stratum ranges add
+ * (keyed mode; stream mode needs all strata). */
+int orc_render_sums(const orc_scene* s, const lum_render_params* p, int mode, int threads, double* sums,
+                    orc_stats* stats);
 /* Renders the image rows rows[0..n_rows) (any order, OpenMP over the list) into out_rgb, row k of
  * the output holding image row rows[k]: a bounded sample of a frame spread over its height that
  * still keeps every host thread busy. */
