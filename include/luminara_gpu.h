@@ -44,7 +44,7 @@ typedef int32_t lum_status;
 enum {
     LUM_OK = 0,
     LUM_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad index, bad size */
-    LUM_ERR_UNSUPPORTED = 2,      /* a feature outside the GPU path (e.g. panorama camera) */
+    LUM_ERR_UNSUPPORTED = 2,      /* a feature outside the GPU path (e.g. a transformed medium) */
     LUM_ERR_CUDA = 3,             /* a CUDA runtime call failed */
     LUM_ERR_OUT_OF_MEMORY = 4,    /* device allocation failed */
     LUM_ERR_NO_DEVICE = 5,        /* no CUDA device visible */
@@ -185,7 +185,9 @@ typedef struct lum_camera {
     double aspect_ratio;
     double aperture;
     double focus_dist;
-    int32_t panorama;   /* must be 0: the panorama branch is not on the GPU path */
+    int32_t panorama;   /* 1: equirectangular 360-degree camera (camera.rs:83-90): longitude
+                           2 pi s - pi, latitude pi (1 - t) about forward = look_at - look_from,
+                           right and up of the camera basis; unit directions, no lens */
     int32_t reserved;
 } lum_camera;
 

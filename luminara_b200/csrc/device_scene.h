@@ -89,9 +89,11 @@ struct CameraDev {
     float llc[3];
     float hor[3];
     float ver[3];
-    float u[3];
-    float v[3];
+    float u[3];          // right (panorama basis)
+    float v[3];          // up (panorama basis)
     float lens_radius;
+    float fwd[3];        // -w: the panorama's forward axis
+    int32_t panorama;    // 1: equirectangular camera (camera.rs:83-90)
 };
 
 // Device scene: raw pointers into the scene's device allocation.

@@ -586,6 +586,8 @@ lum::CameraDev make_camera(const lum_camera& c) {                      // camera
     put(o.u, u);
     put(o.v, v);
     o.lens_radius = (float)(c.aperture / 2.0);
+    put(o.fwd, w * -1.0);                                              // camera.rs:72-74
+    o.panorama = c.panorama ? 1 : 0;
     return o;
 }
 
@@ -762,7 +764,6 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
     if ((desc->n_objects && !desc->objects) || (desc->n_materials && !desc->materials) ||
         (desc->n_lights && !desc->lights) || (desc->n_meshes && !desc->meshes))
         return fail(LUM_ERR_INVALID_ARGUMENT, "null array with non-zero count");
-    if (desc->camera.panorama) return fail(LUM_ERR_UNSUPPORTED, "panorama camera is not on the GPU path");
     for (uint32_t i = 0; i < desc->n_materials; ++i) {
         int k = desc->materials[i].kind;
         if (k < LUM_MAT_LAMBERTIAN || k > LUM_MAT_SUBSURFACE)

@@ -1000,14 +1000,25 @@ __device__ __forceinline__ void start_path_at(const SceneDev& S, const RenderDev
     float uc = ((float)gi + P.jx) / (float)(R.full_w - 1);
     float vc = (y + P.jy) / (float)(R.full_h - 1);
     const CameraDev& C = S.cam;
-    V off = mk(0.f, 0.f, 0.f);
-    if (C.lens_radius > 0.0f) {
-        float r = sqrtf(c.z) * C.lens_radius, sp, cp;
-        sincospif(2.0f * c.w, &sp, &cp);
-        off = mk(C.u) * (r * cp) + mk(C.v) * (r * sp);
+    if (C.panorama) {
+        // equirectangular (camera.rs:83-90): latitude theta = pi (1 - t), longitude
+        // phi = 2 pi s - pi, unit direction; no lens
+        float st_, ct_, sp_, cp_;
+        sincospif(1.0f - vc, &st_, &ct_);
+        sincospif(2.0f * uc - 1.0f, &sp_, &cp_);
+        V d = mk(C.fwd) * (st_ * cp_) + mk(C.u) * (st_ * sp_) + mk(C.v) * ct_;
+        P.ray.o = mk(C.origin);
+        P.ray.d = d * rsqrtf(len2(d));
+    } else {
+        V off = mk(0.f, 0.f, 0.f);
+        if (C.lens_radius > 0.0f) {
+            float r = sqrtf(c.z) * C.lens_radius, sp, cp;
+            sincospif(2.0f * c.w, &sp, &cp);
+            off = mk(C.u) * (r * cp) + mk(C.v) * (r * sp);
+        }
+        P.ray.o = mk(C.origin) + off;
+        P.ray.d = mk(C.llc) + mk(C.hor) * uc + mk(C.ver) * vc - mk(C.origin) - off;
     }
-    P.ray.o = mk(C.origin) + off;
-    P.ray.d = mk(C.llc) + mk(C.hor) * uc + mk(C.ver) * vc - mk(C.origin) - off;
     // time matters only to moving spheres; a static scene skips the draw (the keyed draws of
     // the other calls do not depend on it)
     P.ray.time = S.moving ? draw4(R.key0, R.key1, pixel, st, 0, CALL_CAMERA2).x : 0.0f;

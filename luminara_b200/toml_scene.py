@@ -22,9 +22,8 @@ What is kept from the reference, on purpose:
 
 Post-processing settings (tone_map, gamma, bloom, ...) are returned in `post` untouched: they
 act on the finished image, after the sample loop.  Anything the device path does not
-render (other primitives, procedural/image textures, bump/normal maps, non-uniform box scale,
-panorama camera) raises UnsupportedSceneError naming every such item, instead of rendering a
-different scene.
+render (other primitives, procedural/image textures, bump/normal maps, non-uniform box scale)
+raises UnsupportedSceneError naming every such item, instead of rendering a different scene.
 """
 from __future__ import annotations
 
@@ -246,8 +245,7 @@ class _Loader:
         cam.vfov_degrees = float(c.get("vfov", cam.vfov_degrees))
         cam.aperture = float(c.get("aperture", cam.aperture))
         cam.focus_dist = float(c.get("focus_dist", cam.focus_dist))
-        if c.get("panorama") is True:
-            self.bad("camera.panorama")
+        cam.panorama = c.get("panorama") is True                        # scene.rs:1170-1172
         world.camera = cam
 
         def add(obj, mat, light=None):

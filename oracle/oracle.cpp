@@ -1207,8 +1207,9 @@ inline void build_onb(V3 n, V3& a, V3& b) {
 }
 
 struct Camera {                                                         // camera.rs:48-102
-    V3 origin, llc, hor, ver, u, v;
+    V3 origin, llc, hor, ver, u, v, forward;
     double lens_radius;
+    bool panorama = false;
     void init(const lum_camera& c) {
         double theta = to_radians(c.vfov_degrees);
         double h = std::tan(theta / 2.0);
@@ -1222,8 +1223,19 @@ struct Camera {                                                         // camer
         origin = from(c.look_from);
         llc = origin - hor / 2.0 - ver / 2.0 - w * c.focus_dist;
         lens_radius = c.aperture / 2.0;
+        forward = w * -1.0;                                             // camera.rs:72-74
+        panorama = c.panorama != 0;
     }
     Ray get_ray(double s, double t, Sampler& smp) const {
+        if (panorama) {                                                 // camera.rs:83-90
+            const double pi = 3.14159265358979323846;
+            double theta = pi * (1.0 - t);
+            double phi = 2.0 * pi * s - pi;
+            V3 dir = forward * (std::sin(theta) * std::cos(phi)) + u * (std::sin(theta) * std::sin(phi)) +
+                     v * std::cos(theta);
+            double time = smp.draw(CALL_CAMERA2, 0);
+            return {origin, unit(dir), time};
+        }
         V3 rd = random_in_unit_disk(smp) * lens_radius;
         V3 off = u * rd.x + v * rd.y;
         double time = smp.draw(CALL_CAMERA2, 0);

@@ -53,14 +53,9 @@ def test_null_arguments_rejected():
     assert lib.lum_scene_destroy(None) == abi.LUM_OK
 
 
-def test_panorama_unsupported_and_bad_material_rejected():
+def test_bad_material_rejected():
     w = S.World()
     w.add(S.Sphere((0, 0, 0), 1.0, S.Lambertian((0.5, 0.5, 0.5))))
-    w.camera.panorama = True
-    with pytest.raises(L.LuminaraError) as e:
-        L.GpuScene(w)
-    assert e.value.status == abi.LUM_ERR_UNSUPPORTED
-    w.camera.panorama = False
     d = w.desc()
     d.c.objects[0].material = 5            # out of range
     h = C.c_void_p()

@@ -116,3 +116,36 @@ def test_autotuner_picks_and_caches(tmp_path, monkeypatch):
     assert b.config() == cfg
     imgs, _, st = b.render()
     assert st.error_flags == 0
+
+
+@pytest.mark.parametrize("mode", [abi.BATCH_WAVEFRONT, abi.BATCH_MEGAKERNEL, abi.BATCH_STREAMS])
+def test_benchmark_batch_scenes_match_keyed_oracle(mode):
+    """Scenes of the 64-scene benchmark batch itself (workloads.batched(): uneven primitive
+    counts, resolutions and materials -- spheres, quads and triangles, Lambertian / Metal /
+    Dielectric / GGX, sphere and rect lights) rendered through the batch API and compared with
+    the oracle's keyed mode, not with another device kernel.  Six scenes from the smallest to the
+    largest primitive count, at their own resolutions and 4 spp (the keyed comparison is path by
+    path, so a few strata per pixel test as much as many).  Tolerance as the keyed render tests:
+    >= 97% of pixels within 2e-3 * (1 + |ref|) per channel, image means within 0.5%."""
+    import oracle as O
+
+    items = W.batched()
+    counts = [w.n_prims() for w, _ in items]
+    order = np.argsort(counts)
+    pick = [int(order[k]) for k in np.linspace(0, len(order) - 1, 6).round().astype(int)]
+    worlds = [items[i][0] for i in pick]
+    cfgs = [items[i][1] for i in pick]
+    for c in cfgs:
+        c.samples_per_pixel = 4
+    scenes = [L.GpuScene(w) for w in worlds]
+    b = L.Batch(scenes, cfgs, config={"mode": mode, "pool_paths": 1 << 18})
+    imgs, _, st = b.render()
+    assert st.error_flags == 0
+    for w, c, img in zip(worlds, cfgs, imgs):
+        ref, ost = O.OracleScene(w).render(c, mode=O.MODE_KEYED)
+        close = np.abs(img - ref) <= 2e-3 * (1.0 + np.abs(ref))
+        frac = close.all(axis=2).mean()
+        assert frac >= 0.97, (w.n_prims(), c.width, frac)
+        m_g, m_r = img.mean(axis=(0, 1)), ref.mean(axis=(0, 1))
+        assert np.all(np.abs(m_g - m_r) <= 5e-3 * np.maximum(m_r, 1e-3)), (w.n_prims(), m_g, m_r)
+    b.close()

@@ -209,3 +209,21 @@ def test_sphere_scene_classes_match_oracle():
     world.add(S.MovingSphere((-2.0, 0.5, 2.0), (-2.0, 0.9, 2.0), 0.5, S.Lambertian((0.7, 0.3, 0.3))))
     world.add(S.MovingSphere((2.0, 0.5, 2.5), (2.4, 0.5, 2.5), 0.5, S.Metal((0.8, 0.8, 0.8), 0.1)))
     keyed_compare(world, cfg)
+
+
+@pytest.mark.parametrize("name", ["box_room", "random_spheres"])
+def test_panorama_camera_matches_keyed_oracle(name):
+    """Equirectangular camera (camera.rs:83-90) on the device against the oracle's keyed mode,
+    and the same frame through the batch (wavefront) equal to lum_render bit for bit."""
+    world, cfg = small(name, 96, 48, 4)
+    world.camera.panorama = True
+    if name == "box_room":
+        world.camera.look_from = (278.0, 278.0, 100.0)     # inside the room
+    img, ref, st, ost = keyed_compare(world, cfg)
+    assert np.isfinite(img).all()
+    sc = L.GpuScene(world)
+    b = L.Batch([sc], [cfg], config={"mode": abi.BATCH_WAVEFRONT, "pool_paths": 1 << 14})
+    imgs, _, bst = b.render()
+    assert bst.error_flags == 0
+    np.testing.assert_array_equal(imgs[0], img)
+    b.close()

@@ -243,6 +243,25 @@ def test_camera_zero_aperture_origin():
     np.testing.assert_allclose(o, [1, 2, 3], atol=1e-6)
 
 
+def test_panorama_camera_axes():
+    """camera.rs:83-90: s maps to longitude 2 pi s - pi, t to latitude pi (1 - t), about the
+    basis forward = -w, right = u, up = v; unit directions from the camera origin, no lens."""
+    cam = S.CameraConfig(look_from=(1, 2, 3), look_at=(1, 2, 0), vfov_degrees=40.0, aspect_ratio=2.0,
+                         aperture=0.5, focus_dist=3.0, panorama=True)
+    fwd, right, up = np.array([0, 0, -1.0]), np.array([1.0, 0, 0]), np.array([0, 1.0, 0])
+    for s_, t_, want in [(0.5, 0.5, fwd), (0.75, 0.5, right), (0.25, 0.5, -right), (0.0, 0.5, -fwd),
+                         (0.5, 1.0, up), (0.5, 0.0, -up)]:
+        o, d, _ = O.camera_ray(cam, s_, t_, seed=5)
+        np.testing.assert_allclose(o, [1, 2, 3], atol=1e-12)           # no lens offset
+        np.testing.assert_allclose(d, want, atol=1e-12)
+        assert abs(np.linalg.norm(d) - 1.0) < 1e-12
+    # a general point: theta = pi (1 - t), phi = 2 pi s - pi
+    s_, t_ = 0.3, 0.8
+    th, ph = np.pi * (1 - t_), 2 * np.pi * s_ - np.pi
+    want = fwd * np.sin(th) * np.cos(ph) + right * np.sin(th) * np.sin(ph) + up * np.cos(th)
+    np.testing.assert_allclose(O.camera_ray(cam, s_, t_)[1], want, atol=1e-12)
+
+
 # ---------------------------------------------------------------- material.rs:909-1235
 HIT = dict(ray_o=(0, 1, 0), ray_d=(0, -1, 0), point=(0, 0, 0), outward_normal=(0, 1, 0), t=1.0, u=0.5, v=0.5)
 

@@ -350,9 +350,6 @@ def test_unsupported_features_are_named():
 [render]
 firefly_filter = 4.0
 
-[camera]
-panorama = true
-
 [[torus]]
 center = [0.0, 0.0, 0.0]
 major_radius = 1.0
@@ -368,8 +365,15 @@ material = { type = "marble", color = [0.5, 0.5, 0.5] }
     with pytest.raises(UnsupportedSceneError) as e:
         load_scene(text)
     items = e.value.items
-    for want in ("[torus]", "render.firefly_filter", "camera.panorama", "bump_strength", "'marble'"):
+    for want in ("[torus]", "render.firefly_filter", "bump_strength", "'marble'"):
         assert any(want in it for it in items), (want, items)
+
+
+def test_panorama_camera_is_read():
+    cfg, world, _ = load_scene('[camera]\nlook_from = [0.0, 1.0, 0.0]\npanorama = true\n')
+    assert world.camera.panorama is True
+    cfg, world, _ = load_scene('[camera]\nlook_from = [0.0, 1.0, 0.0]\n')
+    assert world.camera.panorama is False
 
 
 # The reference project's example scene directory (examples/scenes of a Luminara checkout),
