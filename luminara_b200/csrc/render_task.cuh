@@ -36,7 +36,13 @@ __device__ __forceinline__ void fixed_pixel(const unsigned long long* a, float e
 // the sums.  acc (32 x 4) and *next are the warp's shared memory; the call zeroes them.
 // EXT: the scene may use the other materials or backgrounds; NEE: it has lights; SPH: its
 // primitives are spheres and its materials the basic four (shade's and trace's template flags).
-template <bool COUNT, bool EXT = true, bool NEE = true, bool SPH = false>
+// SUSPEND: lanes still walking the BVH when at most SUSPEND of the warp are left keep their place
+// and let the finished lanes shade and start new rays first (trace_resume); 0 = every walk runs to
+// its end before any lane shades.
+#ifndef LUM_SUSPEND_LANES
+#define LUM_SUSPEND_LANES 0
+#endif
+template <bool COUNT, bool EXT = true, bool NEE = true, bool SPH = false, int SUSPEND = LUM_SUSPEND_LANES>
 __device__ __forceinline__ void tile_task(const SceneDev& S, const RenderDev& R, uint32_t x0, uint32_t y0,
                                           uint32_t tw, uint32_t th, uint32_t s_lo, uint32_t s_hi,
                                           unsigned long long (*acc)[4], uint32_t* next, V* exit_stash, int* stack,
@@ -52,6 +58,9 @@ __device__ __forceinline__ void tile_task(const SceneDev& S, const RenderDev& R,
     uint32_t cur = 0, pixel = 0;
     Path P;
     Pending pend;
+    Hit h;                    // closest hit so far of the lane's walk
+    Trav tv;                  // place of a suspended walk
+    bool found = false, walking = false;
     for (;;) {
         if (state == ST_IDLE) {
             const uint32_t idx = atomicAdd(next, 1u);
@@ -71,12 +80,18 @@ __device__ __forceinline__ void tile_task(const SceneDev& S, const RenderDev& R,
             r.o = P.ray.o;
             r.d = shadow ? pend.dir : P.ray.d;
             r.time = shadow ? 0.0f : P.ray.time;                  // Ray::new (render.rs:1457)
-            Hit h;
-            h.t = shadow ? (EXT ? fabsf(pend.tmax) : pend.tmax) : CUDART_INF_F;
-            h.prim = -1;
-            h.b1 = h.b2 = 0.0f;
-            const bool found = trace<COUNT, SPH>(S, r, 0.001f, shadow, h, stack, err, tally);
-            if (shadow) {
+            if (!walking) {
+                h.t = shadow ? (EXT ? fabsf(pend.tmax) : pend.tmax) : CUDART_INF_F;
+                h.prim = -1;
+                h.b1 = h.b2 = 0.0f;
+                tv.node = S.n_nodes > 0 ? 0 : kSentinel;
+                tv.sp = 0;
+                found = false;
+            }
+            walking = !trace_resume<COUNT, SPH, SUSPEND>(S, r, 0.001f, shadow, h, found, tv, stack, err, tally);
+            if (walking) {
+                // suspended: resumes in a later iteration
+            } else if (shadow) {
                 ++nsh;
                 if (!found) P.L = P.L + pend.contrib;
                 shadow_done<EXT>(P, pend, exit_stash + lane);

@@ -272,17 +272,23 @@ __device__ __forceinline__ uint32_t tone_gamma_fast(float v, float exposure32, d
     return (uint32_t)q;
 }
 
-// The common chain -- exposure, tone curve KIND, sRGB or gamma -- inline; anything else goes
-// through pixel_full (kept out of line so the hot loop stays small in the instruction cache).
+// The common chain -- exposure, tone curve KIND, sRGB or gamma -- inline, in f32 with the exact
+// f64 fallback near byte boundaries (the channel values stay f32 until the fallback needs them).
 template <int KIND>
-__device__ __forceinline__ uint32_t pixel_rgba(const Chain& C, double r, double g, double b, uint32_t p, uint32_t w,
-                                               uint32_t h, double exposure) {
-    if (C.extra) return pixel_full(C, r, g, b, p, w, h, exposure);
-    const float e32 = (float)exposure;
-    const uint32_t R = tone_gamma_fast<KIND>((float)r, e32, exposure, C.inv_gamma);
-    const uint32_t G = tone_gamma_fast<KIND>((float)g, e32, exposure, C.inv_gamma);
-    const uint32_t B = tone_gamma_fast<KIND>((float)b, e32, exposure, C.inv_gamma);
+__device__ __forceinline__ uint32_t pixel_fast(float r, float g, float b, float e32, double exposure, float inv_gamma) {
+    const uint32_t R = tone_gamma_fast<KIND>(r, e32, exposure, inv_gamma);
+    const uint32_t G = tone_gamma_fast<KIND>(g, e32, exposure, inv_gamma);
+    const uint32_t B = tone_gamma_fast<KIND>(b, e32, exposure, inv_gamma);
     return R | (G << 8) | (B << 16) | (255u << 24);
+}
+
+// Any chain: the fast path, or pixel_full (kept out of line so the hot loop stays small in the
+// instruction cache) when an optional step is on.
+template <int KIND>
+__device__ __forceinline__ uint32_t pixel_rgba(const Chain& C, float r, float g, float b, uint32_t p, uint32_t w,
+                                               uint32_t h, float e32, double exposure) {
+    if (C.extra) return pixel_full(C, r, g, b, p, w, h, exposure);
+    return pixel_fast<KIND>(r, g, b, e32, exposure, C.inv_gamma);
 }
 
 __device__ __forceinline__ double log_lum(float r, float g, float b) {
@@ -318,7 +324,7 @@ __global__ void __launch_bounds__(kLogThreads) k_loglum(const float* __restrict_
 }
 
 template <bool VEC, int KIND>
-__global__ void __launch_bounds__(kThreads, 3) k_tonemap(const float* __restrict__ hdr, uint32_t w, uint32_t h, const __grid_constant__ Chain C,
+__global__ void __launch_bounds__(kThreads, 6) k_tonemap(const float* __restrict__ hdr, uint32_t w, uint32_t h, const __grid_constant__ Chain C,
                                                       double exposure, const double* __restrict__ partials,
                                                       uint8_t* __restrict__ rgba) {
     __shared__ double s_exposure;
@@ -336,24 +342,36 @@ __global__ void __launch_bounds__(kThreads, 3) k_tonemap(const float* __restrict
     const uint32_t n = w * h;
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const float e32 = (float)exposure;
     uint32_t scalar_from = 0;
     if constexpr (VEC) {
         const uint32_t n4 = n / 4;
         const float4* in = reinterpret_cast<const float4*>(hdr);
         uint4* out = reinterpret_cast<uint4*>(rgba);
-        for (uint32_t q = t0; q < n4; q += stride) {
-            const float4 a = in[3 * q], b = in[3 * q + 1], c = in[3 * q + 2];
-            const uint32_t p = 4 * q;
-            out[q] = make_uint4(pixel_rgba<KIND>(C, a.x, a.y, a.z, p, w, h, exposure),
-                                pixel_rgba<KIND>(C, a.w, b.x, b.y, p + 1, w, h, exposure),
-                                pixel_rgba<KIND>(C, b.z, b.w, c.x, p + 2, w, h, exposure),
-                                pixel_rgba<KIND>(C, c.y, c.z, c.w, p + 3, w, h, exposure));
+        if (!C.extra) {          // the common chain: f32 all the way (uniform branch, hoisted)
+            const float ig = C.inv_gamma;
+            for (uint32_t q = t0; q < n4; q += stride) {
+                const float4 a = __ldcs(in + 3 * q), b = __ldcs(in + 3 * q + 1), c = __ldcs(in + 3 * q + 2);
+                __stcs(out + q, make_uint4(pixel_fast<KIND>(a.x, a.y, a.z, e32, exposure, ig),
+                                           pixel_fast<KIND>(a.w, b.x, b.y, e32, exposure, ig),
+                                           pixel_fast<KIND>(b.z, b.w, c.x, e32, exposure, ig),
+                                           pixel_fast<KIND>(c.y, c.z, c.w, e32, exposure, ig)));
+            }
+        } else {
+            for (uint32_t q = t0; q < n4; q += stride) {
+                const float4 a = in[3 * q], b = in[3 * q + 1], c = in[3 * q + 2];
+                const uint32_t p = 4 * q;
+                out[q] = make_uint4(pixel_rgba<KIND>(C, a.x, a.y, a.z, p, w, h, e32, exposure),
+                                    pixel_rgba<KIND>(C, a.w, b.x, b.y, p + 1, w, h, e32, exposure),
+                                    pixel_rgba<KIND>(C, b.z, b.w, c.x, p + 2, w, h, e32, exposure),
+                                    pixel_rgba<KIND>(C, c.y, c.z, c.w, p + 3, w, h, e32, exposure));
+            }
         }
         scalar_from = 4 * n4;
     }
     for (uint32_t p = scalar_from + t0; p < n; p += stride) {   // any output alignment: byte stores
         const uint32_t v = pixel_rgba<KIND>(C, hdr[3 * (size_t)p], hdr[3 * (size_t)p + 1], hdr[3 * (size_t)p + 2], p,
-                                            w, h, exposure);
+                                            w, h, e32, exposure);
         rgba[4 * (size_t)p] = (uint8_t)v;
         rgba[4 * (size_t)p + 1] = (uint8_t)(v >> 8);
         rgba[4 * (size_t)p + 2] = (uint8_t)(v >> 16);
@@ -410,7 +428,7 @@ cudaError_t launch_tonemap(const float* hdr, uint32_t w, uint32_t h, const lum_t
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const size_t work = vec ? (n + 3) / 4 : n;
-    const int grid = (int)std::min<size_t>((work + tone::kThreads - 1) / tone::kThreads, (size_t)nsm * 8);
+    const int grid = (int)std::min<size_t>((work + tone::kThreads - 1) / tone::kThreads, (size_t)nsm * 64);
     auto go = [&](auto kind) {
         constexpr int K = decltype(kind)::value;
         if (vec)

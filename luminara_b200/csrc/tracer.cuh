@@ -301,17 +301,29 @@ __device__ __forceinline__ bool hit_plane(const PlaneDev& P, const Ray& ray, flo
 // near child first.  Stack entries (shared memory, entry k of thread j at
 // stack[k * blockDim.x + j]) are inner-node indices (>= 0) or leaf ranges ~(first << 3 |
 // count - 1); kSentinel marks the empty stack.
-//
-// Closest hit (any = false) keeps the nearest accepted t; any = true returns at the first
-// accepted hit (the shadow query, render.rs:1457-1460).  Unbounded planes follow the BVH
-// (scene.rs:826-831).
 constexpr int kSentinel = 0x7fffffff;
 
-template <bool COUNT = false, bool SPH = false>
-__device__ __forceinline__ bool trace(const SceneDev& S, const Ray& ray, float tmin, bool any, Hit& hit, int* stack,
-                                      uint32_t& err, TestTally* tl = nullptr) {
-    bool found = false;
-    if (S.n_nodes > 0) {
+// Place of a suspended BVH walk (trace_resume): the next node to visit (an inner node index, or
+// kSentinel when the walk is over) and the stack depth; the stack entries stay in shared memory
+// and the closest hit so far in the caller's Hit.
+struct Trav {
+    int node;
+    int sp;
+};
+
+// The BVH walk of `trace`, resumable.  With SUSPEND > 0 the walk stops at the top of an outer
+// iteration (no postponed leaf pending) once at most SUSPEND lanes of the warp are still
+// walking: it saves its place in tv and returns false, so that the lanes which finished can
+// shade and start new rays before the warp walks on (Aila & Laine 2009 replace terminated rays
+// in the same spirit: a warp's traversal otherwise runs as long as its longest ray while the
+// finished lanes idle).  Returns true when the walk is complete (planes tested, `found` final).
+// SUSPEND == 0 never stops early.  tv starts as {0, 0} (or kSentinel for a scene without
+// nodes), found as false.
+template <bool COUNT = false, bool SPH = false, int SUSPEND = 0>
+__device__ __forceinline__ bool trace_resume(const SceneDev& S, const Ray& ray, float tmin, bool any, Hit& hit,
+                                             bool& found, Trav& tv, int* stack, uint32_t& err,
+                                             TestTally* tl = nullptr) {
+    if (tv.node != kSentinel) {
         // Reciprocals of direction components clamped away from zero: the FMA slab form
         // lo*inv - o*inv would give inf - inf = NaN for an axis-parallel ray, while a finite
         // +-1e20 keeps the ordering of the reference's (lo - o) * (1/d) (aabb.rs:23-25).
@@ -321,9 +333,9 @@ __device__ __forceinline__ bool trace(const SceneDev& S, const Ray& ray, float t
         const float ox = -ray.o.x * ix, oy = -ray.o.y * iy, oz = -ray.o.z * iz;
         const float4* nodes = reinterpret_cast<const float4*>(S.nodes);
         const int stride = blockDim.x;
-        int sp = 0;
-        int node = 0;   // inner node index, leaf (< 0) or kSentinel
-        int leaf = 0;   // postponed leaf (< 0) or 0
+        int sp = tv.sp;
+        int node = tv.node;   // inner node index, leaf (< 0) or kSentinel
+        int leaf = 0;         // postponed leaf (< 0) or 0
         for (;;) {
             while ((unsigned)node < (unsigned)kSentinel) {
                 float4 n0 = __ldg(nodes + 4 * node + 0);
@@ -368,7 +380,10 @@ __device__ __forceinline__ bool trace(const SceneDev& S, const Ray& ray, float t
                 for (int k = 0; k < cnt; ++k) {
                     if (test_prim<COUNT, SPH>(S, first + k, ray, tmin, hit, tl)) {
                         found = true;
-                        if (any) return true;
+                        if (any) {
+                            tv.node = kSentinel;
+                            return true;
+                        }
                     }
                 }
                 leaf = 0;
@@ -378,7 +393,15 @@ __device__ __forceinline__ bool trace(const SceneDev& S, const Ray& ray, float t
                 }
             }
             if (node == kSentinel) break;
+            if constexpr (SUSPEND > 0) {
+                if (__popc(__activemask()) <= SUSPEND) {
+                    tv.node = node;
+                    tv.sp = sp;
+                    return false;
+                }
+            }
         }
+        tv.node = kSentinel;
     }
     for (int k = 0; k < S.n_planes; ++k) {                             // scene.rs:826-831
         if constexpr (COUNT) tl->plane++;
@@ -390,6 +413,18 @@ __device__ __forceinline__ bool trace(const SceneDev& S, const Ray& ray, float t
             if (any) return true;
         }
     }
+    return true;
+}
+
+// Closest hit (any = false) keeps the nearest accepted t; any = true returns at the first
+// accepted hit (the shadow query, render.rs:1457-1460).  Unbounded planes follow the BVH
+// (scene.rs:826-831).
+template <bool COUNT = false, bool SPH = false>
+__device__ __forceinline__ bool trace(const SceneDev& S, const Ray& ray, float tmin, bool any, Hit& hit, int* stack,
+                                      uint32_t& err, TestTally* tl = nullptr) {
+    bool found = false;
+    Trav tv{S.n_nodes > 0 ? 0 : kSentinel, 0};
+    trace_resume<COUNT, SPH, 0>(S, ray, tmin, any, hit, found, tv, stack, err, tl);
     return found;
 }
 
