@@ -1038,10 +1038,15 @@ __device__ __forceinline__ void start_path_at(const SceneDev& S, const RenderDev
     if (C.panorama) {
         // equirectangular (camera.rs:83-90): latitude theta = pi (1 - t), longitude
         // phi = 2 pi s - pi, unit direction; no lens
+        // (explicitly rounded: the compiler contracts a * b + c into an FMA per call site, and
+        // every kernel must produce the same direction bit for bit)
         float st_, ct_, sp_, cp_;
         sincospif(1.0f - vc, &st_, &ct_);
-        sincospif(2.0f * uc - 1.0f, &sp_, &cp_);
-        V d = mk(C.fwd) * (st_ * cp_) + mk(C.u) * (st_ * sp_) + mk(C.v) * ct_;
+        sincospif(fmaf(2.0f, uc, -1.0f), &sp_, &cp_);
+        const float a_ = __fmul_rn(st_, cp_), b_ = __fmul_rn(st_, sp_);
+        const V d = mk(fmaf(C.fwd[0], a_, fmaf(C.u[0], b_, __fmul_rn(C.v[0], ct_))),
+                       fmaf(C.fwd[1], a_, fmaf(C.u[1], b_, __fmul_rn(C.v[1], ct_))),
+                       fmaf(C.fwd[2], a_, fmaf(C.u[2], b_, __fmul_rn(C.v[2], ct_))));
         P.ray.o = mk(C.origin);
         P.ray.d = d * rsqrtf(len2(d));
     } else {
