@@ -569,7 +569,10 @@ void lum_tonemap_default(lum_tonemap_params* out);
  * default stream).  d_scratch: LUM_TONEMAP_SCRATCH_BYTES of device memory, used only with
  * auto_exposure (may be NULL otherwise; 8-byte aligned).  d_hdr_rgb must be 4-byte aligned,
  * d_rgba may have any alignment (16-byte aligned buffers take the vectorised path).
- * Allocates nothing; does not synchronise. */
+ * Allocates nothing; does not synchronise, except that the first call on a device for a given
+ * (tone_map, gamma) pair without optional steps computes that chain's byte-threshold table on
+ * the host (a few milliseconds) and copies it synchronously into a fixed device table (16
+ * pairs per device); make that first call outside stream capture. */
 lum_status lum_tonemap_device(const float* d_hdr_rgb, uint32_t width, uint32_t height,
                               const lum_tonemap_params* tm, void* d_scratch, uint8_t* d_rgba,
                               void* stream);

@@ -15,14 +15,19 @@
 //   k_tonemap  4 pixels per thread: three 16-byte loads of 12 floats, one 16-byte store of
 //              4 RGBA pixels (a scalar tail with byte stores for pixel counts not divisible
 //              by 4, or for buffers that are not 16-byte aligned).  With auto-exposure each block first
-//              sums the 256 partials in the same fixed order.
+//              sums the 256 partials in the same fixed order.  The common chain (no optional
+//              step) reads each channel's byte from a table of the chain's 255 byte thresholds
+//              (one entry lookup per channel, see ByteTable); chains with optional steps, and
+//              tone curves whose table does not fit, take the f32 path with its f64 fallback.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <type_traits>
+#include <vector>
 
 #include "../../include/luminara_gpu.h"
 #include "kernels.h"
@@ -46,16 +51,16 @@ struct Chain {
 };
 
 // Rust's `as u8` from f64: truncation, saturating, NaN -> 0.
-__device__ __forceinline__ uint32_t sat_u8(double x) {
+__host__ __device__ __forceinline__ uint32_t sat_u8(double x) {
     if (!(x > 0.0)) return 0u;
     if (x >= 255.0) return 255u;
     return (uint32_t)x;
 }
 
-__device__ __forceinline__ double clamp01(double x) { return fmin(fmax(x, 0.0), 1.0); }
+__host__ __device__ __forceinline__ double clamp01(double x) { return fmin(fmax(x, 0.0), 1.0); }
 
 // Tone curves (src/render.rs:3608-3641).
-__device__ __forceinline__ double tone_curve(int kind, double x) {
+__host__ __device__ __forceinline__ double tone_curve(int kind, double x) {
     x = fmax(x, 0.0);   // f64::max ignores NaN
     switch (kind) {
         case LUM_TONEMAP_REINHARD:
@@ -100,13 +105,13 @@ __device__ __forceinline__ float tone_curve_f(int kind, float x) {
 
 // gamma_correct (src/render.rs:3648-3658): sRGB transfer function (gamma <= 0) or 1/gamma
 // power, plus the dither offset, quantised as (s + dither).clamp(0, 0.999) * 256.
-__device__ __forceinline__ double quantised(double s, double dither) {
+__host__ __device__ __forceinline__ double quantised(double s, double dither) {
     double q = s + dither;
     if (q != q) return -1.0;
     return fmin(fmax(q, 0.0), 0.999) * 256.0;
 }
 
-__device__ __forceinline__ double srgb64(double x, double gamma) {
+__host__ __device__ __forceinline__ double srgb64(double x, double gamma) {
     if (gamma > 0.0) return pow(x, 1.0 / gamma);
     return x <= 0.0031308 ? 12.92 * x : 1.055 * pow(x, 1.0 / 2.4) - 0.055;
 }
@@ -272,8 +277,57 @@ __device__ __forceinline__ uint32_t tone_gamma_fast(float v, float exposure32, d
     return (uint32_t)q;
 }
 
+// Byte tables of the common chain.  Without dither, vignette or the other optional steps, a
+// channel's byte is a non-decreasing step function of x = (double)v * exposure: the tone curve,
+// the sRGB or 1/gamma power and the quantisation are all monotone.  So it is fixed by the 255
+// thresholds T_k = min{x : byte(x) >= k}, found once per (tone curve, gamma) on the host by
+// bisection over the f64 bit patterns with the reference's own f64 formulas (the host's libm
+// pow, as the f64 restatement uses) -- exact, not a fit.  The kernel finds x's byte from one
+// table entry: positive doubles order like their bit patterns, and the bucket of x is its top
+// 19 bits (sign, exponent, 7 mantissa bits), chosen so that no bucket holds two thresholds.
+// Entry i (a u64): byte at the bucket's lower end in bits 56-63, the low 45 bits of the bucket's
+// threshold (or 2^45: none) in bits 0-45; x's byte is that base, plus one if x's low 45 bits reach
+// the threshold's.  Entry 0 stands for every bucket below the first, entry nb + 1 for every
+// bucket above the last.  Non-finite, huge or non-positive x take the f64 path as before.
+constexpr int kTabShift = 45;                                  // 52 - 7 mantissa bits
+constexpr unsigned long long kTabLowMask = (1ull << kTabShift) - 1ull;
+constexpr int kTabMaxEntries = 4096;                           // nb + 2 per table
+constexpr int kTabSlots = 16;                                  // (tone curve, gamma) pairs per device
+
+struct ByteTable {
+    const unsigned long long* tab;   // device address of the slot, or null: no table
+    long long k0;                    // bucket key of entry 1
+    int nb;                          // buckets with an entry of their own
+};
+
+static __device__ __align__(256) unsigned long long g_byte_tables[kTabSlots][kTabMaxEntries];
+
+template <int KIND>
+__device__ __forceinline__ uint32_t tone_table(float v, double exposure, const ByteTable& T, float inv_gamma) {
+    const double x = (double)v * exposure;
+    if (!(x > 0.0)) return 0u;                                 // NaN, zero and negatives: byte 0
+    if (!(x < 1e30)) {
+        const double q64 = tone_gamma64(KIND, x, inv_gamma > 0.0f ? 1.0 / (double)inv_gamma : 0.0, 0.0);
+        return q64 < 0.0 ? 0u : sat_u8(q64);
+    }
+    const long long b = __double_as_longlong(x);
+    const long long i = min(max((b >> kTabShift) - T.k0 + 1, 0ll), (long long)T.nb + 1);
+    const unsigned long long e = __ldg(T.tab + i);
+    return (uint32_t)(e >> 56) + (((unsigned long long)b & kTabLowMask) >= (e & (2ull * kTabLowMask + 1ull)) ? 1u : 0u);
+}
+
+template <int KIND>
+__device__ __forceinline__ uint32_t pixel_table(float r, float g, float b, double exposure, const ByteTable& T,
+                                                float inv_gamma) {
+    const uint32_t R = tone_table<KIND>(r, exposure, T, inv_gamma);
+    const uint32_t G = tone_table<KIND>(g, exposure, T, inv_gamma);
+    const uint32_t B = tone_table<KIND>(b, exposure, T, inv_gamma);
+    return R | (G << 8) | (B << 16) | (255u << 24);
+}
+
 // The common chain -- exposure, tone curve KIND, sRGB or gamma -- inline, in f32 with the exact
-// f64 fallback near byte boundaries (the channel values stay f32 until the fallback needs them).
+// f64 fallback near byte boundaries (the channel values stay f32 until the fallback needs them);
+// used when no byte table is available.
 template <int KIND>
 __device__ __forceinline__ uint32_t pixel_fast(float r, float g, float b, float e32, double exposure, float inv_gamma) {
     const uint32_t R = tone_gamma_fast<KIND>(r, e32, exposure, inv_gamma);
@@ -326,7 +380,7 @@ __global__ void __launch_bounds__(kLogThreads) k_loglum(const float* __restrict_
 template <bool VEC, int KIND>
 __global__ void __launch_bounds__(kThreads, 6) k_tonemap(const float* __restrict__ hdr, uint32_t w, uint32_t h, const __grid_constant__ Chain C,
                                                       double exposure, const double* __restrict__ partials,
-                                                      uint8_t* __restrict__ rgba) {
+                                                      uint8_t* __restrict__ rgba, const ByteTable T) {
     __shared__ double s_exposure;
     if (partials) {   // auto-exposure: key value 0.18 over the log-average luminance
         if (threadIdx.x == 0) {
@@ -348,7 +402,16 @@ __global__ void __launch_bounds__(kThreads, 6) k_tonemap(const float* __restrict
         const uint32_t n4 = n / 4;
         const float4* in = reinterpret_cast<const float4*>(hdr);
         uint4* out = reinterpret_cast<uint4*>(rgba);
-        if (!C.extra) {          // the common chain: f32 all the way (uniform branch, hoisted)
+        if (!C.extra && T.tab) {   // the common chain from its byte table (uniform branch, hoisted)
+            const float ig = C.inv_gamma;
+            for (uint32_t q = t0; q < n4; q += stride) {
+                const float4 a = __ldcs(in + 3 * q), b = __ldcs(in + 3 * q + 1), c = __ldcs(in + 3 * q + 2);
+                __stcs(out + q, make_uint4(pixel_table<KIND>(a.x, a.y, a.z, exposure, T, ig),
+                                           pixel_table<KIND>(a.w, b.x, b.y, exposure, T, ig),
+                                           pixel_table<KIND>(b.z, b.w, c.x, exposure, T, ig),
+                                           pixel_table<KIND>(c.y, c.z, c.w, exposure, T, ig)));
+            }
+        } else if (!C.extra) {     // the common chain in f32 with the exact fallback
             const float ig = C.inv_gamma;
             for (uint32_t q = t0; q < n4; q += stride) {
                 const float4 a = __ldcs(in + 3 * q), b = __ldcs(in + 3 * q + 1), c = __ldcs(in + 3 * q + 2);
@@ -405,6 +468,98 @@ Chain make_chain(const lum_tonemap_params& p) {
     return C;
 }
 
+// Host side of the byte tables: the chain's byte for an exact f64 x (gamma <= 0: sRGB).
+static uint32_t host_byte(int kind, double x, double gamma) {
+    return sat_u8(quantised(srgb64(clamp01(tone_curve(kind, x)), gamma), 0.0));
+}
+
+static long long dbits(double x) {
+    long long b;
+    std::memcpy(&b, &x, sizeof b);
+    return b;
+}
+static double bdouble(long long b) {
+    double x;
+    std::memcpy(&x, &b, sizeof x);
+    return x;
+}
+
+// Builds the entries of one table; false when the chain is not the step function the table
+// encodes (a bucket with two thresholds, too many buckets, or a byte that does not match).
+static bool build_byte_table(int kind, double gamma, std::vector<unsigned long long>& ent, long long& k0, int& nb) {
+    const long long top = dbits(1e30);
+    std::vector<long long> th;                                  // bit patterns of T_1 .. T_bmax
+    const uint32_t bmax = host_byte(kind, 1e30, gamma);
+    if (host_byte(kind, bdouble(1), gamma) != 0u) return false;  // smallest positive x must be byte 0
+    for (uint32_t k = 1; k <= bmax; ++k) {
+        long long lo = th.empty() ? 0 : th.back() - 1, hi = top;   // byte(lo) < k <= byte(hi)
+        if (lo < 0) lo = 0;
+        while (hi - lo > 1) {
+            const long long m = lo + (hi - lo) / 2;
+            if (host_byte(kind, bdouble(m), gamma) >= k) hi = m;
+            else lo = m;
+        }
+        th.push_back(hi);
+    }
+    if (th.empty()) return false;
+    k0 = th.front() >> kTabShift;
+    const long long k1 = th.back() >> kTabShift;
+    nb = (int)(k1 - k0 + 1);
+    if (nb + 2 > kTabMaxEntries) return false;
+    ent.assign(nb + 2, 0ull);
+    ent[0] = 2ull * kTabLowMask + 1ull;                          // below: byte 0, no threshold
+    ent[nb + 1] = ((unsigned long long)bmax << 56) | (2ull * kTabLowMask + 1ull);
+    size_t t = 0;                                               // thresholds at or below the bucket start
+    for (int i = 0; i < nb; ++i) {
+        const long long key = k0 + i, lo = key << kTabShift, hi = (key + 1) << kTabShift;
+        while (t < th.size() && th[t] <= lo) ++t;
+        const uint32_t base = (uint32_t)t;
+        if (host_byte(kind, bdouble(lo), gamma) != base) return false;        // not monotone here
+        unsigned long long thr = 2ull * kTabLowMask + 1ull;     // none
+        if (t < th.size() && th[t] < hi) {
+            if (t + 1 < th.size() && th[t + 1] < hi) return false;            // two in one bucket
+            thr = (unsigned long long)th[t] & kTabLowMask;
+        }
+        ent[i + 1] = ((unsigned long long)base << 56) | thr;
+    }
+    return true;
+}
+
+// One table per (device, tone curve, gamma), uploaded once into a slot of g_byte_tables.
+struct TableSlot {
+    int device, kind;
+    long long gamma_bits;
+    ByteTable T;
+};
+
+static ByteTable byte_table(int kind, double gamma) {
+    static std::mutex mu;
+    static std::vector<TableSlot> slots;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return ByteTable{nullptr, 0, 0};
+    if (!(gamma > 0.0)) gamma = 0.0;
+    const long long gb = dbits(gamma);
+    std::lock_guard<std::mutex> lk(mu);
+    int used = 0;
+    for (const TableSlot& sl : slots) {
+        if (sl.device != dev) continue;
+        if (sl.kind == kind && sl.gamma_bits == gb) return sl.T;
+        ++used;
+    }
+    TableSlot sl{dev, kind, gb, ByteTable{nullptr, 0, 0}};
+    std::vector<unsigned long long> ent;
+    void* base = nullptr;
+    if (used < kTabSlots && build_byte_table(kind, gamma, ent, sl.T.k0, sl.T.nb) &&
+        cudaGetSymbolAddress(&base, g_byte_tables) == cudaSuccess &&
+        cudaMemcpyToSymbol(g_byte_tables, ent.data(), ent.size() * sizeof(unsigned long long),
+                           (size_t)used * kTabMaxEntries * sizeof(unsigned long long)) == cudaSuccess)
+        sl.T.tab = static_cast<const unsigned long long*>(base) + (size_t)used * kTabMaxEntries;
+    cudaGetLastError();
+    if (!sl.T.tab) sl.kind = -1 - kind;                         // remembered as "no table"
+    slots.push_back(sl);
+    return sl.T;
+}
+
 }  // namespace tone
 
 cudaError_t launch_tonemap(const float* hdr, uint32_t w, uint32_t h, const lum_tonemap_params& tm, double exposure,
@@ -424,6 +579,7 @@ cudaError_t launch_tonemap(const float* hdr, uint32_t w, uint32_t h, const lum_t
         partials = scratch;
     }
     const tone::Chain C = tone::make_chain(tm);
+    const tone::ByteTable T = C.extra ? tone::ByteTable{nullptr, 0, 0} : tone::byte_table(tm.tone_map, tm.gamma);
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -433,10 +589,10 @@ cudaError_t launch_tonemap(const float* hdr, uint32_t w, uint32_t h, const lum_t
         constexpr int K = decltype(kind)::value;
         if (vec)
             tone::k_tonemap<true, K><<<grid, tone::kThreads, 0, stream>>>(hdr, (uint32_t)w, (uint32_t)h, C, exposure,
-                                                                          partials, rgba);
+                                                                          partials, rgba, T);
         else
             tone::k_tonemap<false, K><<<grid, tone::kThreads, 0, stream>>>(hdr, (uint32_t)w, (uint32_t)h, C, exposure,
-                                                                           partials, rgba);
+                                                                           partials, rgba, T);
     };
     switch (tm.tone_map) {
         case LUM_TONEMAP_REINHARD: go(std::integral_constant<int, LUM_TONEMAP_REINHARD>()); break;
