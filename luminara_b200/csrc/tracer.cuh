@@ -102,7 +102,8 @@ __device__ __forceinline__ float4 ldp(const SceneDev& S, int i, int k) {
 // f64: in f32 that difference loses ~r * 6e-8 absolutely, which near the surface of an
 // r = 1000 sphere is a large relative error of the near root.
 constexpr float kBigSphere = 32.0f;
-__device__ __forceinline__ bool sphere_roots(V c, float r, const Ray& ray, float& t0, float& t1) {
+// a = |d|^2 and ia = 1 / a are the ray's (the caller may compute them once per ray).
+__device__ __forceinline__ bool sphere_roots(V c, float r, const Ray& ray, float a, float ia, float& t0, float& t1) {
     V oc;
     float cc;
     if (r >= kBigSphere) {
@@ -113,9 +114,7 @@ __device__ __forceinline__ bool sphere_roots(V c, float r, const Ray& ray, float
         oc = ray.o - c;
         cc = fmaf(-r, r, len2(oc));
     }
-    float a = len2(ray.d);
     float b = dot(oc, ray.d);
-    const float ia = 1.0f / a;
     V f = fma3(ray.d, -b * ia, oc);
     float disc = a * (r * r - len2(f));
     if (disc < 0.0f) return false;
@@ -127,12 +126,20 @@ __device__ __forceinline__ bool sphere_roots(V c, float r, const Ray& ray, float
     return true;
 }
 
-// sphere.rs:24-45: near root if in [tmin, tmax], else far root.
-__device__ __forceinline__ bool hit_sphere(float4 a, float4 b, const Ray& ray, float tmin, float tmax, float& t) {
+__device__ __forceinline__ bool sphere_roots(V c, float r, const Ray& ray, float& t0, float& t1) {
+    const float a = len2(ray.d);
+    return sphere_roots(c, r, ray, a, 1.0f / a, t0, t1);
+}
+
+// sphere.rs:24-45: near root if in [tmin, tmax], else far root.  ia: 1 / |d|^2 of the ray, or 0
+// to compute it here.
+__device__ __forceinline__ bool hit_sphere(float4 a, float4 b, const Ray& ray, float tmin, float tmax, float& t,
+                                           float ia = 0.0f) {
     V c = xyz(a);
     if (b.w != 0.0f) c = fma3(xyz(b) - c, ray.time, c);   // MovingSphere::center_at
     float t0, t1;
-    if (!sphere_roots(c, a.w, ray, t0, t1)) return false;
+    const float aa = len2(ray.d);
+    if (!sphere_roots(c, a.w, ray, aa, ia != 0.0f ? ia : 1.0f / aa, t0, t1)) return false;
     if (t0 >= tmin && t0 <= tmax) { t = t0; return true; }
     if (t1 >= tmin && t1 <= tmax) { t = t1; return true; }
     return false;
@@ -234,13 +241,14 @@ __device__ __forceinline__ bool hit_fog(int type, float4 a, float4 b, float4 c, 
 // One primitive test; updates the closest hit when t is within [tmin, hit.t].
 // SPH: the scene's primitives are all static spheres (SceneDev::spheres_basic), so the other
 // primitive tests are left out of the kernel and a test reads only record 0 (centre, radius).
+// ia_ray: 1 / |d|^2 of the ray, computed once per walk by the sphere-class build (0 elsewhere).
 template <bool COUNT = false, bool SPH = false>
 __device__ __forceinline__ bool test_prim(const SceneDev& S, int i, const Ray& ray, float tmin, Hit& hit,
-                                          TestTally* tl = nullptr) {
+                                          TestTally* tl = nullptr, float ia_ray = 0.0f) {
     float4 a = ldp(S, i, 0);
     float t;
     if constexpr (SPH && !COUNT) {
-        if (hit_sphere(a, make_float4(0.0f, 0.0f, 0.0f, 0.0f), ray, tmin, hit.t, t)) {
+        if (hit_sphere(a, make_float4(0.0f, 0.0f, 0.0f, 0.0f), ray, tmin, hit.t, t, ia_ray)) {
             hit.t = t;
             hit.prim = i;
             return true;
@@ -331,6 +339,9 @@ __device__ __forceinline__ bool trace_resume(const SceneDev& S, const Ray& ray, 
         const float iy = 1.0f / (fabsf(ray.d.y) > 1e-20f ? ray.d.y : copysignf(1e-20f, ray.d.y));
         const float iz = 1.0f / (fabsf(ray.d.z) > 1e-20f ? ray.d.z : copysignf(1e-20f, ray.d.z));
         const float ox = -ray.o.x * ix, oy = -ray.o.y * iy, oz = -ray.o.z * iz;
+        // the sphere class divides by |d|^2 once per walk instead of once per sphere test
+        float ia_ray = 0.0f;
+        if constexpr (SPH && !COUNT) ia_ray = 1.0f / len2(ray.d);
         const float4* nodes = reinterpret_cast<const float4*>(S.nodes);
         const int stride = blockDim.x;
         int sp = tv.sp;
@@ -378,7 +389,7 @@ __device__ __forceinline__ bool trace_resume(const SceneDev& S, const Ray& ray, 
             while (leaf < 0) {
                 const int first = (~leaf) >> 3, cnt = ((~leaf) & 7) + 1;
                 for (int k = 0; k < cnt; ++k) {
-                    if (test_prim<COUNT, SPH>(S, first + k, ray, tmin, hit, tl)) {
+                    if (test_prim<COUNT, SPH>(S, first + k, ray, tmin, hit, tl, ia_ray)) {
                         found = true;
                         if (any) {
                             tv.node = kSentinel;

@@ -11,11 +11,13 @@
    - every emission parameter, per seed, step 1e-3, within 1e-2 relative (emission moves no
      sampling decision, so the per-seed difference is smooth);
    - albedo and roughness along fixed unit directions (each parameter stepped by ~1e-3),
-     averaged over 256 seeds: a per-seed difference of albedo or roughness also contains the
+     averaged over 2048 seeds: a per-seed difference of albedo or roughness also contains the
      jumps of paths whose Russian-roulette, lobe or visibility decision flips, whose mean is
-     what the adjoint's held-probability and score terms account for; the seed average agrees
-     within 2e-2 (albedo) and 6e-2 (roughness, whose visibility changes are not
-     differentiated) and within 3 standard errors.
+     what the adjoint's held-probability and score terms account for.  The bar is 1e-2
+     relative on the expectation; the seed means carry sampling error (standard error about
+     0.3% for albedo and 1.1% for roughness at 2048 seeds), so the test requires the measured
+     difference to lie within 1e-2 plus two standard errors.  A 4096-seed run measured
+     -0.66% +- 0.22% (albedo) and -0.06% +- 0.77% (roughness).
 """
 import numpy as np
 import pytest
@@ -147,27 +149,31 @@ def test_c5_albedo_roughness_finite_differences_seed_average():
     dirs = {k: acc[k] / np.linalg.norm(acc[k]) for k in sels}
     eps = 5e-2                      # along a unit direction over ~3000 parameters: ~1e-3 each
     rows = {k: [] for k in sels}
-    for s in range(256):
+    # the perturbed worlds are fixed: one scene each, rendered with every seed
+    pert = {}
+    for k in sels:
+        for sign in (1, -1):
+            undo = directional(world, dict(zip(sels[k], dirs[k])), sign * eps)
+            pert[(k, sign)] = L.GpuScene(world)
+            undo()
+    idx = {k: [(m, c) for _, m, c in sels[k]] for k in sels}
+    g64 = g.astype(np.float64)
+    for s in range(2048):
         cfg.seed = 1000 + s
-        da, dr, de, _ = L.GpuScene(world).backward(cfg, g, lm)
+        da, dr, de, _ = sc.backward(cfg, g, lm)
         for k in sels:
-            v = dirs[k]
-            ad = float(np.array([grad_of(*p, da, dr, de) for p in sels[k]], dtype=np.float64) @ v)
-            vals = []
-            for sign in (1, -1):
-                undo = directional(world, dict(zip(sels[k], v)), sign * eps)
-                im, _ = L.GpuScene(world).render(cfg)
-                undo()
-                vals.append(float((g * im.astype(np.float64)).sum()))
+            grads = (np.array([da[m, c] for m, c in idx[k]]) if k == ALBEDO
+                     else np.array([dr[m] for m, _ in idx[k]]))
+            ad = float(grads.astype(np.float64) @ dirs[k])
+            vals = [float((g64 * pert[(k, sign)].render(cfg)[0]).sum()) for sign in (1, -1)]
             rows[k].append(((vals[0] - vals[1]) / (2 * eps), ad))
-    for k, tol in ((ALBEDO, 2e-2), (ROUGHNESS, 6e-2)):
+    for k in (ALBEDO, ROUGHNESS):
         r = np.array(rows[k])
         diff = r[:, 0] - r[:, 1]
         se = diff.std(ddof=1) / np.sqrt(len(diff))
         fd, ad = r[:, 0].mean(), r[:, 1].mean()
         print(f"{k}: mean FD {fd:.2f}, mean adjoint {ad:.2f}, rel diff {(fd - ad) / ad:+.4f}, rel SE {se / abs(ad):.4f}")
-        assert abs(fd - ad) <= tol * abs(ad), (k, fd, ad, se)
-        assert abs(fd - ad) <= 3 * se, (k, fd, ad, se)
+        assert abs(fd - ad) <= 1e-2 * abs(ad) + 2.0 * se, (k, fd, ad, se)
 
 
 def test_c5_adjoint_costs_at_most_three_forward_renders():
