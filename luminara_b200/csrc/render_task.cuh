@@ -36,15 +36,6 @@ __device__ __forceinline__ void fixed_pixel(const unsigned long long* a, float e
 // the sums.  acc (32 x 4) and *next are the warp's shared memory; the call zeroes them.
 // EXT: the scene may use the other materials or backgrounds; NEE: it has lights; SPH: its
 // primitives are spheres and its materials the basic four (shade's and trace's template flags).
-// SUSPEND: lanes still walking the BVH when at most SUSPEND of the warp are left keep their place
-// and let the finished lanes shade and start new rays first (trace_resume); 0 = every walk runs to
-// its end before any lane shades.  Measured on B200 against 0 (kernel time per frame, images
-// identical): 4 / 8 / 16 lanes gave the sphere field 101.7 -> 91.1 / 91.9 / 92.4 ms, the box room
-// 2.57 -> 2.40 / 2.29 / 2.23 ms, the quad scene 13.6 -> 11.5 / 11.4 / 11.8 ms and the dense mesh
-// 238.4 -> 200.6 / 198.3 / 199.7 ms.
-#ifndef LUM_SUSPEND_LANES
-#define LUM_SUSPEND_LANES 8
-#endif
 template <bool COUNT, bool EXT = true, bool NEE = true, bool SPH = false, int SUSPEND = LUM_SUSPEND_LANES>
 __device__ __forceinline__ void tile_task(const SceneDev& S, const RenderDev& R, uint32_t x0, uint32_t y0,
                                           uint32_t tw, uint32_t th, uint32_t s_lo, uint32_t s_hi,

@@ -64,6 +64,9 @@ __device__ __forceinline__ void sample_pool(const SceneDev& S, const RenderDev& 
     uint32_t px = 0, k = 0, pixel = 0;
     Path P;
     Pending pend;
+    Hit h;                    // closest hit so far of the lane's walk
+    Trav tv;                  // place of a suspended walk
+    bool found = false, walking = false;
     for (;;) {
         if (state == ST_IDLE) {
             const uint32_t idx = atomicAdd(next, 1u);
@@ -86,12 +89,18 @@ __device__ __forceinline__ void sample_pool(const SceneDev& S, const RenderDev& 
             r.o = P.ray.o;
             r.d = shadow ? pend.dir : P.ray.d;
             r.time = shadow ? 0.0f : P.ray.time;                  // Ray::new (render.rs:1457)
-            Hit h;
-            h.t = shadow ? (EXT ? fabsf(pend.tmax) : pend.tmax) : CUDART_INF_F;
-            h.prim = -1;
-            h.b1 = h.b2 = 0.0f;
-            const bool found = trace<false, SPH>(S, r, 0.001f, shadow, h, stack, err);
-            if (shadow) {
+            if (!walking) {
+                h.t = shadow ? (EXT ? fabsf(pend.tmax) : pend.tmax) : CUDART_INF_F;
+                h.prim = -1;
+                h.b1 = h.b2 = 0.0f;
+                tv.node = S.n_nodes > 0 ? 0 : kSentinel;
+                tv.sp = 0;
+                found = false;
+            }
+            walking = !trace_resume<false, SPH, LUM_SUSPEND_LANES>(S, r, 0.001f, shadow, h, found, tv, stack, err);
+            if (walking) {
+                // suspended: resumes in a later iteration
+            } else if (shadow) {
                 ++nsh;
                 if (!found) P.L = P.L + pend.contrib;
                 shadow_done<EXT>(P, pend, exit_stash + lane);
