@@ -165,19 +165,24 @@ __device__ __forceinline__ bool hit_quad(float4 a, float4 b, float4 c, float4 d,
 }
 
 // triangle.rs:21-64 (Moller-Trumbore)
+// The barycentric bounds are tested on the numerators against the determinant (u = su / aa in
+// [0, 1] <=> su between 0 and aa, and likewise v >= 0, u + v <= 1), so the division is done only
+// for the few candidates that pass them; u, v and t are then the reference's f * numerator.
 __device__ __forceinline__ bool hit_tri(float4 a, float4 b, float4 c, const Ray& ray, float tmin, float tmax,
                                         float& t, float& bu, float& bv) {
     V e1 = xyz(b), e2 = xyz(c);
     V h = cross(ray.d, e2);
     float aa = dot(e1, h);
     if (fabsf(aa) < 1e-8f) return false;
-    float f = 1.0f / aa;
     V s = ray.o - xyz(a);
-    float u = f * dot(s, h);
-    if (!(u >= 0.0f && u <= 1.0f)) return false;
+    const float su = dot(s, h);
+    const float sg = aa > 0.0f ? 1.0f : -1.0f, da = fabsf(aa);   // numerators scaled to aa > 0
+    if (!(su * sg >= 0.0f && su * sg <= da)) return false;
     V q = cross(s, e1);
-    float v = f * dot(ray.d, q);
-    if (v < 0.0f || u + v > 1.0f) return false;
+    const float sv = dot(ray.d, q);
+    if (sv * sg < 0.0f || (su + sv) * sg > da) return false;
+    const float f = 1.0f / aa;
+    const float u = f * su, v = f * sv;
     float tt = f * dot(e2, q);
     if (!(tt >= tmin && tt <= tmax)) return false;
     t = tt;
