@@ -136,7 +136,14 @@ __device__ __forceinline__ void finish(const Tables& T, const Ctl* ctl, const Re
     atomicAdd(a + 1, (unsigned long long)fix(v.y));
     atomicAdd(a + 2, (unsigned long long)fix(v.z));
     atomicAdd(a + 3, (unsigned long long)fix(v.w));
-    unsigned long long k = atomicAdd(T.done_count + scene, 1ull) + 1ull;
+    // per-scene completion count: one atomic per scene among the warp's finishing lanes (every
+    // finishing path adding 1 to one of a few counters serialised on them)
+    const unsigned grp = __match_any_sync(__activemask(), scene);
+    const int lane = threadIdx.x & 31, leader = __ffs(grp) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(T.done_count + scene, (unsigned long long)__popc(grp));
+    base = __shfl_sync(grp, base, leader);
+    const unsigned long long k = base + (unsigned long long)__popc(grp & ((1u << lane) - 1u)) + 1ull;
     if (k == T.scene_total[scene]) {
         T.finish_ns[scene] = globaltimer();
         T.finish_iter[scene] = ctl->iteration;
