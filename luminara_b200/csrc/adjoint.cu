@@ -619,6 +619,9 @@ __global__ void __launch_bounds__(128, LUM_ADJ_MIN_BLOCKS) k_replay(SceneDev S, 
         V bg = mk(0.f, 0.f, 0.f);
         Path P;
         Pending pend;
+        Hit h;                  // closest hit so far of the lane's walk
+        Trav tv;                // place of a suspended walk
+        bool found = false, walking = false;
         for (;;) {
             if (state == A_IDLE && st < s_hi) {
                 start_path(S, R, gi, gj, pixel, st, P);
@@ -635,12 +638,18 @@ __global__ void __launch_bounds__(128, LUM_ADJ_MIN_BLOCKS) k_replay(SceneDev S, 
                 r.o = P.ray.o;
                 r.d = shadow ? pend.dir : P.ray.d;
                 r.time = shadow ? 0.0f : P.ray.time;
-                Hit h;
-                h.t = shadow ? pend.tmax : CUDART_INF_F;
-                h.prim = -1;
-                h.b1 = h.b2 = 0.0f;
-                const bool found = trace(S, r, 0.001f, shadow, h, stack, err);
-                if (shadow) {
+                if (!walking) {
+                    h.t = shadow ? pend.tmax : CUDART_INF_F;
+                    h.prim = -1;
+                    h.b1 = h.b2 = 0.0f;
+                    tv.node = S.n_nodes > 0 ? 0 : kSentinel;
+                    tv.sp = 0;
+                    found = false;
+                }
+                walking = !trace_resume<false, false, LUM_SUSPEND_LANES>(S, r, 0.001f, shadow, h, found, tv, stack, err);
+                if (walking) {
+                    // suspended: resumes in a later iteration
+                } else if (shadow) {
                     if (!found) {
                         P.L = P.L + pend.contrib;
                         vflags |= VF_VIS;
