@@ -382,7 +382,7 @@ __global__ void __launch_bounds__(kLogThreads) k_loglum(const float* __restrict_
 }
 
 template <bool VEC, int KIND>
-__global__ void __launch_bounds__(kThreads, 6) k_tonemap(const float* __restrict__ hdr, uint32_t w, uint32_t h, const __grid_constant__ Chain C,
+__global__ void __launch_bounds__(kThreads, 5) k_tonemap(const float* __restrict__ hdr, uint32_t w, uint32_t h, const __grid_constant__ Chain C,
                                                       double exposure, const double* __restrict__ partials,
                                                       uint8_t* __restrict__ rgba, const ByteTable T) {
     __shared__ double s_exposure;
@@ -408,12 +408,29 @@ __global__ void __launch_bounds__(kThreads, 6) k_tonemap(const float* __restrict
         uint4* out = reinterpret_cast<uint4*>(rgba);
         if (!C.extra && T.tab) {   // the common chain from its byte table (uniform branch, hoisted)
             const float ig = C.inv_gamma;
+            // the next quad's 48 bytes are requested before this quad is converted, so each
+            // thread keeps two quads of loads in flight across the grid-stride loop
+            float4 a, b, c;
+            if (t0 < n4) {
+                a = __ldcs(in + 3 * t0);
+                b = __ldcs(in + 3 * t0 + 1);
+                c = __ldcs(in + 3 * t0 + 2);
+            }
             for (uint32_t q = t0; q < n4; q += stride) {
-                const float4 a = __ldcs(in + 3 * q), b = __ldcs(in + 3 * q + 1), c = __ldcs(in + 3 * q + 2);
+                const uint32_t qn = q + stride;
+                float4 a2 = a, b2 = b, c2 = c;
+                if (qn < n4) {
+                    a2 = __ldcs(in + 3 * qn);
+                    b2 = __ldcs(in + 3 * qn + 1);
+                    c2 = __ldcs(in + 3 * qn + 2);
+                }
                 __stcs(out + q, make_uint4(pixel_table<KIND>(a.x, a.y, a.z, exposure, T, ig),
                                            pixel_table<KIND>(a.w, b.x, b.y, exposure, T, ig),
                                            pixel_table<KIND>(b.z, b.w, c.x, exposure, T, ig),
                                            pixel_table<KIND>(c.y, c.z, c.w, exposure, T, ig)));
+                a = a2;
+                b = b2;
+                c = c2;
             }
         } else if (!C.extra) {     // the common chain in f32 with the exact fallback
             const float ig = C.inv_gamma;
@@ -586,7 +603,11 @@ cudaError_t launch_tonemap(const float* hdr, uint32_t w, uint32_t h, const lum_t
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const size_t work = vec ? (n + 3) / 4 : n;
-    const int grid = (int)std::min<size_t>((work + tone::kThreads - 1) / tone::kThreads, (size_t)nsm * 64);
+    // the table path runs one wave of resident blocks looping over the frame (its loads run a quad
+    // ahead); the others one quad per thread
+    int per_sm = 5;
+    const int grid = (int)std::min<size_t>((work + tone::kThreads - 1) / tone::kThreads,
+                                           (size_t)nsm * (T.tab ? per_sm : 64));
     auto go = [&](auto kind) {
         constexpr int K = decltype(kind)::value;
         if (vec)
