@@ -25,7 +25,6 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
-#include <limits>
 #include <mutex>
 #include <type_traits>
 #include <vector>
@@ -284,42 +283,39 @@ __device__ __forceinline__ uint32_t tone_gamma_fast(float v, float exposure32, d
 // thresholds T_k = min{x : byte(x) >= k}, found once per (tone curve, gamma) on the host by
 // bisection over the f64 bit patterns with the reference's own f64 formulas (the host's libm
 // pow, as the f64 restatement uses) -- exact, not a fit.  The kernel finds x's byte from one
-// table entry: the bucket of x is its top 19 bits (sign, exponent, 7 mantissa bits; the high
-// word shifted right by 13), chosen so that no bucket holds two thresholds.  Entry i holds the
-// byte at the bucket's lower end and the bucket's threshold (+inf: none); x's byte is that base,
-// plus one if x reaches the threshold.  Entry 0 stands for every bucket below the first (and
-// for negative x, whose high word is negative), entry nb + 1 for every bucket above the last.
-// NaN, infinite and huge x take the f64 path as before.
+// table entry: positive doubles order like their bit patterns, and the bucket of x is its top
+// 19 bits (sign, exponent, 7 mantissa bits), chosen so that no bucket holds two thresholds.
+// Entry i (a u64): byte at the bucket's lower end in bits 56-63, the low 45 bits of the bucket's
+// threshold (or 2^45: none) in bits 0-45; x's byte is that base, plus one if x's low 45 bits reach
+// the threshold's.  Entry 0 stands for every bucket below the first, entry nb + 1 for every
+// bucket above the last.  Non-finite, huge or non-positive x take the f64 path as before.
 constexpr int kTabShift = 45;                                  // 52 - 7 mantissa bits
+constexpr unsigned long long kTabLowMask = (1ull << kTabShift) - 1ull;
 constexpr int kTabMaxEntries = 4096;                           // nb + 2 per table
 constexpr int kTabSlots = 16;                                  // (tone curve, gamma) pairs per device
 
-struct alignas(16) TabEntry {
-    double thr;                                                // threshold in the bucket, or +inf
-    uint32_t base;                                             // byte at the bucket's lower end
-    uint32_t pad;
-};
-
 struct ByteTable {
-    const TabEntry* tab;             // device address of the slot, or null: no table
-    int k0;                          // bucket key of entry 1
+    const unsigned long long* tab;   // device address of the slot, or null: no table
+    long long k0;                    // bucket key of entry 1
     int nb;                          // buckets with an entry of their own
 };
 
-static __device__ TabEntry g_byte_tables[kTabSlots][kTabMaxEntries];
+static __device__ __align__(256) unsigned long long g_byte_tables[kTabSlots][kTabMaxEntries];
 
 template <int KIND>
 __device__ __forceinline__ uint32_t tone_table(float v, double exposure, const ByteTable& T, float inv_gamma) {
     const double x = (double)v * exposure;
-    if (!(x < 1e30)) {                                         // NaN, inf, huge: the f64 chain
+    if (!(x > 0.0)) return 0u;                                 // NaN, zero and negatives: byte 0
+    if (!(x < 1e30)) {
         const double q64 = tone_gamma64(KIND, x, inv_gamma > 0.0f ? 1.0 / (double)inv_gamma : 0.0, 0.0);
         return q64 < 0.0 ? 0u : sat_u8(q64);
     }
-    const int key = (__double2hiint(x) >> (kTabShift - 32)) - T.k0 + 1;   // negative x: below
-    const int i = min(max(key, 0), T.nb + 1);
-    const double2 e = __ldg(reinterpret_cast<const double2*>(T.tab) + i);   // (thr, base | pad)
-    return (uint32_t)__double2loint(e.y) + (x >= e.x ? 1u : 0u);
+    const long long b = __double_as_longlong(x);
+    const long long i = min(max((b >> kTabShift) - T.k0 + 1, 0ll), (long long)T.nb + 1);
+    const unsigned long long e = __ldg(T.tab + i);
+    return (uint32_t)(e >> 56) + (((unsigned long long)b & kTabLowMask) >= (e & (2ull * kTabLowMask + 1ull)) ? 1u : 0u);
 }
+
 template <int KIND>
 __device__ __forceinline__ uint32_t pixel_table(float r, float g, float b, double exposure, const ByteTable& T,
                                                 float inv_gamma) {
@@ -382,7 +378,7 @@ __global__ void __launch_bounds__(kLogThreads) k_loglum(const float* __restrict_
 }
 
 template <bool VEC, int KIND>
-__global__ void __launch_bounds__(kThreads, 5) k_tonemap(const float* __restrict__ hdr, uint32_t w, uint32_t h, const __grid_constant__ Chain C,
+__global__ void __launch_bounds__(kThreads, 6) k_tonemap(const float* __restrict__ hdr, uint32_t w, uint32_t h, const __grid_constant__ Chain C,
                                                       double exposure, const double* __restrict__ partials,
                                                       uint8_t* __restrict__ rgba, const ByteTable T) {
     __shared__ double s_exposure;
@@ -408,29 +404,12 @@ __global__ void __launch_bounds__(kThreads, 5) k_tonemap(const float* __restrict
         uint4* out = reinterpret_cast<uint4*>(rgba);
         if (!C.extra && T.tab) {   // the common chain from its byte table (uniform branch, hoisted)
             const float ig = C.inv_gamma;
-            // the next quad's 48 bytes are requested before this quad is converted, so each
-            // thread keeps two quads of loads in flight across the grid-stride loop
-            float4 a, b, c;
-            if (t0 < n4) {
-                a = __ldcs(in + 3 * t0);
-                b = __ldcs(in + 3 * t0 + 1);
-                c = __ldcs(in + 3 * t0 + 2);
-            }
             for (uint32_t q = t0; q < n4; q += stride) {
-                const uint32_t qn = q + stride;
-                float4 a2 = a, b2 = b, c2 = c;
-                if (qn < n4) {
-                    a2 = __ldcs(in + 3 * qn);
-                    b2 = __ldcs(in + 3 * qn + 1);
-                    c2 = __ldcs(in + 3 * qn + 2);
-                }
+                const float4 a = __ldcs(in + 3 * q), b = __ldcs(in + 3 * q + 1), c = __ldcs(in + 3 * q + 2);
                 __stcs(out + q, make_uint4(pixel_table<KIND>(a.x, a.y, a.z, exposure, T, ig),
                                            pixel_table<KIND>(a.w, b.x, b.y, exposure, T, ig),
                                            pixel_table<KIND>(b.z, b.w, c.x, exposure, T, ig),
                                            pixel_table<KIND>(c.y, c.z, c.w, exposure, T, ig)));
-                a = a2;
-                b = b2;
-                c = c2;
             }
         } else if (!C.extra) {     // the common chain in f32 with the exact fallback
             const float ig = C.inv_gamma;
@@ -507,7 +486,7 @@ static double bdouble(long long b) {
 
 // Builds the entries of one table; false when the chain is not the step function the table
 // encodes (a bucket with two thresholds, too many buckets, or a byte that does not match).
-static bool build_byte_table(int kind, double gamma, std::vector<TabEntry>& ent, int& k0, int& nb) {
+static bool build_byte_table(int kind, double gamma, std::vector<unsigned long long>& ent, long long& k0, int& nb) {
     const long long top = dbits(1e30);
     std::vector<long long> th;                                  // bit patterns of T_1 .. T_bmax
     const uint32_t bmax = host_byte(kind, 1e30, gamma);
@@ -523,23 +502,25 @@ static bool build_byte_table(int kind, double gamma, std::vector<TabEntry>& ent,
         th.push_back(hi);
     }
     if (th.empty()) return false;
-    const long long kk0 = th.front() >> kTabShift, k1 = th.back() >> kTabShift;
-    if (k1 - kk0 + 3 > kTabMaxEntries) return false;
-    k0 = (int)kk0;
-    nb = (int)(k1 - kk0 + 1);
-    const double inf = std::numeric_limits<double>::infinity();
-    ent.assign(nb + 2, TabEntry{inf, 0u, 0u});
-    ent[nb + 1].base = bmax;                                    // above: the top byte
+    k0 = th.front() >> kTabShift;
+    const long long k1 = th.back() >> kTabShift;
+    nb = (int)(k1 - k0 + 1);
+    if (nb + 2 > kTabMaxEntries) return false;
+    ent.assign(nb + 2, 0ull);
+    ent[0] = 2ull * kTabLowMask + 1ull;                          // below: byte 0, no threshold
+    ent[nb + 1] = ((unsigned long long)bmax << 56) | (2ull * kTabLowMask + 1ull);
     size_t t = 0;                                               // thresholds at or below the bucket start
     for (int i = 0; i < nb; ++i) {
-        const long long key = kk0 + i, lo = key << kTabShift, hi = (key + 1) << kTabShift;
+        const long long key = k0 + i, lo = key << kTabShift, hi = (key + 1) << kTabShift;
         while (t < th.size() && th[t] <= lo) ++t;
-        if (host_byte(kind, bdouble(lo), gamma) != (uint32_t)t) return false;   // not monotone here
-        ent[i + 1].base = (uint32_t)t;
+        const uint32_t base = (uint32_t)t;
+        if (host_byte(kind, bdouble(lo), gamma) != base) return false;        // not monotone here
+        unsigned long long thr = 2ull * kTabLowMask + 1ull;     // none
         if (t < th.size() && th[t] < hi) {
             if (t + 1 < th.size() && th[t + 1] < hi) return false;            // two in one bucket
-            ent[i + 1].thr = bdouble(th[t]);
+            thr = (unsigned long long)th[t] & kTabLowMask;
         }
+        ent[i + 1] = ((unsigned long long)base << 56) | thr;
     }
     return true;
 }
@@ -566,13 +547,13 @@ static ByteTable byte_table(int kind, double gamma) {
         ++used;
     }
     TableSlot sl{dev, kind, gb, ByteTable{nullptr, 0, 0}};
-    std::vector<TabEntry> ent;
+    std::vector<unsigned long long> ent;
     void* base = nullptr;
     if (used < kTabSlots && build_byte_table(kind, gamma, ent, sl.T.k0, sl.T.nb) &&
         cudaGetSymbolAddress(&base, g_byte_tables) == cudaSuccess &&
-        cudaMemcpyToSymbol(g_byte_tables, ent.data(), ent.size() * sizeof(TabEntry),
-                           (size_t)used * kTabMaxEntries * sizeof(TabEntry)) == cudaSuccess)
-        sl.T.tab = static_cast<const TabEntry*>(base) + (size_t)used * kTabMaxEntries;
+        cudaMemcpyToSymbol(g_byte_tables, ent.data(), ent.size() * sizeof(unsigned long long),
+                           (size_t)used * kTabMaxEntries * sizeof(unsigned long long)) == cudaSuccess)
+        sl.T.tab = static_cast<const unsigned long long*>(base) + (size_t)used * kTabMaxEntries;
     cudaGetLastError();
     if (!sl.T.tab) sl.kind = -1 - kind;                         // remembered as "no table"
     slots.push_back(sl);
@@ -603,11 +584,7 @@ cudaError_t launch_tonemap(const float* hdr, uint32_t w, uint32_t h, const lum_t
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const size_t work = vec ? (n + 3) / 4 : n;
-    // the table path runs one wave of resident blocks looping over the frame (its loads run a quad
-    // ahead); the others one quad per thread
-    int per_sm = 5;
-    const int grid = (int)std::min<size_t>((work + tone::kThreads - 1) / tone::kThreads,
-                                           (size_t)nsm * (T.tab ? per_sm : 64));
+    const int grid = (int)std::min<size_t>((work + tone::kThreads - 1) / tone::kThreads, (size_t)nsm * 64);
     auto go = [&](auto kind) {
         constexpr int K = decltype(kind)::value;
         if (vec)
