@@ -116,6 +116,8 @@ struct SceneDev {
                              // Metal / Dielectric / Emissive (planes allowed): the SPH kernels apply
     int32_t stack_depth;     // traversal stack entries this BVH can need (<= kStackDepth)
     int32_t moving;          // some sphere moves: camera rays draw their time
+    int32_t cls;             // scene class of the general megakernel build (CLS_*, tracer.cuh)
+    int32_t pad_cls;
     const BlendEmit* blend_emit;   // emissive leaves of Blend materials
     const float* env;        // environment map, env_w * env_h RGB floats (or null)
     uint32_t env_w, env_h;

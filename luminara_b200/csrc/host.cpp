@@ -917,6 +917,23 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
     for (uint32_t i = 0; i < desc->n_materials && sph; ++i)
         sph = desc->materials[i].kind >= LUM_MAT_LAMBERTIAN && desc->materials[i].kind <= LUM_MAT_EMISSIVE;
     D.spheres_basic = sph ? 1 : 0;
+    // the scene class of the general megakernel build: the primitive types and light kinds
+    // present (planes are tested apart from the BVH in every class)
+    {
+        bool quad_only = true, mesh_only = true;
+        for (size_t k = 0; k < np; ++k) {
+            const int t = meta[k] & 15;
+            quad_only = quad_only && t == lum::PT_QUAD;
+            mesh_only = mesh_only && (t == lum::PT_TRIANGLE || t == lum::PT_DISK || t == lum::PT_FOG_SPHERE ||
+                                      t == lum::PT_FOG_BOX);
+        }
+        for (uint32_t i = 0; i < desc->n_lights; ++i) {
+            const int k = desc->lights[i].kind;
+            quad_only = quad_only && k == LUM_LIGHT_RECT;
+            mesh_only = mesh_only && (k == LUM_LIGHT_RECT || k == LUM_LIGHT_DISK);
+        }
+        D.cls = np == 0 ? 0 : quad_only ? 1 : mesh_only ? 2 : 0;   // CLS_QUAD, CLS_MESH, CLS_ALL
+    }
     D.moving = 0;
     for (size_t k = 0; k < np && !D.moving; ++k)
         D.moving = (meta[k] & 15) == lum::PT_SPHERE && prims[16 * k + 7] != 0.0f ? 1 : 0;

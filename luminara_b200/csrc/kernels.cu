@@ -57,7 +57,9 @@ __device__ __forceinline__ void flush_counters(WorkCounters* wc, uint32_t err, u
 // The SPH builds are small enough for more blocks per SM without spills (72 registers without
 // NEE, 80 with); their shared memory then fits when the traversal stack is sized to the scene's
 // BVH (SceneDev::stack_depth).
-template <bool COUNT, bool EXT, bool NEE, bool SPH>
+// CLS (CLS_QUAD, CLS_MESH): general builds carrying only the primitive tests and light samplers
+// of one scene class (SceneDev::cls).
+template <bool COUNT, bool EXT, bool NEE, bool SPH, int CLS = CLS_ALL>
 __global__ void __launch_bounds__(kRenderThreads, SPH ? (NEE ? 6 : 7) : LUM_RENDER_MIN_BLOCKS) k_render(SceneDev S, RenderDev R, float* __restrict__ out,
                                                            WorkCounters* wc, unsigned long long* __restrict__ gacc,
                                                            uint32_t n_groups, uint32_t group_strata) {
@@ -79,7 +81,7 @@ __global__ void __launch_bounds__(kRenderThreads, SPH ? (NEE ? 6 : 7) : LUM_REND
         const uint32_t tw = min(8u, R.w - x0), th = min(4u, R.h - y0);
         const uint32_t s_lo = R.s_begin + group * group_strata;
         const uint32_t s_hi = min(R.s_end, s_lo + group_strata);
-        tile_task<COUNT, EXT, NEE, SPH>(S, R, x0, y0, tw, th, s_lo, s_hi, s_acc[wid], &s_next[wid], s_exit[wid], stack,
+        tile_task<COUNT, EXT, NEE, SPH, LUM_SUSPEND_LANES, CLS>(S, R, x0, y0, tw, th, s_lo, s_hi, s_acc[wid], &s_next[wid], s_exit[wid], stack,
                                         err,
                               nseg, nsh, &tally);
         if (lane < (int)(tw * th)) {
@@ -218,7 +220,9 @@ static int render_occupancy() {
         for (auto fn : {k_render<false, false, false, false>, k_render<false, false, true, false>,
                         k_render<false, true, false, false>, k_render<false, true, true, false>,
                         k_render<false, false, false, true>, k_render<false, false, true, true>,
-                        k_render<true, false, true, false>, k_render<true, true, true, false>})
+                        k_render<true, false, true, false>, k_render<true, true, true, false>,
+                        k_render<false, false, false, false, CLS_QUAD>, k_render<false, false, true, false, CLS_QUAD>,
+                        k_render<false, false, false, false, CLS_MESH>, k_render<false, false, true, false, CLS_MESH>})
             cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stack_bytes(kRenderThreads));
         int o = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_render<false, false, true, false>, kRenderThreads,
@@ -277,8 +281,13 @@ static cudaError_t launch_render_t(const SceneDev& S, const RenderDev& R, float*
     }
     const bool nee = COUNT || S.n_lights > 0;
     const bool sph = !COUNT && !R.ext && S.spheres_basic;
+    const int cls = (COUNT || R.ext || sph) ? (int)CLS_ALL : S.cls;
     auto kernel = R.ext ? (nee ? k_render<COUNT, true, true, false> : k_render<COUNT, true, COUNT, false>)
                 : sph   ? (nee ? k_render<COUNT, false, true, !COUNT> : k_render<COUNT, false, COUNT, !COUNT>)
+                : cls == CLS_QUAD ? (nee ? k_render<COUNT, false, true, false, CLS_QUAD>
+                                         : k_render<COUNT, false, COUNT, false, CLS_QUAD>)
+                : cls == CLS_MESH ? (nee ? k_render<COUNT, false, true, false, CLS_MESH>
+                                         : k_render<COUNT, false, COUNT, false, CLS_MESH>)
                         : (nee ? k_render<COUNT, false, true, false> : k_render<COUNT, false, COUNT, false>);
     // the traversal stack sized to the scene's BVH; resident blocks for that size
     const size_t smem = (size_t)S.stack_depth * kRenderThreads * sizeof(int);

@@ -36,7 +36,8 @@ __device__ __forceinline__ void fixed_pixel(const unsigned long long* a, float e
 // the sums.  acc (32 x 4) and *next are the warp's shared memory; the call zeroes them.
 // EXT: the scene may use the other materials or backgrounds; NEE: it has lights; SPH: its
 // primitives are spheres and its materials the basic four (shade's and trace's template flags).
-template <bool COUNT, bool EXT = true, bool NEE = true, bool SPH = false, int SUSPEND = LUM_SUSPEND_LANES>
+template <bool COUNT, bool EXT = true, bool NEE = true, bool SPH = false, int SUSPEND = LUM_SUSPEND_LANES,
+          int CLS = CLS_ALL>
 __device__ __forceinline__ void tile_task(const SceneDev& S, const RenderDev& R, uint32_t x0, uint32_t y0,
                                           uint32_t tw, uint32_t th, uint32_t s_lo, uint32_t s_hi,
                                           unsigned long long (*acc)[4], uint32_t* next, V* exit_stash, int* stack,
@@ -82,7 +83,7 @@ __device__ __forceinline__ void tile_task(const SceneDev& S, const RenderDev& R,
                 tv.sp = 0;
                 found = false;
             }
-            walking = !trace_resume<COUNT, SPH, SUSPEND>(S, r, 0.001f, shadow, h, found, tv, stack, err, tally);
+            walking = !trace_resume<COUNT, SPH, SUSPEND, CLS>(S, r, 0.001f, shadow, h, found, tv, stack, err, tally);
             if (walking) {
                 // suspended: resumes in a later iteration
             } else if (shadow) {
@@ -92,7 +93,7 @@ __device__ __forceinline__ void tile_task(const SceneDev& S, const RenderDev& R,
                 state = P.bounce >= R.max_depth ? ST_DONE : ST_CLOSEST;
             } else {
                 ++nseg;
-                state = shade<-1, EXT, NEE, SPH>(S, R, pixel, P, found, h, pend, exit_stash + lane);
+                state = shade<-1, EXT, NEE, SPH, CLS>(S, R, pixel, P, found, h, pend, exit_stash + lane);
             }
         }
         if (state == ST_DONE) {

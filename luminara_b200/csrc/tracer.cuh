@@ -243,11 +243,30 @@ __device__ __forceinline__ bool hit_fog(int type, float4 a, float4 b, float4 c, 
     return true;
 }
 
+// Scene classes of the general megakernel build (CLS): the primitive types and NEE light kinds
+// the kernel carries code for.  A scene runs the smallest class that holds all its primitives
+// and lights (SceneDev::cls, chosen by lum_scene_create); code a scene cannot reach costs
+// instruction-fetch time in the megakernel.
+enum : int {
+    CLS_ALL = 0,    // every primitive type and light kind
+    CLS_QUAD = 1,   // quads (rects, boxes) with rect lights (box room, quad scenes)
+    CLS_MESH = 2    // triangles, disks and media with disk and rect lights (meshes)
+};
+template <int CLS>
+__host__ __device__ constexpr bool cls_has_prim(int type) {
+    return CLS == CLS_ALL || (CLS == CLS_QUAD && type == PT_QUAD) ||
+           (CLS == CLS_MESH && (type == PT_TRIANGLE || type == PT_DISK || type == PT_FOG_SPHERE || type == PT_FOG_BOX));
+}
+template <int CLS>
+__host__ __device__ constexpr bool cls_has_light(int kind) {   // 1 sphere, 2 rect, 3 disk
+    return CLS == CLS_ALL || (CLS == CLS_QUAD && kind == 2) || (CLS == CLS_MESH && (kind == 2 || kind == 3));
+}
+
 // One primitive test; updates the closest hit when t is within [tmin, hit.t].
 // SPH: the scene's primitives are all static spheres (SceneDev::spheres_basic), so the other
 // primitive tests are left out of the kernel and a test reads only record 0 (centre, radius).
 // ia_ray: 1 / |d|^2 of the ray, computed once per walk by the sphere-class build (0 elsewhere).
-template <bool COUNT = false, bool SPH = false>
+template <bool COUNT = false, bool SPH = false, int CLS = CLS_ALL>
 __device__ __forceinline__ bool test_prim(const SceneDev& S, int i, const Ray& ray, float tmin, Hit& hit,
                                           TestTally* tl = nullptr, float ia_ray = 0.0f) {
     float4 a = ldp(S, i, 0);
@@ -264,16 +283,19 @@ __device__ __forceinline__ bool test_prim(const SceneDev& S, int i, const Ray& r
     if constexpr (COUNT) tl->prim[type]++;
     switch (type) {
         case PT_SPHERE: {
+            if constexpr (!cls_has_prim<CLS>(PT_SPHERE)) return false;
             float4 b = ldp(S, i, 1);
             if (hit_sphere(a, b, ray, tmin, hit.t, t)) { hit.t = t; hit.prim = i; return true; }
             return false;
         }
         case PT_QUAD: {
+            if constexpr (!cls_has_prim<CLS>(PT_QUAD)) return false;
             float4 b = ldp(S, i, 1), c = ldp(S, i, 2), d = ldp(S, i, 3);
             if (hit_quad(a, b, c, d, ray, tmin, hit.t, t)) { hit.t = t; hit.prim = i; return true; }
             return false;
         }
         case PT_TRIANGLE: {
+            if constexpr (!cls_has_prim<CLS>(PT_TRIANGLE)) return false;
             float4 b = ldp(S, i, 1), c = ldp(S, i, 2);
             float bu, bv;
             if (hit_tri(a, b, c, ray, tmin, hit.t, t, bu, bv)) {
@@ -283,11 +305,13 @@ __device__ __forceinline__ bool test_prim(const SceneDev& S, int i, const Ray& r
             return false;
         }
         case PT_DISK: {
+            if constexpr (!cls_has_prim<CLS>(PT_DISK)) return false;
             float4 b = ldp(S, i, 1);
             if (hit_disk(a, b, ray, tmin, hit.t, t)) { hit.t = t; hit.prim = i; return true; }
             return false;
         }
         default: {
+            if constexpr (!cls_has_prim<CLS>(PT_FOG_BOX)) return false;
             float4 b = ldp(S, i, 1), c = ldp(S, i, 2);
             if (hit_fog(type, a, b, c, ray, tmin, hit.t, t)) { hit.t = t; hit.prim = i; return true; }
             return false;
@@ -332,7 +356,7 @@ struct Trav {
 // finished lanes idle).  Returns true when the walk is complete (planes tested, `found` final).
 // SUSPEND == 0 never stops early.  tv starts as {0, 0} (or kSentinel for a scene without
 // nodes), found as false.
-template <bool COUNT = false, bool SPH = false, int SUSPEND = 0>
+template <bool COUNT = false, bool SPH = false, int SUSPEND = 0, int CLS = CLS_ALL>
 __device__ __forceinline__ bool trace_resume(const SceneDev& S, const Ray& ray, float tmin, bool any, Hit& hit,
                                              bool& found, Trav& tv, int* stack, uint32_t& err,
                                              TestTally* tl = nullptr) {
@@ -394,7 +418,7 @@ __device__ __forceinline__ bool trace_resume(const SceneDev& S, const Ray& ray, 
             while (leaf < 0) {
                 const int first = (~leaf) >> 3, cnt = ((~leaf) & 7) + 1;
                 for (int k = 0; k < cnt; ++k) {
-                    if (test_prim<COUNT, SPH>(S, first + k, ray, tmin, hit, tl, ia_ray)) {
+                    if (test_prim<COUNT, SPH, CLS>(S, first + k, ray, tmin, hit, tl, ia_ray)) {
                         found = true;
                         if (any) {
                             tv.node = kSentinel;
@@ -463,7 +487,7 @@ struct Surface {
 };
 
 // Point, outward normal, face orientation and material of a hit (hit.rs:19-43).
-template <bool SPH = false>
+template <bool SPH = false, int CLS = CLS_ALL>
 __device__ __forceinline__ Surface surface_of(const SceneDev& S, const Ray& ray, const Hit& h) {
     Surface s;
     s.p = fma3(ray.d, h.t, ray.o);
@@ -479,6 +503,7 @@ __device__ __forceinline__ Surface surface_of(const SceneDev& S, const Ray& ray,
         float4 a = ldp(S, h.prim, 0);
         switch (type) {
             case PT_SPHERE: {
+                if constexpr (!cls_has_prim<CLS>(PT_SPHERE)) break;
                 V c = xyz(a);
                 if constexpr (!SPH) {
                     float4 b = ldp(S, h.prim, 1);
@@ -488,11 +513,13 @@ __device__ __forceinline__ Surface surface_of(const SceneDev& S, const Ray& ray,
                 break;
             }
             case PT_QUAD: {
+                if constexpr (!cls_has_prim<CLS>(PT_QUAD)) break;
                 float4 d = ldp(S, h.prim, 3);
                 on = unit(xyz(d)) * d.w;
                 break;
             }
             case PT_TRIANGLE: {
+                if constexpr (!cls_has_prim<CLS>(PT_TRIANGLE)) break;
                 float4 d = ldp(S, h.prim, 3);
                 int si = __float_as_int(d.w);
                 if (si >= 0) {
@@ -504,7 +531,9 @@ __device__ __forceinline__ Surface surface_of(const SceneDev& S, const Ray& ray,
                 }
                 break;
             }
-            case PT_DISK: on = xyz(ldp(S, h.prim, 1)); break;
+            case PT_DISK:
+                if constexpr (cls_has_prim<CLS>(PT_DISK)) on = xyz(ldp(S, h.prim, 1));
+                break;
             default: on = mk(1.0f, 0.0f, 0.0f); break;                 // constant_medium.rs:63
         }
     }
@@ -870,6 +899,7 @@ __device__ __forceinline__ void build_onb(V n, V& a, V& b) {
 
 // Samples one light (render.rs:1346-1455).  Returns false when the sample contributes
 // nothing before visibility; otherwise the shadow ray and unoccluded contribution.
+template <int CLS = CLS_ALL>
 __device__ __forceinline__ bool sample_light(const SceneDev& S, V hp, V normal, V albedo, float4 u, Ray& shadow,
                                              float& shadow_tmax, V& contrib) {
     int nl = S.n_lights;
@@ -877,7 +907,8 @@ __device__ __forceinline__ bool sample_light(const SceneDev& S, V hp, V normal, 
     const LightDev& L = S.lights[idx];
     V lp, ln;
     float area;
-    if (L.kind == 1) {
+    if (!cls_has_light<CLS>(L.kind)) return false;                      // not in this build's class
+    if (cls_has_light<CLS>(1) && L.kind == 1) {
         V to_c = mk(L.p0) - hp;
         float d2c = len2(to_c);
         if (d2c < L.radius * L.radius) return false;
@@ -908,11 +939,11 @@ __device__ __forceinline__ bool sample_light(const SceneDev& S, V hp, V normal, 
         ln = unit(lp - mk(L.p0));
         float solid = 2.0f * CUDART_PI_F * (1.0f - ctm);
         area = solid * t * t / fmaxf(fabsf(dot(-dir, ln)), 0.001f);
-    } else if (L.kind == 2) {
+    } else if (cls_has_light<CLS>(2) && L.kind == 2) {
         lp = mk(L.p0) + mk(L.u) * u.z + mk(L.v) * u.w;
         area = L.area;
         ln = mk(L.n);
-    } else {
+    } else if constexpr (cls_has_light<CLS>(3)) {
         float r = sqrtf(u.z) * L.radius;
         float sp, cp;
         sincospif(2.0f * u.w, &sp, &cp);
@@ -923,6 +954,8 @@ __device__ __forceinline__ bool sample_light(const SceneDev& S, V hp, V normal, 
         lp = mk(L.p0) + ut * (r * cp) + vt * (r * sp);
         area = L.area;
         ln = w;
+    } else {
+        return false;
     }
     V tl = lp - hp;
     float d2 = len2(tl);
@@ -1144,7 +1177,7 @@ __device__ __forceinline__ void shadow_done(Path& P, Pending& pend, const V* exi
 // known to be unoccluded.  Returns the lane's next state.
 // NEE = false builds the shading step of scenes without lights: no light-sampling code in the
 // kernel (the megakernel runs ~11% faster on a light-free scene without it: instruction fetch).
-template <int KIND = -1, bool EXT = true, bool NEE = true, bool SPH = false>
+template <int KIND = -1, bool EXT = true, bool NEE = true, bool SPH = false, int CLS = CLS_ALL>
 __device__ __forceinline__ int shade(const SceneDev& S, const RenderDev& R, uint32_t pixel, Path& P, bool found,
                                      const Hit& h, Pending& pend, V* exit_stash = nullptr) {
     if (!found) {
@@ -1152,7 +1185,7 @@ __device__ __forceinline__ int shade(const SceneDev& S, const RenderDev& R, uint
         return ST_DONE;
     }
     const uint32_t depth = R.max_depth - P.bounce;
-    Surface sf = surface_of<SPH>(S, P.ray, h);
+    Surface sf = surface_of<SPH, CLS>(S, P.ray, h);
     // A non-finite hit point (e.g. a fog hit at t = inf along a zero-length direction, where
     // the reference's distance test compares against NaN) makes this level's result NaN in
     // the reference, which its guard turns into zero for the level and everything deeper
@@ -1196,7 +1229,7 @@ __device__ __forceinline__ int shade(const SceneDev& S, const RenderDev& R, uint
     if (use_nee) {
         Ray sr;
         V contrib;
-        if (sample_light(S, sf.p, sf.n, sc.att, nu, sr, pend.tmax, contrib)) {
+        if (sample_light<CLS>(S, sf.p, sf.n, sc.att, nu, sr, pend.tmax, contrib)) {
             pend.dir = sr.d;
             pend.contrib = mul(P.beta, contrib);
             shadow = !has_nan(pend.contrib);
