@@ -44,6 +44,30 @@ struct BvhResult {
     uint32_t n_leaves = 0;
 };
 
+// A 4-wide node (128 bytes, 8 x float4), collapsed from the binary tree for large meshes:
+//   [0..5] lo.x, hi.x, lo.y, hi.y, lo.z, hi.z of the four children (structure of arrays)
+//   [6]    the four child links (inner 4-wide node index >= 0, or a leaf encoded as in NodeDev;
+//          an unused slot has a zero-volume box at the origin, which no ray enters)
+//   [7]    order[2]: for each of the 8 ray-direction octants (bit 0: d.x < 0, bit 1: d.y < 0,
+//          bit 2: d.z < 0) one byte of four 2-bit child slots, nearest first along that octant's
+//          diagonal, so a walk visits hit children near to far without sorting them.
+struct alignas(16) Node4Dev {
+    float lox[4], hix[4], loy[4], hiy[4], loz[4], hiz[4];
+    int32_t link[4];
+    uint32_t order[2];
+    uint32_t pad[2];
+};
+static_assert(sizeof(Node4Dev) == 128, "4-wide node layout");
+
+// Collapses a binary tree into 4-wide nodes: each node takes its binary children and, while it
+// has fewer than four, replaces the inner child of largest surface area by that child's two
+// children.  Leaves (primitive ranges) stay as they are.  max_depth is the 4-wide tree's depth.
+struct Bvh4Result {
+    std::vector<Node4Dev> nodes;
+    uint32_t max_depth = 0;
+};
+Bvh4Result collapse_bvh4(const std::vector<NodeDev>& nodes2);
+
 // Builds a binned-SAH BVH over `boxes` (centroids are box centres).  `prim_cost`, if given,
 // holds one weight per box: the relative cost of that primitive's intersection test in the SAH
 // (1 when absent).  Deterministic for a given input regardless of the thread count.

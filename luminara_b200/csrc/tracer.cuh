@@ -356,7 +356,11 @@ struct Trav {
 // finished lanes idle).  Returns true when the walk is complete (planes tested, `found` final).
 // SUSPEND == 0 never stops early.  tv starts as {0, 0} (or kSentinel for a scene without
 // nodes), found as false.
-template <bool COUNT = false, bool SPH = false, int SUSPEND = 0, int CLS = CLS_ALL>
+// WIDE: the walk runs over the scene's 4-wide tree (SceneDev::nodes4, Node4Dev) instead of the
+// binary one: one visit slab-tests four children, pushes the hit ones far to near in the order
+// the node stores for the ray's direction octant (no sort), and continues with the nearest.
+// Leaves, postponement and suspension work as in the binary walk.
+template <bool COUNT = false, bool SPH = false, int SUSPEND = 0, int CLS = CLS_ALL, bool WIDE = false>
 __device__ __forceinline__ bool trace_resume(const SceneDev& S, const Ray& ray, float tmin, bool any, Hit& hit,
                                              bool& found, Trav& tv, int* stack, uint32_t& err,
                                              TestTally* tl = nullptr) {
@@ -371,13 +375,65 @@ __device__ __forceinline__ bool trace_resume(const SceneDev& S, const Ray& ray, 
         // the sphere class divides by |d|^2 once per walk instead of once per sphere test
         float ia_ray = 0.0f;
         if constexpr (SPH && !COUNT) ia_ray = 1.0f / len2(ray.d);
-        const float4* nodes = reinterpret_cast<const float4*>(S.nodes);
+        const float4* nodes = reinterpret_cast<const float4*>(WIDE ? S.nodes4 : S.nodes);
         const int stride = blockDim.x;
+        const int stack_cap = WIDE ? S.stack_depth4 : S.stack_depth;
+        // direction octant of the ray (4-wide walks: the nodes' child order for it)
+        const uint32_t oct = (ray.d.x < 0.0f ? 1u : 0u) | (ray.d.y < 0.0f ? 2u : 0u) | (ray.d.z < 0.0f ? 4u : 0u);
         int sp = tv.sp;
         int node = tv.node;   // inner node index, leaf (< 0) or kSentinel
         int leaf = 0;         // postponed leaf (< 0) or 0
         for (;;) {
             while ((unsigned)node < (unsigned)kSentinel) {
+              if constexpr (WIDE) {
+                const float4* nd = nodes + 8 * node;
+                const float4 lx = __ldg(nd + 0), hx = __ldg(nd + 1), ly = __ldg(nd + 2), hy = __ldg(nd + 3);
+                const float4 lz = __ldg(nd + 4), hz = __ldg(nd + 5);
+                const int4 lk = __ldg(reinterpret_cast<const int4*>(nd + 6));
+                const uint2 od = __ldg(reinterpret_cast<const uint2*>(nd + 7));
+                if constexpr (COUNT) tl->node += 2;                    // four boxes = two binary visits
+                auto slab = [&](float x0, float x1, float y0, float y1, float z0, float z1) {
+                    const float a0 = fmaf(x0, ix, ox), a1 = fmaf(x1, ix, ox);
+                    const float b0 = fmaf(y0, iy, oy), b1 = fmaf(y1, iy, oy);
+                    const float c0 = fmaf(z0, iz, oz), c1 = fmaf(z1, iz, oz);
+                    const float en = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), tmin));
+                    const float ex = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), hit.t));
+                    return en < ex;
+                };
+                // (unused slots, link kSentinel, are left out even for a ray whose NaN coordinates
+                // would pass every slab test)
+                const uint32_t mask = (slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x) && lk.x != kSentinel ? 1u : 0u) |
+                                      (slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y) && lk.y != kSentinel ? 2u : 0u) |
+                                      (slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z) && lk.z != kSentinel ? 4u : 0u) |
+                                      (slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w) && lk.w != kSentinel ? 8u : 0u);
+                if (mask == 0u) {
+                    node = sp > 0 ? stack[--sp * stride] : kSentinel;
+                } else {
+                    const uint32_t ord = ((oct & 4u) ? od.y : od.x) >> (8u * (oct & 3u));
+                    int next = kSentinel;
+#pragma unroll
+                    for (int j = 3; j >= 0; --j) {                      // far to near
+                        const uint32_t sl = (ord >> (2 * j)) & 3u;
+                        if ((mask >> sl) & 1u) {
+                            if (next != kSentinel) {
+                                if (sp < stack_cap) {
+                                    stack[sp++ * stride] = next;
+                                } else {
+                                    err |= LUM_KERR_STACK_OVERFLOW;
+                                }
+                            }
+                            next = sl == 0u ? lk.x : sl == 1u ? lk.y : sl == 2u ? lk.z : lk.w;
+                        }
+                    }
+                    node = next;
+                }
+                if (node < 0 && leaf == 0) {
+                    leaf = node;
+                    node = sp > 0 ? stack[--sp * stride] : kSentinel;
+                }
+                if (!__any_sync(__activemask(), leaf == 0)) break;
+                continue;
+              }
                 float4 n0 = __ldg(nodes + 4 * node + 0);
                 float4 n1 = __ldg(nodes + 4 * node + 1);
                 float4 n2 = __ldg(nodes + 4 * node + 2);
