@@ -311,13 +311,11 @@ int emit4(const std::vector<NodeDev>& n2, int i2, std::vector<Node4Dev>& out, ui
     Node4Dev nd{};
     for (int k = 0; k < 4; ++k) {
         const bool used = k < n;
-        nd.lox[k] = used ? ch[k].lo[0] : 0.0f;
-        nd.hix[k] = used ? ch[k].hi[0] : 0.0f;
-        nd.loy[k] = used ? ch[k].lo[1] : 0.0f;
-        nd.hiy[k] = used ? ch[k].hi[1] : 0.0f;
-        nd.loz[k] = used ? ch[k].lo[2] : 0.0f;
-        nd.hiz[k] = used ? ch[k].hi[2] : 0.0f;
-        nd.link[k] = used ? ch[k].link : 0x7fffffff;
+        for (int a = 0; a < 3; ++a) {
+            nd.c[k].lo[a] = used ? ch[k].lo[a] : 0.0f;
+            nd.c[k].hi[a] = used ? ch[k].hi[a] : 0.0f;
+        }
+        nd.c[k].link = used ? ch[k].link : 0x7fffffff;
     }
     // nearest-first slot order per octant: by the child box centre's projection on the octant's
     // diagonal (unused slots last)
@@ -326,15 +324,16 @@ int emit4(const std::vector<NodeDev>& n2, int i2, std::vector<Node4Dev>& out, ui
         int slot[4] = {0, 1, 2, 3};
         float key[4];
         for (int k = 0; k < 4; ++k)
-            key[k] = k < n ? dx * (nd.lox[k] + nd.hix[k]) + dy * (nd.loy[k] + nd.hiy[k]) + dz * (nd.loz[k] + nd.hiz[k])
+            key[k] = k < n ? dx * (nd.c[k].lo[0] + nd.c[k].hi[0]) + dy * (nd.c[k].lo[1] + nd.c[k].hi[1]) +
+                                 dz * (nd.c[k].lo[2] + nd.c[k].hi[2])
                            : std::numeric_limits<float>::infinity();
         std::stable_sort(slot, slot + 4, [&](int a, int b) { return key[a] < key[b]; });
         uint32_t byte = 0;
         for (int j = 0; j < 4; ++j) byte |= (uint32_t)slot[j] << (2 * j);
-        nd.order[o >> 2] |= byte << (8 * (o & 3));
+        nd.c[o >> 2].word |= byte << (8 * (o & 3));
     }
     for (int k = 0; k < n; ++k)
-        if (ch[k].link >= 0) nd.link[k] = emit4(n2, ch[k].link, out, depth + 1, max_depth);
+        if (ch[k].link >= 0) nd.c[k].link = emit4(n2, ch[k].link, out, depth + 1, max_depth);
     out[me] = nd;
     return me;
 }

@@ -44,18 +44,23 @@ struct BvhResult {
     uint32_t n_leaves = 0;
 };
 
-// A 4-wide node (128 bytes, 8 x float4), collapsed from the binary tree for large meshes:
-//   [0..5] lo.x, hi.x, lo.y, hi.y, lo.z, hi.z of the four children (structure of arrays)
-//   [6]    the four child links (inner 4-wide node index >= 0, or a leaf encoded as in NodeDev;
-//          an unused slot has a zero-volume box at the origin, which no ray enters)
-//   [7]    order[2]: for each of the 8 ray-direction octants (bit 0: d.x < 0, bit 1: d.y < 0,
-//          bit 2: d.z < 0) one byte of four 2-bit child slots, nearest first along that octant's
-//          diagonal, so a walk visits hit children near to far without sorting them.
+// A 4-wide node (128 bytes, 8 x float4), collapsed from the binary tree for large meshes.
+// Child k occupies float4s 2k and 2k + 1, so a visit can test one child at a time:
+//   [2k]     lo.x, lo.y, lo.z, link (the child's link as int bits: inner 4-wide node index >= 0,
+//            a leaf encoded as in NodeDev, or kSentinel for an unused slot, whose zero-volume box
+//            at the origin no ray enters)
+//   [2k + 1] hi.x, hi.y, hi.z, word: children 0 and 1 carry the node's child orders, for each of
+//            the 8 ray-direction octants (bit 0: d.x < 0, bit 1: d.y < 0, bit 2: d.z < 0) one byte
+//            of four 2-bit child slots, nearest first along that octant's diagonal (octants 0-3
+//            in child 0's word, 4-7 in child 1's), so a walk visits hit children near to far
+//            without sorting them.
 struct alignas(16) Node4Dev {
-    float lox[4], hix[4], loy[4], hiy[4], loz[4], hiz[4];
-    int32_t link[4];
-    uint32_t order[2];
-    uint32_t pad[2];
+    struct {
+        float lo[3];
+        int32_t link;
+        float hi[3];
+        uint32_t word;
+    } c[4];
 };
 static_assert(sizeof(Node4Dev) == 128, "4-wide node layout");
 

@@ -387,29 +387,26 @@ __device__ __forceinline__ bool trace_resume(const SceneDev& S, const Ray& ray, 
             while ((unsigned)node < (unsigned)kSentinel) {
               if constexpr (WIDE) {
                 const float4* nd = nodes + 8 * node;
-                const float4 lx = __ldg(nd + 0), hx = __ldg(nd + 1), ly = __ldg(nd + 2), hy = __ldg(nd + 3);
-                const float4 lz = __ldg(nd + 4), hz = __ldg(nd + 5);
-                const int4 lk = __ldg(reinterpret_cast<const int4*>(nd + 6));
-                const uint2 od = __ldg(reinterpret_cast<const uint2*>(nd + 7));
                 if constexpr (COUNT) tl->node += 2;                    // four boxes = two binary visits
-                auto slab = [&](float x0, float x1, float y0, float y1, float z0, float z1) {
-                    const float a0 = fmaf(x0, ix, ox), a1 = fmaf(x1, ix, ox);
-                    const float b0 = fmaf(y0, iy, oy), b1 = fmaf(y1, iy, oy);
-                    const float c0 = fmaf(z0, iz, oz), c1 = fmaf(z1, iz, oz);
+                uint32_t mask = 0u, ord = 0u;
+                int lk[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {                          // one child at a time
+                    const float4 A = __ldg(nd + 2 * k), B = __ldg(nd + 2 * k + 1);
+                    lk[k] = __float_as_int(A.w);
+                    if (k == (int)(oct >> 2)) ord = __float_as_uint(B.w) >> (8u * (oct & 3u));
+                    const float a0 = fmaf(A.x, ix, ox), a1 = fmaf(B.x, ix, ox);
+                    const float b0 = fmaf(A.y, iy, oy), b1 = fmaf(B.y, iy, oy);
+                    const float c0 = fmaf(A.z, iz, oz), c1 = fmaf(B.z, iz, oz);
                     const float en = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), tmin));
                     const float ex = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), hit.t));
-                    return en < ex;
-                };
-                // (unused slots, link kSentinel, are left out even for a ray whose NaN coordinates
-                // would pass every slab test)
-                const uint32_t mask = (slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x) && lk.x != kSentinel ? 1u : 0u) |
-                                      (slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y) && lk.y != kSentinel ? 2u : 0u) |
-                                      (slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z) && lk.z != kSentinel ? 4u : 0u) |
-                                      (slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w) && lk.w != kSentinel ? 8u : 0u);
+                    // (an unused slot, link kSentinel, is left out even for a ray whose NaN
+                    // coordinates would pass every slab test)
+                    if (en < ex && lk[k] != kSentinel) mask |= 1u << k;
+                }
                 if (mask == 0u) {
                     node = sp > 0 ? stack[--sp * stride] : kSentinel;
                 } else {
-                    const uint32_t ord = ((oct & 4u) ? od.y : od.x) >> (8u * (oct & 3u));
                     int next = kSentinel;
 #pragma unroll
                     for (int j = 3; j >= 0; --j) {                      // far to near
@@ -422,7 +419,7 @@ __device__ __forceinline__ bool trace_resume(const SceneDev& S, const Ray& ray, 
                                     err |= LUM_KERR_STACK_OVERFLOW;
                                 }
                             }
-                            next = sl == 0u ? lk.x : sl == 1u ? lk.y : sl == 2u ? lk.z : lk.w;
+                            next = sl == 0u ? lk[0] : sl == 1u ? lk[1] : sl == 2u ? lk[2] : lk[3];
                         }
                     }
                     node = next;
