@@ -260,92 +260,4 @@ BvhResult build_bvh(const std::vector<BuildBox>& boxes, const BvhOptions& option
     return res;
 }
 
-namespace {
-
-struct Child4 {
-    float lo[3], hi[3];
-    int32_t link;
-};
-
-float child_area(const Child4& c) {
-    const float dx = c.hi[0] - c.lo[0], dy = c.hi[1] - c.lo[1], dz = c.hi[2] - c.lo[2];
-    return 2.0f * (dx * dy + dy * dz + dz * dx);
-}
-
-// The two children of binary node i.
-void children2(const std::vector<NodeDev>& n2, int i, Child4 out[2]) {
-    const NodeDev& n = n2[i];
-    for (int c = 0; c < 2; ++c) {
-        const float* xy = c == 0 ? n.n0 : n.n1;
-        out[c].lo[0] = xy[0];
-        out[c].hi[0] = xy[1];
-        out[c].lo[1] = xy[2];
-        out[c].hi[1] = xy[3];
-        out[c].lo[2] = n.n2[2 * c];
-        out[c].hi[2] = n.n2[2 * c + 1];
-        out[c].link = n.link[c];
-    }
-}
-
-int emit4(const std::vector<NodeDev>& n2, int i2, std::vector<Node4Dev>& out, uint32_t depth, uint32_t& max_depth) {
-    Child4 ch[4];
-    int n = 2;
-    children2(n2, i2, ch);
-    while (n < 4) {                    // open the inner child of largest area
-        int best = -1;
-        float best_a = -1.0f;
-        for (int k = 0; k < n; ++k)
-            if (ch[k].link >= 0 && child_area(ch[k]) > best_a) {
-                best_a = child_area(ch[k]);
-                best = k;
-            }
-        if (best < 0) break;
-        Child4 sub[2];
-        children2(n2, ch[best].link, sub);
-        ch[best] = sub[0];
-        ch[n++] = sub[1];
-    }
-    const int me = (int)out.size();
-    out.emplace_back();
-    max_depth = std::max(max_depth, depth + 1);
-    Node4Dev nd{};
-    for (int k = 0; k < 4; ++k) {
-        const bool used = k < n;
-        for (int a = 0; a < 3; ++a) {
-            nd.c[k].lo[a] = used ? ch[k].lo[a] : 0.0f;
-            nd.c[k].hi[a] = used ? ch[k].hi[a] : 0.0f;
-        }
-        nd.c[k].link = used ? ch[k].link : 0x7fffffff;
-    }
-    // nearest-first slot order per octant: by the child box centre's projection on the octant's
-    // diagonal (unused slots last)
-    for (int o = 0; o < 8; ++o) {
-        const float dx = (o & 1) ? -1.0f : 1.0f, dy = (o & 2) ? -1.0f : 1.0f, dz = (o & 4) ? -1.0f : 1.0f;
-        int slot[4] = {0, 1, 2, 3};
-        float key[4];
-        for (int k = 0; k < 4; ++k)
-            key[k] = k < n ? dx * (nd.c[k].lo[0] + nd.c[k].hi[0]) + dy * (nd.c[k].lo[1] + nd.c[k].hi[1]) +
-                                 dz * (nd.c[k].lo[2] + nd.c[k].hi[2])
-                           : std::numeric_limits<float>::infinity();
-        std::stable_sort(slot, slot + 4, [&](int a, int b) { return key[a] < key[b]; });
-        uint32_t byte = 0;
-        for (int j = 0; j < 4; ++j) byte |= (uint32_t)slot[j] << (2 * j);
-        nd.c[o >> 2].word |= byte << (8 * (o & 3));
-    }
-    for (int k = 0; k < n; ++k)
-        if (ch[k].link >= 0) nd.c[k].link = emit4(n2, ch[k].link, out, depth + 1, max_depth);
-    out[me] = nd;
-    return me;
-}
-
-}  // namespace
-
-Bvh4Result collapse_bvh4(const std::vector<NodeDev>& nodes2) {
-    Bvh4Result r;
-    if (nodes2.empty()) return r;
-    r.nodes.reserve(nodes2.size() / 2 + 1);
-    emit4(nodes2, 0, r.nodes, 0, r.max_depth);
-    return r;
-}
-
 }  // namespace lum

@@ -117,10 +117,7 @@ struct SceneDev {
     int32_t stack_depth;     // traversal stack entries this BVH can need (<= kStackDepth)
     int32_t moving;          // some sphere moves: camera rays draw their time
     int32_t cls;             // scene class of the general megakernel build (CLS_*, tracer.cuh)
-    int32_t stack_depth4;    // traversal stack entries the 4-wide tree can need (<= kStackDepth)
-    const void* nodes4;      // float4[8 * n_nodes4]: 4-wide tree of a large mesh, or null
-    int32_t n_nodes4;
-    int32_t pad_n4;
+    int32_t pad_cls;
     const BlendEmit* blend_emit;   // emissive leaves of Blend materials
     const float* env;        // environment map, env_w * env_h RGB floats (or null)
     uint32_t env_w, env_h;

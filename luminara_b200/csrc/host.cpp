@@ -863,21 +863,7 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
         std::memcpy(&prims012[12 * k], &prims[16 * k], 12 * sizeof(float));
         std::memcpy(&prims3[4 * k], &prims[16 * k + 12], 4 * sizeof(float));
     }
-    // Large meshes also get the 4-wide tree (the megakernel's mesh build walks it; every other
-    // kernel walks the binary tree): triangles, disks and media only, with disk and rect lights,
-    // at least kWideMinPrims primitives.
-    constexpr size_t kWideMinPrims = 100000;
-    bool mesh_class = np >= kWideMinPrims;
-    for (size_t k = 0; k < np && mesh_class; ++k) {
-        const int t = F.prims[bvh.order[k]].type;
-        mesh_class = t == lum::PT_TRIANGLE || t == lum::PT_DISK || t == lum::PT_FOG_SPHERE || t == lum::PT_FOG_BOX;
-    }
-    for (uint32_t i = 0; i < desc->n_lights && mesh_class; ++i)
-        mesh_class = desc->lights[i].kind == LUM_LIGHT_RECT || desc->lights[i].kind == LUM_LIGHT_DISK;
-    lum::Bvh4Result bvh4;
-    if (mesh_class) bvh4 = lum::collapse_bvh4(bvh.nodes);
-    size_t off_nodes4 = align256(off_nodes + bvh.nodes.size() * sizeof(lum::NodeDev));
-    size_t off_prims = align256(off_nodes4 + bvh4.nodes.size() * sizeof(lum::Node4Dev));
+    size_t off_prims = align256(off_nodes + bvh.nodes.size() * sizeof(lum::NodeDev));
     size_t off_prims3 = align256(off_prims + prims012.size() * sizeof(float));
     size_t off_meta = align256(off_prims3 + prims3.size() * sizeof(float));
     size_t off_orig = align256(off_meta + meta.size() * 4);
@@ -897,7 +883,6 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
         return cudaMemcpy(base + off, src, bytes, cudaMemcpyHostToDevice);
     };
     if ((ce = up(off_nodes, bvh.nodes.data(), bvh.nodes.size() * sizeof(lum::NodeDev))) != cudaSuccess ||
-        (ce = up(off_nodes4, bvh4.nodes.data(), bvh4.nodes.size() * sizeof(lum::Node4Dev))) != cudaSuccess ||
         (ce = up(off_prims, prims012.data(), prims012.size() * 4)) != cudaSuccess ||
         (ce = up(off_prims3, prims3.data(), prims3.size() * 4)) != cudaSuccess ||
         (ce = up(off_meta, meta.data(), meta.size() * 4)) != cudaSuccess ||
@@ -921,10 +906,6 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
     D.planes = (const lum::PlaneDev*)(base + off_planes);
     D.blend_emit = (const lum::BlendEmit*)(base + off_blend);
     D.n_nodes = (int32_t)bvh.nodes.size();
-    D.nodes4 = bvh4.nodes.empty() ? nullptr : base + off_nodes4;
-    D.n_nodes4 = (int32_t)bvh4.nodes.size();
-    // a 4-wide visit can push three entries
-    D.stack_depth4 = (int32_t)std::min<uint32_t>((uint32_t)lum::kStackDepth, 3u * bvh4.max_depth + 1u);
     D.n_prims = (int32_t)np;
     D.n_lights = (int32_t)lights.size();
     D.n_planes = (int32_t)F.planes.size();
@@ -964,7 +945,6 @@ lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out) {
     if (const char* sb = std::getenv("LUM_STACK_BUDGET")) {
         const long b = std::strtol(sb, nullptr, 10);
         if (b >= 1 && b < D.stack_depth) D.stack_depth = (int32_t)b;
-        if (b >= 1 && b < D.stack_depth4) D.stack_depth4 = (int32_t)b;
     }
     D.cam = make_camera(desc->camera);
     s->n_prims = (uint32_t)(np + F.planes.size());

@@ -59,12 +59,8 @@ __device__ __forceinline__ void flush_counters(WorkCounters* wc, uint32_t err, u
 // BVH (SceneDev::stack_depth).
 // CLS (CLS_QUAD, CLS_MESH): general builds carrying only the primitive tests and light samplers
 // of one scene class (SceneDev::cls).
-// WIDE: walks over the scene's 4-wide tree (large meshes; CLS_MESH builds only).
-#ifndef LUM_WIDE_MIN_BLOCKS
-#define LUM_WIDE_MIN_BLOCKS LUM_RENDER_MIN_BLOCKS
-#endif
-template <bool COUNT, bool EXT, bool NEE, bool SPH, int CLS = CLS_ALL, bool WIDE = false>
-__global__ void __launch_bounds__(kRenderThreads, SPH ? (NEE ? 6 : 7) : WIDE ? LUM_WIDE_MIN_BLOCKS : LUM_RENDER_MIN_BLOCKS) k_render(SceneDev S, RenderDev R, float* __restrict__ out,
+template <bool COUNT, bool EXT, bool NEE, bool SPH, int CLS = CLS_ALL>
+__global__ void __launch_bounds__(kRenderThreads, SPH ? (NEE ? 6 : 7) : LUM_RENDER_MIN_BLOCKS) k_render(SceneDev S, RenderDev R, float* __restrict__ out,
                                                            WorkCounters* wc, unsigned long long* __restrict__ gacc,
                                                            uint32_t n_groups, uint32_t group_strata) {
     extern __shared__ int s_stack[];
@@ -85,7 +81,7 @@ __global__ void __launch_bounds__(kRenderThreads, SPH ? (NEE ? 6 : 7) : WIDE ? L
         const uint32_t tw = min(8u, R.w - x0), th = min(4u, R.h - y0);
         const uint32_t s_lo = R.s_begin + group * group_strata;
         const uint32_t s_hi = min(R.s_end, s_lo + group_strata);
-        tile_task<COUNT, EXT, NEE, SPH, LUM_SUSPEND_LANES, CLS, WIDE>(S, R, x0, y0, tw, th, s_lo, s_hi, s_acc[wid], &s_next[wid], s_exit[wid], stack,
+        tile_task<COUNT, EXT, NEE, SPH, LUM_SUSPEND_LANES, CLS>(S, R, x0, y0, tw, th, s_lo, s_hi, s_acc[wid], &s_next[wid], s_exit[wid], stack,
                                         err,
                               nseg, nsh, &tally);
         if (lane < (int)(tw * th)) {
@@ -226,9 +222,7 @@ static int render_occupancy() {
                         k_render<false, false, false, true>, k_render<false, false, true, true>,
                         k_render<true, false, true, false>, k_render<true, true, true, false>,
                         k_render<false, false, false, false, CLS_QUAD>, k_render<false, false, true, false, CLS_QUAD>,
-                        k_render<false, false, false, false, CLS_MESH>, k_render<false, false, true, false, CLS_MESH>,
-                        k_render<false, false, false, false, CLS_MESH, true>,
-                        k_render<false, false, true, false, CLS_MESH, true>, k_render<true, false, true, false, CLS_MESH, true>})
+                        k_render<false, false, false, false, CLS_MESH>, k_render<false, false, true, false, CLS_MESH>})
             cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stack_bytes(kRenderThreads));
         int o = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_render<false, false, true, false>, kRenderThreads,
@@ -288,12 +282,7 @@ static cudaError_t launch_render_t(const SceneDev& S, const RenderDev& R, float*
     const bool nee = COUNT || S.n_lights > 0;
     const bool sph = !COUNT && !R.ext && S.spheres_basic;
     const int cls = (COUNT || R.ext || sph) ? (int)CLS_ALL : S.cls;
-    // a large mesh walks its 4-wide tree (the counter build too, so the counts are of that walk)
-    const bool wide = !R.ext && !sph && S.cls == CLS_MESH && S.nodes4 != nullptr;
-    auto kernel = wide  ? (COUNT ? k_render<COUNT, false, true, false, CLS_MESH, true>
-                           : nee ? k_render<COUNT, false, true, false, CLS_MESH, true>
-                                 : k_render<COUNT, false, COUNT, false, CLS_MESH, true>)
-                : R.ext ? (nee ? k_render<COUNT, true, true, false> : k_render<COUNT, true, COUNT, false>)
+    auto kernel = R.ext ? (nee ? k_render<COUNT, true, true, false> : k_render<COUNT, true, COUNT, false>)
                 : sph   ? (nee ? k_render<COUNT, false, true, !COUNT> : k_render<COUNT, false, COUNT, !COUNT>)
                 : cls == CLS_QUAD ? (nee ? k_render<COUNT, false, true, false, CLS_QUAD>
                                          : k_render<COUNT, false, COUNT, false, CLS_QUAD>)
@@ -301,7 +290,7 @@ static cudaError_t launch_render_t(const SceneDev& S, const RenderDev& R, float*
                                          : k_render<COUNT, false, COUNT, false, CLS_MESH>)
                         : (nee ? k_render<COUNT, false, true, false> : k_render<COUNT, false, COUNT, false>);
     // the traversal stack sized to the scene's BVH; resident blocks for that size
-    const size_t smem = (size_t)(wide ? S.stack_depth4 : S.stack_depth) * kRenderThreads * sizeof(int);
+    const size_t smem = (size_t)S.stack_depth * kRenderThreads * sizeof(int);
     if (blocks_per_sm == occ) blocks_per_sm = kernel_occupancy((const void*)kernel, smem);
     int grid = num_sms() * blocks_per_sm;
     const uint64_t tasks = (uint64_t)R.n_tasks * grp.n_groups;

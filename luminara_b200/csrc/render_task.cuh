@@ -37,7 +37,7 @@ __device__ __forceinline__ void fixed_pixel(const unsigned long long* a, float e
 // EXT: the scene may use the other materials or backgrounds; NEE: it has lights; SPH: its
 // primitives are spheres and its materials the basic four (shade's and trace's template flags).
 template <bool COUNT, bool EXT = true, bool NEE = true, bool SPH = false, int SUSPEND = LUM_SUSPEND_LANES,
-          int CLS = CLS_ALL, bool WIDE = false>
+          int CLS = CLS_ALL>
 __device__ __forceinline__ void tile_task(const SceneDev& S, const RenderDev& R, uint32_t x0, uint32_t y0,
                                           uint32_t tw, uint32_t th, uint32_t s_lo, uint32_t s_hi,
                                           unsigned long long (*acc)[4], uint32_t* next, V* exit_stash, int* stack,
@@ -79,12 +79,11 @@ __device__ __forceinline__ void tile_task(const SceneDev& S, const RenderDev& R,
                 h.t = shadow ? (EXT ? fabsf(pend.tmax) : pend.tmax) : CUDART_INF_F;
                 h.prim = -1;
                 h.b1 = h.b2 = 0.0f;
-                tv.node = (WIDE ? S.n_nodes4 : S.n_nodes) > 0 ? 0 : kSentinel;
+                tv.node = S.n_nodes > 0 ? 0 : kSentinel;
                 tv.sp = 0;
                 found = false;
             }
-            walking = !trace_resume<COUNT, SPH, SUSPEND, CLS, WIDE>(S, r, 0.001f, shadow, h, found, tv, stack, err,
-                                                                   tally);
+            walking = !trace_resume<COUNT, SPH, SUSPEND, CLS>(S, r, 0.001f, shadow, h, found, tv, stack, err, tally);
             if (walking) {
                 // suspended: resumes in a later iteration
             } else if (shadow) {

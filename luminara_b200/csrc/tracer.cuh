@@ -356,11 +356,7 @@ struct Trav {
 // finished lanes idle).  Returns true when the walk is complete (planes tested, `found` final).
 // SUSPEND == 0 never stops early.  tv starts as {0, 0} (or kSentinel for a scene without
 // nodes), found as false.
-// WIDE: the walk runs over the scene's 4-wide tree (SceneDev::nodes4, Node4Dev) instead of the
-// binary one: one visit slab-tests four children, pushes the hit ones far to near in the order
-// the node stores for the ray's direction octant (no sort), and continues with the nearest.
-// Leaves, postponement and suspension work as in the binary walk.
-template <bool COUNT = false, bool SPH = false, int SUSPEND = 0, int CLS = CLS_ALL, bool WIDE = false>
+template <bool COUNT = false, bool SPH = false, int SUSPEND = 0, int CLS = CLS_ALL>
 __device__ __forceinline__ bool trace_resume(const SceneDev& S, const Ray& ray, float tmin, bool any, Hit& hit,
                                              bool& found, Trav& tv, int* stack, uint32_t& err,
                                              TestTally* tl = nullptr) {
@@ -375,62 +371,13 @@ __device__ __forceinline__ bool trace_resume(const SceneDev& S, const Ray& ray, 
         // the sphere class divides by |d|^2 once per walk instead of once per sphere test
         float ia_ray = 0.0f;
         if constexpr (SPH && !COUNT) ia_ray = 1.0f / len2(ray.d);
-        const float4* nodes = reinterpret_cast<const float4*>(WIDE ? S.nodes4 : S.nodes);
+        const float4* nodes = reinterpret_cast<const float4*>(S.nodes);
         const int stride = blockDim.x;
-        const int stack_cap = WIDE ? S.stack_depth4 : S.stack_depth;
-        // direction octant of the ray (4-wide walks: the nodes' child order for it)
-        const uint32_t oct = (ray.d.x < 0.0f ? 1u : 0u) | (ray.d.y < 0.0f ? 2u : 0u) | (ray.d.z < 0.0f ? 4u : 0u);
         int sp = tv.sp;
         int node = tv.node;   // inner node index, leaf (< 0) or kSentinel
         int leaf = 0;         // postponed leaf (< 0) or 0
         for (;;) {
             while ((unsigned)node < (unsigned)kSentinel) {
-              if constexpr (WIDE) {
-                const float4* nd = nodes + 8 * node;
-                if constexpr (COUNT) tl->node += 2;                    // four boxes = two binary visits
-                uint32_t mask = 0u, ord = 0u;
-                int lk[4];
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {                          // one child at a time
-                    const float4 A = __ldg(nd + 2 * k), B = __ldg(nd + 2 * k + 1);
-                    lk[k] = __float_as_int(A.w);
-                    if (k == (int)(oct >> 2)) ord = __float_as_uint(B.w) >> (8u * (oct & 3u));
-                    const float a0 = fmaf(A.x, ix, ox), a1 = fmaf(B.x, ix, ox);
-                    const float b0 = fmaf(A.y, iy, oy), b1 = fmaf(B.y, iy, oy);
-                    const float c0 = fmaf(A.z, iz, oz), c1 = fmaf(B.z, iz, oz);
-                    const float en = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), tmin));
-                    const float ex = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), hit.t));
-                    // (an unused slot, link kSentinel, is left out even for a ray whose NaN
-                    // coordinates would pass every slab test)
-                    if (en < ex && lk[k] != kSentinel) mask |= 1u << k;
-                }
-                if (mask == 0u) {
-                    node = sp > 0 ? stack[--sp * stride] : kSentinel;
-                } else {
-                    int next = kSentinel;
-#pragma unroll
-                    for (int j = 3; j >= 0; --j) {                      // far to near
-                        const uint32_t sl = (ord >> (2 * j)) & 3u;
-                        if ((mask >> sl) & 1u) {
-                            if (next != kSentinel) {
-                                if (sp < stack_cap) {
-                                    stack[sp++ * stride] = next;
-                                } else {
-                                    err |= LUM_KERR_STACK_OVERFLOW;
-                                }
-                            }
-                            next = sl == 0u ? lk[0] : sl == 1u ? lk[1] : sl == 2u ? lk[2] : lk[3];
-                        }
-                    }
-                    node = next;
-                }
-                if (node < 0 && leaf == 0) {
-                    leaf = node;
-                    node = sp > 0 ? stack[--sp * stride] : kSentinel;
-                }
-                if (!__any_sync(__activemask(), leaf == 0)) break;
-                continue;
-              }
                 float4 n0 = __ldg(nodes + 4 * node + 0);
                 float4 n1 = __ldg(nodes + 4 * node + 1);
                 float4 n2 = __ldg(nodes + 4 * node + 2);

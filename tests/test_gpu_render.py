@@ -229,11 +229,10 @@ def test_panorama_camera_matches_keyed_oracle(name):
     b.close()
 
 
-def test_large_mesh_four_wide_walk_matches_keyed_oracle():
-    """A mesh of 327,680 triangles (above the size at which lum_scene_create also builds the
-    4-wide tree that the megakernel's mesh build walks): keyed parity with the oracle, which
-    walks its own binary tree, and the ray-set entry point (binary tree) agrees with the oracle
-    on camera rays.  Fog-free, as the keyed mesh test above."""
+def test_large_mesh_matches_keyed_oracle():
+    """A mesh of 327,680 triangles through the megakernel's mesh-class build: keyed parity with
+    the oracle (which builds its own binary tree, one triangle per leaf) and traced segment and
+    shadow-ray counts within 1%.  Fog-free, as the keyed mesh test above."""
     world, cfg = W.dense_mesh(level=7, width=64, height=36, spp=4, fog=False)
     world.camera.aspect_ratio = 64 / 36
     assert world.n_prims() > 300000
