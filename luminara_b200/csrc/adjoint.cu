@@ -563,6 +563,8 @@ constexpr uint32_t kReplayStrata = 8;   // strata per replay task (tile x stratu
 // one 8x4 tile and a group of kReplayStrata strata.  Each path's vertices and head go to the
 // chunk's slots: slot = ((tile - t0) * n_strata + s) * 32 + lane, vertex k of a slot at
 // verts[k * n_slots + slot].
+// CLS: the scene class (tracer.cuh), as for the megakernel's class builds.
+template <int CLS>
 __global__ void __launch_bounds__(128, LUM_ADJ_MIN_BLOCKS) k_replay(SceneDev S, RenderDev R, const float* __restrict__ dldi,
                                                                   uint32_t t0, uint32_t t1, PathHead* __restrict__ heads,
                                                                   Vert* __restrict__ verts, size_t n_slots,
@@ -646,7 +648,8 @@ __global__ void __launch_bounds__(128, LUM_ADJ_MIN_BLOCKS) k_replay(SceneDev S, 
                     tv.sp = 0;
                     found = false;
                 }
-                walking = !trace_resume<false, false, LUM_SUSPEND_LANES>(S, r, 0.001f, shadow, h, found, tv, stack, err);
+                walking = !trace_resume<false, false, LUM_SUSPEND_LANES, CLS>(S, r, 0.001f, shadow, h, found, tv, stack,
+                                                                             err);
                 if (walking) {
                     // suspended: resumes in a later iteration
                 } else if (shadow) {
@@ -664,11 +667,11 @@ __global__ void __launch_bounds__(128, LUM_ADJ_MIN_BLOCKS) k_replay(SceneDev S, 
                     const Ray in = P.ray;
                     const V B = P.beta;
                     const bool skip = P.skip_emission;
-                    Surface sf = surface_of(S, in, h);
+                    Surface sf = surface_of<false, CLS>(S, in, h);
                     const bool finite = isfinite(sf.p.x) && isfinite(sf.p.y) && isfinite(sf.p.z);
                     const uint32_t b0 = P.bounce;
                     // the adjoint rejects the other materials: the base-material shading
-                    const int stt = shade<-1, false>(S, R, pixel, P, true, h, pend);
+                    const int stt = shade<-1, false, true, false, CLS>(S, R, pixel, P, true, h, pend);
                     if (finite) {
                         Vert& vx = verts[(size_t)K * n_slots + slot];
                         vx.p = sf.p;
@@ -832,8 +835,10 @@ lum_status lum_backward(lum_scene* scene, const lum_render_params* params, const
         cudaGetDevice(&devi);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, devi);
         const size_t stack = (size_t)kStackDepth * 128 * sizeof(int);
+        auto replay = dev.cls == CLS_QUAD ? adj::k_replay<CLS_QUAD>
+                    : dev.cls == CLS_MESH ? adj::k_replay<CLS_MESH> : adj::k_replay<CLS_ALL>;
         int occ_r = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_r, adj::k_replay, 128, stack);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_r, replay, 128, stack);
         // Gradients accumulate per block in shared memory when the material table fits
         // (LUM_ADJ_GRADS=smem|global overrides), else with global atomics.
         int use_smem = bytes_g <= 64 * 1024 ? 1 : 0;
@@ -854,7 +859,7 @@ lum_status lum_backward(lum_scene* scene, const lum_render_params* params, const
             const size_t slots = (size_t)(c1 - c0) * 32 * n_st;
             e = cudaMemsetAsync(&wc->next_task, 0, sizeof(uint32_t), stream);
             if (e == cudaSuccess) {
-                adj::k_replay<<<grid_r, 128, stack, stream>>>(dev, R, d_img, c0, c1, d_heads, d_verts, n_slots, d_ws, wc);
+                replay<<<grid_r, 128, stack, stream>>>(dev, R, d_img, c0, c1, d_heads, d_verts, n_slots, d_ws, wc);
                 e = cudaGetLastError();
             }
             if (e == cudaSuccess) {
