@@ -124,6 +124,23 @@ struct SceneDev {
     CameraDev cam;
 };
 
+// Task list of one megakernel launch.  The frame's 8x4 tiles are numbered row-major; tiles
+// [0, n_whole) are one task each (every stratum), tiles [n_whole, n_tiles) are split into
+// n_groups tasks of group_strata consecutive strata (the last group may be shorter).  Whole
+// tiles come first, so the launch ends on short tasks.
+//   pix_sums   non-null: every task adds its sums to these per-pixel fixed-point sums (4 u64 per
+//              pixel) and no pixels are written (raw-sum renders);
+//   tile_sums  otherwise the split tiles' tasks add their sums here (128 u64 per split tile: 32
+//              pixels x 4; zeroed before the launch), and k_split_finalize writes their pixels.
+struct TaskPlan {
+    uint32_t n_whole;
+    uint32_t n_groups;
+    uint32_t group_strata;
+    uint32_t n_total;          // tasks: n_whole + (n_tiles - n_whole) * n_groups
+    unsigned long long* pix_sums;
+    unsigned long long* tile_sums;
+};
+
 // Test counts of the counter build (node visits test two child boxes each).
 struct alignas(16) TestTally {
     unsigned long long node;

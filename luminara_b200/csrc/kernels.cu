@@ -47,22 +47,22 @@ __device__ __forceinline__ void flush_counters(WorkCounters* wc, uint32_t err, u
     }
 }
 
-// Persistent megakernel.  Each warp takes tasks from a global counter: an 8x4 pixel tile and a
-// group of its strata (all of them, unless the frame is small: render_groups).  tile_task
-// (render_task.cuh) runs the task with the warp's lanes drawing (pixel, stratum) pairs from one
-// pool and adding each finished path to the tile's fixed-point pixel sums.  An ungrouped task
-// then writes its pixels; a grouped one adds its sums to the frame's fixed-point accumulators,
-// which k_fixed_finalize turns into pixels.  Integer sums make the image deterministic and the
-// same whether or not the frame was grouped.
+// Persistent megakernel.  Each warp takes tasks of the launch's TaskPlan from a global counter:
+// an 8x4 pixel tile and all of its strata, or, for the split tiles at the end of the list, a
+// group of them.  tile_task (render_task.cuh) runs the task with the warp's lanes drawing
+// (pixel, stratum) pairs from one pool and adding each finished path to the tile's fixed-point
+// pixel sums.  A whole tile's task then writes its pixels; a split tile's tasks add their sums
+// to the tile's sums in global memory, which k_split_finalize turns into pixels (raw-sum
+// renders add every task's sums to the per-pixel sums instead).  Integer sums make the image
+// deterministic and the same however the frame was split.
 // The SPH builds are small enough for more blocks per SM without spills (72 registers without
 // NEE, 80 with); their shared memory then fits when the traversal stack is sized to the scene's
 // BVH (SceneDev::stack_depth).
 // CLS (CLS_QUAD, CLS_MESH): general builds carrying only the primitive tests and light samplers
 // of one scene class (SceneDev::cls).
 template <bool COUNT, bool EXT, bool NEE, bool SPH, int CLS = CLS_ALL>
-__global__ void __launch_bounds__(kRenderThreads, SPH ? (NEE ? 6 : 7) : LUM_RENDER_MIN_BLOCKS) k_render(SceneDev S, RenderDev R, float* __restrict__ out,
-                                                           WorkCounters* wc, unsigned long long* __restrict__ gacc,
-                                                           uint32_t n_groups, uint32_t group_strata) {
+__global__ void __launch_bounds__(kRenderThreads, SPH ? (NEE ? 6 : 7) : LUM_RENDER_MIN_BLOCKS)
+    k_render(SceneDev S, RenderDev R, float* __restrict__ out, WorkCounters* wc, TaskPlan TP) {
     extern __shared__ int s_stack[];
     __shared__ unsigned long long s_acc[kRenderThreads / 32][32][4];
     __shared__ uint32_t s_next[kRenderThreads / 32];
@@ -75,20 +75,28 @@ __global__ void __launch_bounds__(kRenderThreads, SPH ? (NEE ? 6 : 7) : LUM_REND
         uint32_t task = 0;
         if (lane == 0) task = atomicAdd(&wc->next_task, 1u);
         task = __shfl_sync(kFull, task, 0);
-        if (task >= R.n_tasks * n_groups) break;
-        const uint32_t tile = task / n_groups, group = task - tile * n_groups;
+        if (task >= TP.n_total) break;
+        uint32_t tile, s_lo = R.s_begin, s_hi = R.s_end;
+        if (task < TP.n_whole) {
+            tile = task;
+        } else {
+            const uint32_t t2 = task - TP.n_whole;
+            const uint32_t k = t2 / TP.n_groups, g = t2 - k * TP.n_groups;
+            tile = TP.n_whole + k;
+            s_lo = R.s_begin + g * TP.group_strata;
+            s_hi = min(R.s_end, s_lo + TP.group_strata);
+        }
         const uint32_t x0 = (tile % R.tiles_x) * 8, y0 = (tile / R.tiles_x) * 4;
         const uint32_t tw = min(8u, R.w - x0), th = min(4u, R.h - y0);
-        const uint32_t s_lo = R.s_begin + group * group_strata;
-        const uint32_t s_hi = min(R.s_end, s_lo + group_strata);
-        tile_task<COUNT, EXT, NEE, SPH, LUM_SUSPEND_LANES, CLS>(S, R, x0, y0, tw, th, s_lo, s_hi, s_acc[wid], &s_next[wid], s_exit[wid], stack,
-                                        err,
-                              nseg, nsh, &tally);
+        tile_task<COUNT, EXT, NEE, SPH, LUM_SUSPEND_LANES, CLS>(S, R, x0, y0, tw, th, s_lo, s_hi, s_acc[wid],
+                                                                &s_next[wid], s_exit[wid], stack, err, nseg, nsh,
+                                                                &tally);
         if (lane < (int)(tw * th)) {
             const uint32_t i = x0 + lane % tw, j = y0 + lane / tw;
             const unsigned long long* a = s_acc[wid][lane];
-            if (gacc) {                   // grouped frames and raw-sum renders
-                unsigned long long* g = gacc + 4 * ((size_t)j * R.w + i);
+            if (TP.pix_sums || task >= TP.n_whole) {   // raw-sum renders; split tiles
+                unsigned long long* g = TP.pix_sums ? TP.pix_sums + 4 * ((size_t)j * R.w + i)
+                                                    : TP.tile_sums + 128 * (size_t)(tile - TP.n_whole) + 4 * lane;
                 for (int c = 0; c < 4; ++c) atomicAdd(g + c, a[c]);
             } else {
                 fixed_pixel(a, R.exposure, out + 3 * ((size_t)j * R.w + i));
@@ -104,7 +112,21 @@ __global__ void __launch_bounds__(kRenderThreads, SPH ? (NEE ? 6 : 7) : LUM_REND
     }
 }
 
-// Pixels of a grouped frame from its fixed-point accumulators.
+// Pixels of the split tiles (TaskPlan::tile_sums): one thread per pixel slot of a split tile.
+__global__ void k_split_finalize(RenderDev R, TaskPlan TP, uint32_t n_split, float* __restrict__ out) {
+    const uint32_t n_tiles = TP.n_whole + n_split;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < 32u * n_split; q += gridDim.x * blockDim.x) {
+        const uint32_t k = q >> 5, p = q & 31u, tile = TP.n_whole + k;
+        if (tile >= n_tiles) break;
+        const uint32_t x0 = (tile % R.tiles_x) * 8, y0 = (tile / R.tiles_x) * 4;
+        const uint32_t tw = min(8u, R.w - x0), th = min(4u, R.h - y0);
+        if (p >= tw * th) continue;
+        const uint32_t i = x0 + p % tw, j = y0 + p / tw;
+        fixed_pixel(TP.tile_sums + 128 * (size_t)k + 4 * p, R.exposure, out + 3 * ((size_t)j * R.w + i));
+    }
+}
+
+// Pixels from per-pixel fixed-point sums (the raw-sum renders' finalize).
 __global__ void k_fixed_finalize(const unsigned long long* __restrict__ gacc, size_t n_px, float exposure,
                                  float* __restrict__ out) {
     for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < n_px; p += (size_t)gridDim.x * blockDim.x)
@@ -246,37 +268,106 @@ static int kernel_occupancy(const void* fn, size_t smem) {
     return occ;
 }
 
+// Task plans.  A frame with fewer 8x4 tiles than LUM_SMALL_FRAME_TILES per resident warp splits
+// every tile into stratum groups until the launch has about LUM_SMALL_FRAME_TASKS tasks per
+// warp (groups of at least LUM_MIN_GROUP_STRATA strata), and widens the groups to
+// LUM_PREF_GROUP_STRATA strata where the launch keeps LUM_SMALL_FRAME_TILES tasks per warp: a
+// task ends when its warp's slowest lane does, so very short tasks pay that wait too often, but
+// a launch with fewer tasks than warps leaves SMs idle.  Measured on B200 (kernel time):
+//   512x512 x 64 spp quads (8192 tiles)     2 groups of 32 strata 10.26 ms, 4 of 16  9.66 ms
+//   256x256 x 64 spp box room (2048 tiles)  7 groups of 10        1.99 ms, 14 of 5   2.02 ms,
+//                                           8 of 8                 1.94 ms
+//   128x128 x 16 spp box room (512 tiles)   4 groups of 4          0.29 ms, 2 of 8    0.43 ms
+// A larger frame can also split its last LUM_TAIL_TILES_PER_WARP x (resident warps) tiles into
+// LUM_TAIL_GROUPS groups, so that the launch ends on short tasks; on the 1080p frames (spheres
+// 256 spp, dense mesh 144 spp) that gained nothing -- the warps still running at the end of a
+// launch issue faster as the others exit -- so it is off (0).
+#ifndef LUM_SMALL_FRAME_TILES
+#define LUM_SMALL_FRAME_TILES 4
+#endif
+#ifndef LUM_SMALL_FRAME_TASKS
+#define LUM_SMALL_FRAME_TASKS 8
+#endif
+#ifndef LUM_MIN_GROUP_STRATA
+#define LUM_MIN_GROUP_STRATA 4
+#endif
+#ifndef LUM_PREF_GROUP_STRATA
+#define LUM_PREF_GROUP_STRATA 8
+#endif
+#ifndef LUM_TAIL_TILES_PER_WARP
+#define LUM_TAIL_TILES_PER_WARP 0
+#endif
+#ifndef LUM_TAIL_GROUPS
+#define LUM_TAIL_GROUPS 8
+#endif
+
+// Scratch bytes of one split tile: 32 pixels x 4 fixed-point sums.
+constexpr size_t kSplitTileBytes = 32 * 4 * sizeof(unsigned long long);
+
 RenderGroups render_groups(const RenderDev& R) {
-    RenderGroups g{1, R.s_end > R.s_begin ? R.s_end - R.s_begin : 0};
-    const uint32_t n_st = g.group_strata;
-    if (R.n_tasks == 0 || n_st == 0) return g;
+    const uint32_t n_st = R.s_end > R.s_begin ? R.s_end - R.s_begin : 0;
+    RenderGroups g{1, n_st, R.n_tasks};
+    if (R.n_tasks == 0 || n_st < 2) return g;
     const uint64_t warps = (uint64_t)num_sms() * render_occupancy() * (kRenderThreads / 32);
-    // Only frames with fewer tiles than ~4 per resident warp split (groups of >= 4 strata until
-    // they have that many tasks): a task ends when its warp's slowest lane does, so shorter tasks
-    // pay that imbalance more often; on a large frame (1080p, 256 spp) 64-strata tasks were 2%
-    // slower than whole tiles.
-    uint64_t groups = 1;
-    if ((uint64_t)R.n_tasks < 4 * warps && n_st >= 8)
-        groups = std::min<uint64_t>((4 * warps + R.n_tasks - 1) / R.n_tasks, n_st / 4);
-    if (groups <= 1) return g;
+    uint64_t groups, split;
+    if ((uint64_t)R.n_tasks < (uint64_t)LUM_SMALL_FRAME_TILES * warps) {
+        groups = ((uint64_t)LUM_SMALL_FRAME_TASKS * warps + R.n_tasks - 1) / R.n_tasks;
+        groups = std::min<uint64_t>(groups, n_st / LUM_MIN_GROUP_STRATA);
+        const uint64_t wide = n_st / LUM_PREF_GROUP_STRATA;   // groups of the preferred size
+        if (groups > wide && wide * R.n_tasks >= (uint64_t)LUM_SMALL_FRAME_TILES * warps) groups = wide;
+        split = R.n_tasks;
+    } else {
+        groups = std::min<uint64_t>(LUM_TAIL_GROUPS, n_st / LUM_MIN_GROUP_STRATA);
+        split = std::min<uint64_t>(R.n_tasks, (uint64_t)LUM_TAIL_TILES_PER_WARP * warps);
+    }
+    if (groups <= 1 || split == 0) return g;
     g.group_strata = (uint32_t)((n_st + groups - 1) / groups);
     g.n_groups = (n_st + g.group_strata - 1) / g.group_strata;   // no empty group
+    g.n_whole = R.n_tasks - (uint32_t)split;
     return g;
 }
 
-// sums_only: the launch leaves the frame's fixed-point sums in gacc (zeroed first) and writes no
-// pixels.  Otherwise gacc is non-null only for a grouped frame (n_groups > 1).
+size_t render_scratch_bytes(const RenderDev& R, const RenderGroups& g) {
+    if (g.n_groups <= 1 || g.n_whole >= R.n_tasks) return 0;
+    return (size_t)(R.n_tasks - g.n_whole) * kSplitTileBytes;
+}
+
+// The megakernel launch of plan `grp`.  pix_sums non-null: the launch leaves the frame's
+// fixed-point sums there (zeroed first) and writes no pixels.  Otherwise split tiles need
+// `scratch` (render_scratch_bytes); only as many tiles are split as its `scratch_bytes` hold,
+// the others are rendered whole.
 template <bool COUNT>
 static cudaError_t launch_render_t(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
-                                   cudaStream_t stream, int blocks_per_sm, unsigned long long* gacc, RenderGroups grp,
-                                   bool sums_only = false) {
+                                   cudaStream_t stream, int blocks_per_sm, RenderGroups grp, void* scratch,
+                                   size_t scratch_bytes, unsigned long long* pix_sums) {
     const int occ = render_occupancy();
     if (blocks_per_sm <= 0) blocks_per_sm = occ;
-    if (!gacc || grp.n_groups < 1) grp = RenderGroups{1, R.s_end > R.s_begin ? R.s_end - R.s_begin : 0};
-    if (!sums_only && grp.n_groups <= 1) gacc = nullptr;
-    const size_t n_px = (size_t)R.w * R.h;
-    if (gacc) {
-        cudaError_t e = cudaMemsetAsync(gacc, 0, 32 * n_px, stream);
+    const uint32_t n_tiles = R.n_tasks;
+    const uint32_t n_st = R.s_end > R.s_begin ? R.s_end - R.s_begin : 0;
+    TaskPlan TP{};
+    TP.n_whole = n_tiles;
+    TP.n_groups = 1;
+    TP.group_strata = n_st;
+    if (grp.n_groups > 1 && grp.n_whole < n_tiles) {
+        uint64_t k = n_tiles - grp.n_whole;
+        if (!pix_sums) k = std::min<uint64_t>(k, scratch ? scratch_bytes / kSplitTileBytes : 0);
+        if (k > 0) {
+            TP.n_whole = n_tiles - (uint32_t)k;
+            TP.n_groups = grp.n_groups;
+            TP.group_strata = grp.group_strata;
+            if (!pix_sums) {
+                TP.tile_sums = static_cast<unsigned long long*>(scratch);
+                cudaError_t e = cudaMemsetAsync(scratch, 0, (size_t)k * kSplitTileBytes, stream);
+                if (e != cudaSuccess) return e;
+            }
+        }
+    }
+    const uint64_t n_total = (uint64_t)TP.n_whole + (uint64_t)(n_tiles - TP.n_whole) * TP.n_groups;
+    if (n_total > 0xFFFFFFF0ull) return cudaErrorInvalidValue;
+    TP.n_total = (uint32_t)n_total;
+    TP.pix_sums = pix_sums;
+    if (pix_sums) {
+        cudaError_t e = cudaMemsetAsync(pix_sums, 0, 32 * (size_t)R.w * R.h, stream);
         if (e != cudaSuccess) return e;
     }
     const bool nee = COUNT || S.n_lights > 0;
@@ -293,24 +384,23 @@ static cudaError_t launch_render_t(const SceneDev& S, const RenderDev& R, float*
     const size_t smem = (size_t)S.stack_depth * kRenderThreads * sizeof(int);
     if (blocks_per_sm == occ) blocks_per_sm = kernel_occupancy((const void*)kernel, smem);
     int grid = num_sms() * blocks_per_sm;
-    const uint64_t tasks = (uint64_t)R.n_tasks * grp.n_groups;
-    int blocks_needed = (int)((tasks + 3) / 4);   // 4 warps per block, one task per warp at least
+    int blocks_needed = (int)((n_total + 3) / 4);   // 4 warps per block, one task per warp at least
     if (grid > blocks_needed) grid = blocks_needed > 0 ? blocks_needed : 1;
     // (kernel above: scenes without the other materials and backgrounds, without lights, or
     // made of spheres with the basic materials run builds without the code they cannot reach;
     // the counter build is the general one: the same paths either way)
-    kernel<<<grid, kRenderThreads, smem, stream>>>(S, R, out, wc, gacc, grp.n_groups,
-                                                                          grp.group_strata);
+    kernel<<<grid, kRenderThreads, smem, stream>>>(S, R, out, wc, TP);
     cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess || grp.n_groups <= 1 || sums_only) return e;
-    const int cgrid = (int)std::min<size_t>((n_px + 255) / 256, (size_t)num_sms() * 8);
-    k_fixed_finalize<<<cgrid, 256, 0, stream>>>(gacc, n_px, R.exposure, out);
+    const uint32_t n_split = n_tiles - TP.n_whole;
+    if (e != cudaSuccess || pix_sums || n_split == 0) return e;
+    const int fgrid = (int)std::min<size_t>((32 * (size_t)n_split + 255) / 256, (size_t)num_sms() * 8);
+    k_split_finalize<<<fgrid, 256, 0, stream>>>(R, TP, n_split, out);
     return cudaGetLastError();
 }
 
 cudaError_t launch_render_sums(const SceneDev& S, const RenderDev& R, unsigned long long* sums, WorkCounters* wc,
                                cudaStream_t stream) {
-    return launch_render_t<false>(S, R, nullptr, wc, stream, 0, sums, render_groups(R), true);
+    return launch_render_t<false>(S, R, nullptr, wc, stream, 0, render_groups(R), nullptr, 0, sums);
 }
 
 cudaError_t launch_fixed_finalize(const unsigned long long* sums, size_t n_px, float exposure, float* out,
@@ -323,17 +413,18 @@ cudaError_t launch_fixed_finalize(const unsigned long long* sums, size_t n_px, f
 
 cudaError_t launch_render(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc, cudaStream_t stream,
                           int blocks_per_sm) {
-    return launch_render_t<false>(S, R, out, wc, stream, blocks_per_sm, nullptr, RenderGroups{1, 0});
+    return launch_render_t<false>(S, R, out, wc, stream, blocks_per_sm, RenderGroups{1, 0, R.n_tasks}, nullptr, 0,
+                                  nullptr);
 }
 
 cudaError_t launch_render_grouped(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
-                                  cudaStream_t stream, unsigned long long* gacc, RenderGroups groups) {
-    return launch_render_t<false>(S, R, out, wc, stream, 0, gacc, groups);
+                                  cudaStream_t stream, void* scratch, size_t scratch_bytes, RenderGroups groups) {
+    return launch_render_t<false>(S, R, out, wc, stream, 0, groups, scratch, scratch_bytes, nullptr);
 }
 
 cudaError_t launch_render_counted(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
                                   cudaStream_t stream) {
-    return launch_render_t<true>(S, R, out, wc, stream, 0, nullptr, RenderGroups{1, 0});
+    return launch_render_t<true>(S, R, out, wc, stream, 0, RenderGroups{1, 0, R.n_tasks}, nullptr, 0, nullptr);
 }
 
 cudaError_t launch_intersect(const SceneDev& S, const lum_ray* rays, uint32_t n, lum_hit* hits, WorkCounters* wc,

@@ -8,21 +8,25 @@
 
 namespace lum {
 
-// Launches the megakernel on `stream`.  `wc` must be zeroed beforehand.  blocks_per_sm <= 0
-// picks the occupancy limit.
+// Launches the megakernel on `stream`, whole tiles only (no scratch).  `wc` must be zeroed
+// beforehand.  blocks_per_sm <= 0 picks the occupancy limit.
 cudaError_t launch_render(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc, cudaStream_t stream,
                           int blocks_per_sm);
-// Stratum groups of a megakernel launch: frames with fewer 8x4 tiles than ~4x the resident
-// warps split each tile's strata into groups, so more tasks than warps exist.
+// Task plan of a megakernel launch (TaskPlan, device_scene.h): tiles [0, n_whole) whole, the
+// rest split into n_groups stratum groups.  Small frames split every tile; larger ones only
+// their last tiles, so the launch ends on short tasks.
 struct RenderGroups {
-    uint32_t n_groups;      // 1 = no split
+    uint32_t n_groups;      // groups per split tile (1 = no split)
     uint32_t group_strata;  // strata per group
+    uint32_t n_whole;       // tiles rendered whole
 };
 RenderGroups render_groups(const RenderDev& R);
-// The megakernel with stratum groups: `gacc` holds 4 u64 fixed-point accumulators per pixel
-// (zeroed by the launch), which a second kernel turns into `out`.
+// Device scratch the split tiles of plan `g` need (0 without split tiles).
+size_t render_scratch_bytes(const RenderDev& R, const RenderGroups& g);
+// The megakernel with plan `groups`; `scratch` (render_scratch_bytes) holds the split tiles'
+// sums and is cleared by the launch.  With less scratch fewer tiles are split.
 cudaError_t launch_render_grouped(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc,
-                                  cudaStream_t stream, unsigned long long* gacc, RenderGroups groups);
+                                  cudaStream_t stream, void* scratch, size_t scratch_bytes, RenderGroups groups);
 // The megakernel leaving the frame's raw per-pixel sums (4 u64 fixed-point values per pixel:
 // filter-weighted R, G, B and the filter weight, 2^-32 units) in `sums`, zeroed by the launch;
 // no pixels are written.  Sums of disjoint stratum ranges add.

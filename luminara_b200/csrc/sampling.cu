@@ -113,10 +113,10 @@ __device__ __forceinline__ void sample_pool(const SceneDev& S, const RenderDev& 
         if (state == ST_DONE) {
             if (acc) {
                 const float4 v = path_sample(R, P.L, P.jx, P.jy);
-                atomicAdd(&acc[px][0], to_fixed(v.x));
-                atomicAdd(&acc[px][1], to_fixed(v.y));
-                atomicAdd(&acc[px][2], to_fixed(v.z));
-                atomicAdd(&acc[px][3], to_fixed(v.w));
+                add_fixed(&acc[px][0], v.x);
+                add_fixed(&acc[px][1], v.y);
+                add_fixed(&acc[px][2], v.z);
+                add_fixed(&acc[px][3], v.w);
             } else {
                 const V c = clamp_sample(P.L);
                 smp[k][px][0] = c.x;

@@ -124,7 +124,7 @@ __device__ __forceinline__ void store_path(const Pool& pl, uint32_t s, const Pat
                            (P.stratum & 0xFFFFFFu) | ((P.bounce & 0x7Fu) << 24) | (P.skip_emission ? 0x80000000u : 0u));
 }
 
-__device__ __forceinline__ long long fix(float v) { return llrint((double)v * kFix); }
+__device__ __forceinline__ long long fix(float v) { return (long long)to_fixed(v); }
 
 // A finished path: luminance clamp and filter weight (render.rs:1692-1701) into the
 // fixed-point accumulators of its pixel; per-scene completion bookkeeping.
@@ -529,9 +529,11 @@ lum_status run_lanes(lum_batch* b, float* const* d_outs, double* scene_done_ms, 
         cudaStream_t l = b->lanes[q % b->lanes.size()];
         const lum::RenderDev& R = b->R[s];
         if (R.n_tasks > 0 && R.s_end > R.s_begin) {
+            // the scene's slice of the batch accumulators (32 bytes per pixel) as the split tiles'
+            // scratch: as many tiles are split as it holds
             const lum::RenderGroups grp = lum::render_groups(R);
-            unsigned long long* gacc = grp.n_groups > 1 ? b->T.acc + 4 * b->acc_off[s] : nullptr;
-            WF(lum::launch_render_grouped(b->S[s], R, d_outs[s], b->d_wc + s, l, gacc, grp), "render launch");
+            WF(lum::launch_render_grouped(b->S[s], R, d_outs[s], b->d_wc + s, l, b->T.acc + 4 * b->acc_off[s],
+                                          32 * (size_t)R.w * R.h, grp), "render launch");
         } else if (R.w > 0 && R.h > 0) {
             WF(cudaMemsetAsync(d_outs[s], 0, sizeof(float) * 3 * (size_t)R.w * R.h, l), "memset image");
         }

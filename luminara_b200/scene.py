@@ -492,21 +492,82 @@ class World:
         return SceneDesc(self)
 
 
+_ZEROS = tuple((0.0,) * k for k in range(13))
+
+
+def _object_array(objs, materials, transforms) -> np.ndarray:
+    """The objects as OBJECT_DTYPE records, filled column by column."""
+    n = len(objs)
+    a = np.zeros(n, dtype=OBJECT_DTYPE)
+    if not n:
+        return a
+    flat = []
+    for o in objs:
+        p = o.params
+        if len(p) > 12:
+            p = p[:12]
+        flat.extend(p)
+        flat.extend(_ZEROS[12 - len(p)])
+    a["kind"] = [o.kind for o in objs]
+    a["material"] = materials
+    a["transform"] = transforms
+    a["p"] = np.array(flat, dtype=np.float64).reshape(n, 12)
+    return a
+
+
+def _material_array(mats, index_of) -> np.ndarray:
+    """The materials as MATERIAL_DTYPE records: the fields Material.to_c sets, filled column by
+    column."""
+    n = len(mats)
+    a = material_array(n)
+    if not n:
+        return a
+    texture, color, color2, scale = [], [], [], []
+    for m in mats:
+        t, c, c2, sc = abi.TEX_SOLID, m.color, (0.0, 0.0, 0.0), 1.0
+        tex = m.texture
+        if isinstance(tex, SolidColor):
+            c = tex.color
+        elif isinstance(tex, Checker):
+            t, c, c2, sc = abi.TEX_CHECKER, tex.even, tex.odd, tex.scale
+        if m.color2 is not None:
+            c2 = m.color2
+        texture.append(t)
+        color.extend(c)
+        color2.extend(c2)
+        scale.append(sc)
+    a["kind"] = [m.kind for m in mats]
+    a["texture"] = texture
+    a["color"] = np.array(color, dtype=np.float64).reshape(n, 3)
+    a["color2"] = np.array(color2, dtype=np.float64).reshape(n, 3)
+    a["tex_scale"] = scale
+    for f in ("fuzz", "ior", "roughness", "metallic", "intensity", "dispersion"):
+        a[f] = [getattr(m, f) for m in mats]
+    a["tint"] = np.array([x for m in mats for x in m.tint], dtype=np.float64).reshape(n, 3)
+    ex = []
+    for m in mats:
+        e = tuple(m.extra)[:4]
+        ex.extend(e)
+        ex.extend(_ZEROS[4 - len(e)])
+    a["extra"] = np.array(ex, dtype=np.float64).reshape(n, 4)
+    for k, m in enumerate(mats):
+        if m.children is not None:
+            a["sub"][k] = [index_of(c) for c in m.children]
+    return a
+
+
 class SceneDesc:
-    """Owns the ctypes arrays behind one lum_scene_desc."""
+    """Owns the arrays behind one lum_scene_desc.  Objects and materials are built as numpy
+    records laid out as lum_object / lum_material (one row per object or material) and handed
+    to the C ABI in place."""
 
     def __init__(self, world: World):
-        objs = []
         xforms = []
         for o in world.objects:
             world.material_index(o.material)
+        mat_of, tr_of = [], []
         for o in world.objects:
-            lo = abi.LumObject()
-            lo.kind = o.kind
-            lo.material = world.material_index(o.material)
-            lo.transform = -1
-            p = list(map(float, o.params)) + [0.0] * (12 - len(o.params))
-            lo.p[:] = p[:12]
+            tr = -1
             if o.xforms:
                 if len(o.xforms) > abi.MAX_XF_OPS:
                     raise ValueError("too many transform ops")
@@ -515,16 +576,15 @@ class SceneDesc:
                 for i, (op, arg) in enumerate(o.xforms):
                     t.op[i] = op
                     t.arg[i][:] = list(map(float, arg))
-                lo.transform = len(xforms)
+                tr = len(xforms)
                 xforms.append(t)
-            objs.append(lo)
+            mat_of.append(world.material_index(o.material))
+            tr_of.append(tr)
+        obj_np = _object_array(world.objects, mat_of, tr_of)
         n_mat_regular = len(world.materials)
         if world._bulk:
             # interleave the bulk chunks at their insertion positions; their material indices
             # follow the regular materials
-            obj_np = np.zeros(len(objs), dtype=OBJECT_DTYPE)
-            if objs:
-                obj_np[:] = np.frombuffer((abi.LumObject * len(objs))(*objs), dtype=OBJECT_DTYPE)
             parts, mats_np, last, mat_base = [], [], 0, n_mat_regular
             for pos, bobj, bmat in world._bulk:
                 parts.append(obj_np[last:pos])
@@ -536,16 +596,13 @@ class SceneDesc:
                 mat_base += len(bmat)
                 last = pos
             parts.append(obj_np[last:])
-            all_obj = np.concatenate(parts) if parts else np.zeros(0, dtype=OBJECT_DTYPE)
-            self._obj_np = np.ascontiguousarray(all_obj)
-            self._objects = (abi.LumObject * max(len(all_obj), 1)).from_buffer(
-                self._obj_np if len(all_obj) else np.zeros(1, dtype=OBJECT_DTYPE))
-            n_objects = len(all_obj)
+            obj_np = np.concatenate(parts)
             self._bulk_mats = np.concatenate(mats_np)
         else:
-            self._objects = (abi.LumObject * max(len(objs), 1))(*objs)
-            n_objects = len(objs)
             self._bulk_mats = None
+        n_objects = len(obj_np)
+        self._obj_np = np.ascontiguousarray(obj_np if n_objects else np.zeros(1, dtype=OBJECT_DTYPE))
+        self._objects = (abi.LumObject * len(self._obj_np)).from_buffer(self._obj_np)
         self._xforms = (abi.LumTransform * max(len(xforms), 1))(*xforms)
         self._keep = []
         meshes = []
@@ -569,17 +626,12 @@ class SceneDesc:
             lm.material = world.material_index(m.material)
             meshes.append(lm)
         self._meshes = (abi.LumMesh * max(len(meshes), 1))(*meshes)
-        mats = [m.to_c(world.material_index) for m in world.materials]
+        mat_np = _material_array(world.materials, world.material_index)
         if self._bulk_mats is not None:
-            reg = np.zeros(len(mats), dtype=MATERIAL_DTYPE)
-            if mats:
-                reg[:] = np.frombuffer((abi.LumMaterial * len(mats))(*mats), dtype=MATERIAL_DTYPE)
-            self._mat_np = np.ascontiguousarray(np.concatenate([reg, self._bulk_mats]))
-            self._materials = (abi.LumMaterial * len(self._mat_np)).from_buffer(self._mat_np)
-            n_materials = len(self._mat_np)
-        else:
-            self._materials = (abi.LumMaterial * max(len(mats), 1))(*mats)
-            n_materials = len(mats)
+            mat_np = np.concatenate([mat_np, self._bulk_mats])
+        n_materials = len(mat_np)
+        self._mat_np = np.ascontiguousarray(mat_np if n_materials else np.zeros(1, dtype=MATERIAL_DTYPE))
+        self._materials = (abi.LumMaterial * len(self._mat_np)).from_buffer(self._mat_np)
         lights = [l.to_c() for l in world.lights]
         self._lights = (abi.LumLight * max(len(lights), 1))(*lights)
         d = abi.LumSceneDesc()
