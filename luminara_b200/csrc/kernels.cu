@@ -26,9 +26,16 @@ constexpr int kRenderThreads = 128;
 // Minimum resident blocks per SM requested from the register allocator for the general
 // megakernel builds (6 -> 80 registers, 24-58 bytes of spills; on B200 3-6% faster than 5 blocks
 // at 93 registers without spills on the box-room, diff-quads and dense-mesh frames).  The
-// sphere builds use 7 blocks without lights (72 registers, no spills) and 6 with them.
+// scene-class builds (LUM_RENDER_CLASS_BLOCKS) run 7 blocks at 72 registers: more warps to hide
+// the node and triangle fetch latency outweigh their larger spills (40-124 bytes) -- on B200 the
+// dense mesh 194.2 -> 185.4 ms, the 512x512 quad frame 9.66 -> 9.33 ms, the box room unchanged
+// (8 blocks: box room 3% slower).  The sphere builds use 7 blocks without lights (72 registers,
+// no spills; 8 blocks at 64 registers gained nothing) and 6 with them.
 #ifndef LUM_RENDER_MIN_BLOCKS
 #define LUM_RENDER_MIN_BLOCKS 6
+#endif
+#ifndef LUM_RENDER_CLASS_BLOCKS
+#define LUM_RENDER_CLASS_BLOCKS 7
 #endif
 constexpr unsigned kFull = 0xffffffffu;
 
@@ -61,7 +68,8 @@ __device__ __forceinline__ void flush_counters(WorkCounters* wc, uint32_t err, u
 // CLS (CLS_QUAD, CLS_MESH): general builds carrying only the primitive tests and light samplers
 // of one scene class (SceneDev::cls).
 template <bool COUNT, bool EXT, bool NEE, bool SPH, int CLS = CLS_ALL>
-__global__ void __launch_bounds__(kRenderThreads, SPH ? (NEE ? 6 : 7) : LUM_RENDER_MIN_BLOCKS)
+__global__ void __launch_bounds__(kRenderThreads, SPH ? (NEE ? 6 : 7) : CLS != CLS_ALL ? LUM_RENDER_CLASS_BLOCKS
+                                                                               : LUM_RENDER_MIN_BLOCKS)
     k_render(SceneDev S, RenderDev R, float* __restrict__ out, WorkCounters* wc, TaskPlan TP) {
     extern __shared__ int s_stack[];
     __shared__ unsigned long long s_acc[kRenderThreads / 32][32][4];
