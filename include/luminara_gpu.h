@@ -20,7 +20,10 @@
  *   - Every entry point returns a lum_status; LUM_OK is 0.  On failure, lum_last_error()
  *     returns a message for the calling thread.
  *   - Host buffers are owned by the caller.  Device buffers created by lum_scene_create
- *     are owned by the scene handle and freed by lum_scene_destroy.
+ *     are owned by the scene handle and freed by lum_scene_destroy.  They come from one
+ *     stream-ordered memory pool per device, which keeps up to 4 GiB of freed memory for the
+ *     next scenes (creating and destroying scenes then does not call the driver's allocator);
+ *     other allocators of the process do not see that reserve.
  *   - A scene handle owns one CUDA stream; calls on one handle are serialised on it.
  *     Distinct handles may be used from distinct threads.
  *   - Geometry and material parameters are given in double precision (the reference is
@@ -330,7 +333,9 @@ const char* lum_last_error(void);
  * Zero-area sides of a box (a box flat along one axis) are left out, keeping their ids. */
 lum_status lum_scene_create(const lum_scene_desc* desc, lum_scene** out_scene);
 
-/* Frees the scene's device buffers and stream. */
+/* Frees the scene's device buffers (back to the device's pool) and stream.  Synchronises the
+ * device first, as cudaFree would, so work that other streams still run on the scene
+ * finishes before its memory is reused. */
 lum_status lum_scene_destroy(lum_scene* scene);
 
 /* Number of expanded primitives and BVH nodes (diagnostics). */
@@ -339,7 +344,9 @@ lum_status lum_scene_info(const lum_scene* scene, uint32_t* n_prims, uint32_t* n
 
 /* Replaces render::render (src/render.rs:1557-1731): renders into a caller-owned HOST
  * buffer of width*height*3 floats (crop size when has_crop).  Device output buffers are
- * owned by the scene.  stats may be NULL. */
+ * owned by the scene.  The image is read back through pinned staging buffers shared per
+ * device (4 MB chunks, copied into out_rgb by up to 8 host threads); a call that finds them
+ * in use by another thread copies directly.  stats may be NULL. */
 lum_status lum_render(lum_scene* scene, const lum_render_params* params, float* out_rgb,
                       lum_stats* stats);
 
