@@ -316,6 +316,37 @@ __device__ __forceinline__ uint32_t tone_table(float v, double exposure, const B
     return (uint32_t)(e >> 56) + (((unsigned long long)b & kTabLowMask) >= (e & (2ull * kTabLowMask + 1ull)) ? 1u : 0u);
 }
 
+// tone_table for an exposure 2^k (k2 = k): x = (double)v * 2^k is exact, so x's bits follow from v's
+// and the bucket key and the compare against the entry's threshold bits are done in 32-bit
+// integer arithmetic, with no f64 conversion or multiply.  For v normal and positive, x's
+// exponent field is v's + k + 896 and its mantissa v's shifted left 29 bits: key = x_bits >> 45 =
+// (v_bits >> 16) + ((k + 896) << 7), and x's bits below the key are (v_bits & 0xFFFF) << 29.
+// Zero, negative, non-finite, denormal and very large v (x at or above 2^99: the f64 formulas
+// take x >= 1e30) go through tone_table itself, so the bytes are tone_table's in every case.
+template <int KIND>
+__device__ __forceinline__ uint32_t tone_table_pow2(float v, int k2, double exposure, const ByteTable& T,
+                                                    float inv_gamma) {
+    const uint32_t u = __float_as_uint(v);
+    const int ef = (int)(u >> 23) + k2 + 896;                  // x's biased f64 exponent (v > 0)
+    if (u - 0x00800000u >= 0x7F000000u || ef < 1 || ef >= 1023 + 99)
+        return tone_table<KIND>(v, exposure, T, inv_gamma);    // v <= 0, denormal, inf/NaN; x tiny or huge
+    const int key = (int)(u >> 16) + ((k2 + 896) << 7);
+    const int i = min(max(key - (int)T.k0 + 1, 0), T.nb + 1);
+    const unsigned long long e = __ldg(T.tab + i);
+    const uint32_t th = (uint32_t)(e >> 32) & 0x3FFFu, tl = (uint32_t)e;   // threshold bits 0-45
+    const uint32_t m = u & 0xFFFFu, mh = m >> 3, ml = m << 29;              // x's bits 0-44
+    return (uint32_t)(e >> 56) + ((mh > th || (mh == th && ml >= tl)) ? 1u : 0u);
+}
+
+template <int KIND>
+__device__ __forceinline__ uint32_t pixel_table_pow2(float r, float g, float b, int k2, double exposure,
+                                                     const ByteTable& T, float inv_gamma) {
+    const uint32_t R = tone_table_pow2<KIND>(r, k2, exposure, T, inv_gamma);
+    const uint32_t G = tone_table_pow2<KIND>(g, k2, exposure, T, inv_gamma);
+    const uint32_t B = tone_table_pow2<KIND>(b, k2, exposure, T, inv_gamma);
+    return R | (G << 8) | (B << 16) | (255u << 24);
+}
+
 template <int KIND>
 __device__ __forceinline__ uint32_t pixel_table(float r, float g, float b, double exposure, const ByteTable& T,
                                                 float inv_gamma) {
@@ -402,7 +433,19 @@ __global__ void __launch_bounds__(kThreads, 6) k_tonemap(const float* __restrict
         const uint32_t n4 = n / 4;
         const float4* in = reinterpret_cast<const float4*>(hdr);
         uint4* out = reinterpret_cast<uint4*>(rgba);
-        if (!C.extra && T.tab) {   // the common chain from its byte table (uniform branch, hoisted)
+        const long long eb = __double_as_longlong(exposure);
+        const int k2 = (int)((eb >> 52) & 0x7FF) - 1023;
+        const bool pow2 = exposure > 0.0 && (eb & 0xFFFFFFFFFFFFFll) == 0 && k2 > -1000 && k2 < 1000;
+        if (!C.extra && T.tab && pow2) {   // byte table, exposure 2^k2: integer keys (uniform branch)
+            const float ig = C.inv_gamma;
+            for (uint32_t q = t0; q < n4; q += stride) {
+                const float4 a = __ldcs(in + 3 * q), b = __ldcs(in + 3 * q + 1), c = __ldcs(in + 3 * q + 2);
+                __stcs(out + q, make_uint4(pixel_table_pow2<KIND>(a.x, a.y, a.z, k2, exposure, T, ig),
+                                           pixel_table_pow2<KIND>(a.w, b.x, b.y, k2, exposure, T, ig),
+                                           pixel_table_pow2<KIND>(b.z, b.w, c.x, k2, exposure, T, ig),
+                                           pixel_table_pow2<KIND>(c.y, c.z, c.w, k2, exposure, T, ig)));
+            }
+        } else if (!C.extra && T.tab) {   // the common chain from its byte table (uniform branch, hoisted)
             const float ig = C.inv_gamma;
             for (uint32_t q = t0; q < n4; q += stride) {
                 const float4 a = __ldcs(in + 3 * q), b = __ldcs(in + 3 * q + 1), c = __ldcs(in + 3 * q + 2);

@@ -95,3 +95,26 @@ def test_render_ldr_is_the_chain_over_the_hdr_render(chain):
     want = OT.tonemap(hdr, {**CHAINS[chain], "exposure": 1.5})       # the render's exposure, not tm's
     compare(ldr, want)
     assert ldr[..., :3].max() > 100
+
+
+@pytest.mark.parametrize("exposure", [1.0, 4.0, 0.25, 2.0 ** -20])
+def test_power_of_two_exposure_integer_keys(exposure):
+    """An exposure 2^k takes the byte table with keys formed from the f32 bits (x = v * 2^k is
+    exact); zero, negative, NaN, denormal and very large values fall back to the f64 key.  The
+    bytes must be the chain's over eight decades and at those edges."""
+    import torch
+    rng = np.random.default_rng(7)
+    h, w = 64, 256
+    img = np.exp(rng.uniform(-12.0, 12.0, (h, w, 3))).astype(np.float32)
+    edges = np.array([np.nan, 0.0, -0.0, -1.0, 1e-45, 1e-39, 1.17e-38, 2.0 ** 99, 6.4e29, 1e30, 1e35, 3e38],
+                     dtype=np.float32)
+    img.reshape(-1)[: edges.size] = edges
+    d_hdr = torch.from_numpy(img).cuda()
+    d_out = torch.empty((h, w, 4), dtype=torch.uint8, device="cuda")
+    scratch = torch.empty(abi.TONEMAP_SCRATCH_BYTES, dtype=torch.uint8, device="cuda")
+    L.tonemap_device(d_hdr.data_ptr(), w, h, tm_config({"exposure": exposure}), scratch.data_ptr(), d_out.data_ptr())
+    torch.cuda.synchronize()
+    got = d_out.cpu().numpy()
+    want = OT.tonemap(img, {"exposure": exposure})
+    compare(got, want)
+    np.testing.assert_array_equal(got.reshape(-1, 4)[:4, :3].reshape(-1), want.reshape(-1, 4)[:4, :3].reshape(-1))
