@@ -38,6 +38,8 @@ struct Box {
     }
 };
 
+constexpr int kMaxBins = 64;            // largest BvhOptions::bins
+
 struct TNode {
     Box box[2];
     int first[2] = {0, 0};
@@ -51,9 +53,11 @@ struct Builder {
     std::vector<uint32_t>& order;
     std::vector<float> cent;            // 3 per primitive
     const float* pcost;                 // per-primitive test weight, or null (all 1)
+    std::vector<uint32_t> scratch;      // partition buffer; a split of [begin, end) uses only that range
 
     Builder(const std::vector<BuildBox>& b, const BvhOptions& o, std::vector<uint32_t>& ord, const float* pc)
         : boxes(b), opt(o), order(ord), pcost(pc) {
+        scratch.resize(b.size());
         cent.resize(3 * b.size());
         for (size_t i = 0; i < b.size(); ++i)
             for (int k = 0; k < 3; ++k) cent[3 * i + k] = 0.5f * (b[i].lo[k] + b[i].hi[k]);
@@ -89,20 +93,22 @@ struct Builder {
         int best_axis = -1, best_bin = -1;
         float best_cost = std::numeric_limits<float>::infinity();
         if (depth < kMedianDepth) {
+            // per-bin tallies on the stack: a split allocates nothing (heap allocations per node
+            // were most of the build time of small scenes)
             const int B = opt.bins;
-            std::vector<int> cnt(B);
-            std::vector<float> wsum(B);
-            std::vector<Box> bb(B);
-            std::vector<float> rarea(B);
-            std::vector<int> rcnt(B);
-            std::vector<float> rw(B);
+            int cnt[kMaxBins];
+            float wsum[kMaxBins];
+            Box bb[kMaxBins];
+            float rarea[kMaxBins];
+            int rcnt[kMaxBins];
+            float rw[kMaxBins];
             for (int ax = 0; ax < 3; ++ax) {
                 float ext = cb.hi[ax] - cb.lo[ax];
                 if (!(ext > 0.0f)) continue;
                 float scale = (float)B / ext;
-                std::fill(cnt.begin(), cnt.end(), 0);
-                std::fill(wsum.begin(), wsum.end(), 0.0f);
-                std::fill(bb.begin(), bb.end(), Box());
+                std::fill(cnt, cnt + B, 0);
+                std::fill(wsum, wsum + B, 0.0f);
+                std::fill(bb, bb + B, Box());
                 for (int i = begin; i < end; ++i) {
                     uint32_t p = order[i];
                     int k = bin_of(cent[3 * p + ax], cb.lo[ax], scale, B);
@@ -146,10 +152,18 @@ struct Builder {
                 float lo = cb.lo[best_axis];
                 const float* cp = cent.data();
                 int ax = best_axis, bin = best_bin;
-                auto it = std::stable_partition(order.begin() + begin, order.begin() + end, [&](uint32_t p) {
-                    return bin_of(cp[3 * p + ax], lo, scale, B2) < bin;
-                });
-                int mid = (int)(it - order.begin());
+                // stable partition (the left side first, each side in its previous order),
+                // the right side through the range's part of the scratch buffer
+                int l = begin, r = begin;
+                for (int i = begin; i < end; ++i) {
+                    const uint32_t p = order[i];
+                    if (bin_of(cp[3 * p + ax], lo, scale, B2) < bin)
+                        order[l++] = p;
+                    else
+                        scratch[r++] = p;
+                }
+                std::copy(scratch.begin() + begin, scratch.begin() + r, order.begin() + l);
+                int mid = l;
                 if (mid > begin && mid < end) return mid;
             }
         }
@@ -227,6 +241,7 @@ BvhResult build_bvh(const std::vector<BuildBox>& boxes, const BvhOptions& option
     BvhOptions opt = options;
     opt.max_leaf = std::max(1, std::min(opt.max_leaf, 8));        // a link holds count - 1 in 3 bits
     opt.force_leaf = std::max(1, std::min(opt.force_leaf, opt.max_leaf));
+    opt.bins = std::max(2, std::min(opt.bins, kMaxBins));
     const int n = (int)boxes.size();
     res.order.resize(n);
     for (int i = 0; i < n; ++i) res.order[i] = (uint32_t)i;
@@ -250,7 +265,7 @@ BvhResult build_bvh(const std::vector<BuildBox>& boxes, const BvhOptions& option
         root->first[1] = b1;
         root->count[1] = n - b1;
     } else {
-#pragma omp parallel
+#pragma omp parallel if (n > 65536)
 #pragma omp single
         root = b.inner(0, mid, n, 0);
     }
