@@ -626,7 +626,7 @@ __global__ void __launch_bounds__(128, LUM_ADJ_MIN_BLOCKS) k_replay(SceneDev S, 
         bool found = false, walking = false;
         for (;;) {
             if (state == A_IDLE && st < s_hi) {
-                start_path(S, R, gi, gj, pixel, st, P);
+                start_path<philox_unroll<CLS>()>(S, R, gi, gj, pixel, st, P);
                 cur = st++;
                 K = 0;
                 bg = mk(0.f, 0.f, 0.f);

@@ -115,7 +115,7 @@ __device__ __forceinline__ void tile_task(const SceneDev& S, const RenderDev& R,
                 const uint32_t st = s_lo + idx / nv;
                 const uint32_t gi = x0 + cur % tw + R.crop_x, gj = y0 + cur / tw + R.crop_y;
                 pixel = gj * R.full_w + gi;
-                start_path(S, R, gi, gj, pixel, st, P);
+                start_path<philox_unroll<CLS>()>(S, R, gi, gj, pixel, st, P);
                 state = R.max_depth > 0 ? ST_CLOSEST : ST_DONE;
             }
         }

@@ -46,24 +46,40 @@ __device__ __forceinline__ V reflect(V v, V n) { return v - n * (2.0f * dot(v, n
 __device__ __forceinline__ bool has_nan(V a) { return isnan(a.x) || isnan(a.y) || isnan(a.z); }
 
 // -------------------------------------------------------------------------------- RNG
-// Philox4x32-10 (Salmon et al., SC'11).
+// Philox4x32-10 (Salmon et al., SC'11).  U: unroll factor of the ten rounds (philox_unroll).
+__device__ __forceinline__ void philox_round(uint4& c, uint32_t k0, uint32_t k1) {
+    uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+    uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+    c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+}
+template <int U = 10>
 __device__ __forceinline__ uint4 philox(uint4 c, uint32_t k0, uint32_t k1) {
+    if constexpr (U >= 10) {
 #pragma unroll
-    for (int r = 0; r < 10; ++r) {
-        if (r > 0) {
-            k0 += 0x9E3779B9u;
-            k1 += 0xBB67AE85u;
+        for (int r = 0; r < 10; ++r) {
+            if (r > 0) {
+                k0 += 0x9E3779B9u;
+                k1 += 0xBB67AE85u;
+            }
+            philox_round(c, k0, k1);
         }
-        uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
-        uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
-        c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+    } else {
+#pragma unroll U
+        for (int r = 0; r < 10; ++r) {
+            if (r > 0) {
+                k0 += 0x9E3779B9u;
+                k1 += 0xBB67AE85u;
+            }
+            philox_round(c, k0, k1);
+        }
     }
     return c;
 }
 __device__ __forceinline__ float u24(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
+template <int U = 10>
 __device__ __forceinline__ float4 draw4(uint32_t k0, uint32_t k1, uint32_t pixel, uint32_t stratum, uint32_t bounce,
                                         uint32_t call) {
-    uint4 o = philox(make_uint4(pixel, stratum, bounce, call), k0, k1);
+    uint4 o = philox<U>(make_uint4(pixel, stratum, bounce, call), k0, k1);
     return make_float4(u24(o.x), u24(o.y), u24(o.z), u24(o.w));
 }
 enum : uint32_t { CALL_CAMERA = 0, CALL_CAMERA2 = 1, CALL_SCATTER = 2, CALL_NEE = 3, CALL_EXTRA = 4, CALL_BLEND = 5 };
@@ -252,6 +268,14 @@ enum : int {
     CLS_QUAD = 1,   // quads (rects, boxes) with rect lights (box room, quad scenes)
     CLS_MESH = 2    // triangles, disks and media with disk and rect lights (meshes)
 };
+
+// Unroll factor of the Philox rounds in a scene-class build.  The mesh class's megakernel is
+// bound by instruction fetch (no_instructions is a quarter of its stall samples), and each
+// inlined draw site carries the ten rounds: rolled by two they shrink it, and the dense mesh
+// ran 186.1 -> 173.3 ms on B200; the sphere field, bound by issue, ran 6% slower that way and
+// keeps them unrolled, as do the other classes (box room 1% slower rolled).
+template <int CLS>
+constexpr int philox_unroll() { return CLS == CLS_MESH ? 2 : 10; }
 template <int CLS>
 __host__ __device__ constexpr bool cls_has_prim(int type) {
     return CLS == CLS_ALL || (CLS == CLS_QUAD && type == PT_QUAD) ||
@@ -776,7 +800,7 @@ __device__ __forceinline__ ScatterMore scatter_more(const MatDev* mp, V rd, V hp
 // EXT = false leaves out the other materials (material.rs:396-865): kernels for scenes
 // without them carry none of their code (the megakernel is sensitive to its code size).
 // SPH: the scene's materials are Lambertian / Metal / Dielectric / Emissive only.
-template <int KIND = -1, bool EXT = true, bool SPH = false>
+template <int KIND = -1, bool EXT = true, bool SPH = false, int U = 10>
 __device__ __forceinline__ bool scatter(const MatDev& m, const Ray& ray, const Surface& sf, float hit_t, float4 s,
                                         const RenderDev& R, uint32_t pixel, uint32_t stratum, uint32_t bounce,
                                         Scatter& out) {
@@ -805,7 +829,7 @@ __device__ __forceinline__ bool scatter(const MatDev& m, const Ray& ray, const S
             float ior = m.ior;
             V chan = mk(1.f, 1.f, 1.f);
             if (m.dispersion > 0.0f) {
-                float4 ex = draw4(R.key0, R.key1, pixel, stratum, bounce, CALL_EXTRA);
+                float4 ex = draw4<U>(R.key0, R.key1, pixel, stratum, bounce, CALL_EXTRA);
                 uint32_t ch = (uint32_t)(ex.x * 3.0f);
                 ior += ch == 0 ? -m.dispersion : (ch == 1 ? 0.0f : m.dispersion);
                 chan = ch == 0 ? mk(3.f, 0.f, 0.f) : (ch == 1 ? mk(0.f, 3.f, 0.f) : mk(0.f, 0.f, 3.f));
@@ -1087,6 +1111,7 @@ __device__ __forceinline__ unsigned long long globaltimer() {
 
 // Camera ray through sub-pixel position (jx, jy) of pixel (gi, gj) for stratum st; c holds
 // the stratum's camera draws (z, w: lens) (render.rs:1683-1690, camera.rs:82-102).
+template <int U = 10>
 __device__ __forceinline__ void start_path_at(const SceneDev& S, const RenderDev& R, uint32_t gi, uint32_t gj,
                                               uint32_t pixel, uint32_t st, float4 c, float jx, float jy, Path& P) {
     P.jx = jx;
@@ -1121,7 +1146,7 @@ __device__ __forceinline__ void start_path_at(const SceneDev& S, const RenderDev
     }
     // time matters only to moving spheres; a static scene skips the draw (the keyed draws of
     // the other calls do not depend on it)
-    P.ray.time = S.moving ? draw4(R.key0, R.key1, pixel, st, 0, CALL_CAMERA2).x : 0.0f;
+    P.ray.time = S.moving ? draw4<U>(R.key0, R.key1, pixel, st, 0, CALL_CAMERA2).x : 0.0f;
     P.beta = mk(1.f, 1.f, 1.f);
     P.L = mk(0.f, 0.f, 0.f);
     P.stratum = st;
@@ -1130,12 +1155,13 @@ __device__ __forceinline__ void start_path_at(const SceneDev& S, const RenderDev
 }
 
 // Camera ray of stratum st: stratified jitter (render.rs:1683-1690).
+template <int U = 10>
 __device__ __forceinline__ void start_path(const SceneDev& S, const RenderDev& R, uint32_t gi, uint32_t gj,
                                            uint32_t pixel, uint32_t st, Path& P) {
     uint32_t sx = st % R.sqrt_spp, sy = st / R.sqrt_spp;
-    float4 c = draw4(R.key0, R.key1, pixel, st, 0, CALL_CAMERA);
+    float4 c = draw4<U>(R.key0, R.key1, pixel, st, 0, CALL_CAMERA);
     float inv_n = 1.0f / (float)R.sqrt_spp;
-    start_path_at(S, R, gi, gj, pixel, st, c, ((float)sx + c.x) * inv_n, ((float)sy + c.y) * inv_n, P);
+    start_path_at<U>(S, R, gi, gj, pixel, st, c, ((float)sx + c.x) * inv_n, ((float)sy + c.y) * inv_n, P);
 }
 
 // The one sample of a pixel after the time limit: stratum 0's draws, the pixel centre
@@ -1195,11 +1221,11 @@ __device__ __forceinline__ int shade(const SceneDev& S, const RenderDev& R, uint
     const MatDev& m = S.mats[sf.mat];
     V e = P.skip_emission ? mk(0.f, 0.f, 0.f)
                           : (EXT && KIND < 0 ? emitted_at(S, sf.mat, m, sf.p) : emitted(m, sf.p));
-    float4 su = draw4(R.key0, R.key1, pixel, P.stratum, P.bounce, CALL_SCATTER);
+    float4 su = draw4<philox_unroll<CLS>()>(R.key0, R.key1, pixel, P.stratum, P.bounce, CALL_SCATTER);
     Scatter sc;
     sc.org = sf.p;
     const MatDev& ms = EXT && KIND < 0 ? blend_leaf(S, m, R, pixel, P.stratum, P.bounce) : m;
-    if (!scatter<KIND, EXT, SPH>(ms, P.ray, sf, h.t, su, R, pixel, P.stratum, P.bounce, sc)) {
+    if (!scatter<KIND, EXT, SPH, philox_unroll<CLS>()>(ms, P.ray, sf, h.t, su, R, pixel, P.stratum, P.bounce, sc)) {
         P.L = P.L + mul(P.beta, e);
         return ST_DONE;
     }
@@ -1214,7 +1240,7 @@ __device__ __forceinline__ int shade(const SceneDev& S, const RenderDev& R, uint
     // that ends below no longer reads its ray)
     P.ray.o = sc.org;
     P.ray.d = sc.dir;
-    float4 nu = draw4(R.key0, R.key1, pixel, P.stratum, P.bounce, CALL_NEE);
+    float4 nu = draw4<philox_unroll<CLS>()>(R.key0, R.key1, pixel, P.stratum, P.bounce, CALL_NEE);
     float surv = fminf(fmaxf(fmaxf(fmaxf(sc.att.x, sc.att.y), sc.att.z), 0.05f), 1.0f);
     if (depth < 47 && nu.x > surv) {                                   // Russian roulette
         P.L = P.L + mul(P.beta, e);
