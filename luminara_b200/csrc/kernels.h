@@ -13,8 +13,8 @@ namespace lum {
 cudaError_t launch_render(const SceneDev& S, const RenderDev& R, float* out, WorkCounters* wc, cudaStream_t stream,
                           int blocks_per_sm);
 // Task plan of a megakernel launch (TaskPlan, device_scene.h): tiles [0, n_whole) whole, the
-// rest split into n_groups stratum groups.  Small frames split every tile; larger ones only
-// their last tiles, so the launch ends on short tasks.
+// rest split into n_groups stratum groups.  Small frames split every tile; larger frames render
+// whole tiles (splitting their last tiles is available, LUM_TAIL_TILES_PER_WARP, and off).
 struct RenderGroups {
     uint32_t n_groups;      // groups per split tile (1 = no split)
     uint32_t group_strata;  // strata per group

@@ -514,9 +514,9 @@ lum_status enqueue_iteration(lum_batch* b) {
 
 std::mutex g_const_mu;   // guards the constant scene tables of megakernel-mode renders
 
-// Streams mode: each scene is lum_render's launch (the megakernel, stratum groups as
-// lum_render chooses them, the scene's slice of the batch accumulators as their fixed-point
-// sums), issued heaviest first round robin over the lanes with no host synchronisation in
+// Streams mode: each scene is lum_render's launch (the megakernel, the task plan lum_render
+// chooses, the scene's slice of the batch accumulators as the split tiles' fixed-point sums),
+// issued heaviest first round robin over the lanes with no host synchronisation in
 // between, so the hardware starts a scene's CTAs as the previous scenes' CTAs retire.
 lum_status run_lanes(lum_batch* b, float* const* d_outs, double* scene_done_ms, lum_batch_stats* stats,
                      std::chrono::steady_clock::time_point t0) {
