@@ -627,7 +627,9 @@ cudaError_t launch_tonemap(const float* hdr, uint32_t w, uint32_t h, const lum_t
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const size_t work = vec ? (n + 3) / 4 : n;
-    const int grid = (int)std::min<size_t>((work + tone::kThreads - 1) / tone::kThreads, (size_t)nsm * 64);
+    // at most two resident waves (6 blocks/SM), threads looping over the rest: on B200 the 1080p
+    // frame 20.5 -> 18.4 us against one block per 256 quads (2.3 waves), the 8K frame unchanged
+    const int grid = (int)std::min<size_t>((work + tone::kThreads - 1) / tone::kThreads, (size_t)nsm * 12);
     auto go = [&](auto kind) {
         constexpr int K = decltype(kind)::value;
         if (vec)
